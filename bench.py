@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the batched 1D lookup-table integration on B200.
+
+Workload (default): Eiger-4M-shaped detector (2167 x 2070, 75 um pixels,
+tilted, module gaps + 2% dead pixels masked), 256 seeded uint32 frames,
+PixelSplit, 2000 radial bins, errors + azimuthal spread. One step integrates
+the 256 frames already resident in HBM with one batched gather launch (plus
+its finalize pass). Frames are Poisson-sampled on the device from a seeded
+ring pattern; no dataset is read.
+
+Reported on one JSON line (rank 0):
+  value     whole-job frames/s, device-resident frames, max over ranks
+  e2e       frames/s through dg_integrate with pinned HOST frames: copies in,
+            gather, results back, every step
+  roofline  achieved GB/s of the gather kernel (algorithmic bytes / its
+            CUDA-event time) against the measured HBM copy bandwidth
+  plain     frames/s of the one-frame-per-launch GPU path on the same frames
+  cpu_baseline  the CPU oracle (restated reference algorithm) on host cores
+
+Multi-GPU: one process per GPU (torchrun); every rank integrates its own 256
+frames (frames are independent: weak scaling, no collective on the data path).
+`--impl reference` times the reference's CPU algorithm (the C oracle port,
+since the Rust crate cannot be built here) on all host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "eiger4m_1d_frames_per_s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="eiger4m_ps2000_b256")
+    ap.add_argument("--frames", type=int, default=None, help="frames per step (default: workload)")
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e, plain and CPU legs")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def cpu_reference(w, frames_np, threads: int, budget_s: float, n_steps: int):
+    """Times the oracle (restated reference CPU algorithm) frame-parallel on
+    host cores; returns (frames/s, frames per sample, seconds)."""
+    from oracle import oracle as o
+    p = o.poni(**w.poni_dict())
+    full = o.build_ps1d(p, w.dim1, w.dim2, w.n_points)
+    mask = w.mask().ravel()
+    norm = o.centres(p, w.dim1, w.dim2, polarization_factor=w.polarization_factor)["norm"]
+    table = o.compact(full, mask)
+    den = o.denominators(table, norm)
+    # calibrate on a small sample, then size the per-step sample to the budget
+    t = time.perf_counter()
+    o.integrate_frames_mt(table, den, full, mask, norm, frames_np[:2], w.errors,
+                          w.azimuthal_std, threads)
+    rate = 2 / (time.perf_counter() - t)
+    per_step = max(1, min(len(frames_np), int(budget_s * rate / max(1, n_steps))))
+    times = []
+    for _ in range(n_steps):
+        t = time.perf_counter()
+        o.integrate_frames_mt(table, den, full, mask, norm, frames_np[:per_step], w.errors,
+                              w.azimuthal_std, threads)
+        times.append(time.perf_counter() - t)
+    return per_step * n_steps / sum(times), per_step, sum(times)
+
+
+def run_reference(args, w):
+    import numpy as np
+    from dioptrin_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    n_src = 16
+    frames = W.frames_numpy(w, n_src)
+    steps = args.steps + args.warmup
+    rate, per_step, secs = cpu_reference(w, frames, threads, 120.0, steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(rate, 3), "unit": "frames/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * per_step / rate, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "frames_per_step": per_step, "n_points": w.n_points,
+                   "method": w.method, "errors": w.errors, "azimuthal_std": w.azimuthal_std},
+        "cpu_baseline": {"value": round(rate, 3), "unit": "frames/s", "cores": threads,
+                         "kind": "port",
+                         "sample": f"{per_step} frames per step x {steps} steps of {w.name}; "
+                                   "C restatement of the reference's strict CSR row kernel "
+                                   "and azimuthal spread, frames in parallel"},
+        "e2e": {"value": round(rate, 3), "unit": "frames/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    from dioptrin_b200 import workloads as W
+    w = W.WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, w)
+        return
+
+    import numpy as np
+    import torch
+    import dioptrin_b200 as dg
+    from dioptrin_b200 import _native as N
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    n_frames = args.frames or w.n_frames
+    it = dg.Integrator.from_poni_dict(w.poni_dict(), method=w.method, n_ss=w.n_ss,
+                                      polarization_factor=w.polarization_factor)
+    it.set_mask(w.mask())
+    plan = it.prepare_cuda1d(w.shape, w.n_points, device=local)
+    info = plan.info()
+    L = N.lib()
+    frames = W.frames_torch(w, n_frames, device=f"cuda:{local}")
+    nb = w.n_points
+    oi = torch.empty((n_frames, nb), dtype=torch.float64, device=frames.device)
+    os_ = torch.empty_like(oi)
+    od = torch.empty_like(oi)
+    flags = (N.DG_ERRORS if w.errors else 0) | (N.DG_AZIMUTHAL_STD if w.azimuthal_std else 0)
+    dtype_code = {"uint16": 0, "uint32": 1, "int32": 2, "float32": 3, "float64": 4}[w.dtype]
+    stream = torch.cuda.current_stream()
+
+    def step(fn=L.dg_integrate_device, nf=n_frames):
+        N.check(fn(plan.handle, C.c_void_p(frames.data_ptr()), dtype_code, nf, flags,
+                   C.c_void_p(oi.data_ptr()), C.c_void_p(os_.data_ptr()),
+                   C.c_void_p(od.data_ptr()), C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    N.check(L.dg_plan_profile(plan.handle, 1))
+    N.check(L.dg_plan_kernel_time(plan.handle, 1, None, None, None))
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    gms, gl, launches = C.c_double(), C.c_int64(), C.c_int64()
+    N.check(L.dg_plan_kernel_time(plan.handle, 1, C.byref(gms), C.byref(gl),
+                                  C.byref(launches)))
+    N.check(L.dg_plan_profile(plan.handle, 0))
+    t = torch.tensor([ms], dtype=torch.float64, device=frames.device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n_frames * args.steps / (ms_max / 1000.0)
+
+    # Roofline of the gather kernel: algorithmic bytes per launch (table once,
+    # frames, outputs) over its event-timed duration.
+    E = info.table_entries
+    px = frames.element_size()
+    k_out = 1 + int(w.errors) + int(w.azimuthal_std)
+    alg = E * 8 + (nb + 1) * 4 + nb * 8 + n_frames * w.dim1 * w.dim2 * px + n_frames * nb * k_out * 8
+    per_launch_s = gms.value / 1000.0 / max(1, gl.value)
+    achieved = alg / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": w.name, "frames_per_step": n_frames, "detector": list(w.shape),
+                   "n_points": nb, "method": w.method, "errors": w.errors,
+                   "azimuthal_std": w.azimuthal_std, "table_entries": E,
+                   "l2": "inputs larger than L2: each step reads %.2f GB of frames"
+                         % (n_frames * w.dim1 * w.dim2 * px / 1e9),
+                   "parallelism": f"frames x{world} (independent, no collective)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_kind": peak_kind, "kernel": "k_gather",
+                     "alg_bytes_per_launch": alg,
+                     "kernel_ms_per_launch": round(per_launch_s * 1000, 4)},
+        "clocks": clk,
+        "gpu_launches": int(launches.value),
+        "build_ms": round(info.build_ms, 2),
+    }
+    if not args.no_extras and rank == 0:
+        # plain one-frame-per-launch GPU path on the same resident frames
+        nplain = min(n_frames, 64)
+        step(L.dg_integrate_device_plain, nplain)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        reps = 3
+        for _ in range(reps):
+            step(L.dg_integrate_device_plain, nplain)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        line["plain"] = {"value": round(nplain * reps / (p0.elapsed_time(p1) / 1000), 2),
+                         "unit": "frames/s", "frames": nplain * reps}
+        # end to end through the public host API: pinned host frames in,
+        # results back, every step
+        host = torch.empty(frames.shape, dtype=frames.dtype, pin_memory=True)
+        host.copy_(frames)
+        hi = np.empty((n_frames, nb))
+        hs = np.empty((n_frames, nb)) if w.errors else None
+        hd = np.empty((n_frames, nb)) if w.azimuthal_std else None
+        dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+        def e2e_step():
+            N.check(L.dg_integrate(plan.handle, C.c_void_p(host.data_ptr()), dtype_code,
+                                   n_frames, flags, dp(hi), dp(hs), dp(hd)))
+
+        e2e_step()
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            e2e_step()
+        dt = time.perf_counter() - t0
+        line["e2e"] = {"value": round(n_frames * reps / dt, 2), "unit": "frames/s",
+                       "h2d_bytes_per_step": int(host.numel() * host.element_size()),
+                       "d2h_bytes_per_step": int(n_frames * nb * k_out * 8)}
+        if world == 1:
+            fr_np = frames[:16].cpu().numpy()
+            rate, per_step, secs = cpu_reference(w, fr_np, os.cpu_count() or 1, 15.0, 3)
+            line["cpu_baseline"] = {
+                "value": round(rate, 3), "unit": "frames/s", "cores": os.cpu_count() or 1,
+                "kind": "port",
+                "sample": f"{per_step * 3} frames of {w.name} in 3 timed samples; C restatement "
+                          "of the reference's strict CSR row kernel and azimuthal spread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,467 @@
+// C ABI of libdioptrin_b200: plan lifecycle and integration entry points.
+//
+// Every entry point converts failures into a dg_status and a thread-local
+// message (dg_last_error); no C++ exception crosses the boundary. Calls on one
+// plan are serialised by the plan's mutex; separate plans run concurrently
+// (src/integration/cuda.rs:374-386 gives the reference's same rule).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "dg_internal.h"
+
+namespace dg {
+
+[[noreturn]] void fail(dg_status status, const std::string &message) {
+    throw Error{status, message};
+}
+
+void check_cuda(cudaError_t err, const char *what) {
+    if (err == cudaSuccess) return;
+    (void)cudaGetLastError();
+    fail(DG_DEVICE, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+}  // namespace dg
+
+namespace {
+
+thread_local std::string g_last_error;
+
+}  // namespace
+
+void dg::set_last_error(const std::string &message) { g_last_error = message; }
+
+namespace {
+
+template <class F>
+dg_status guarded(F &&f) {
+    try {
+        f();
+        return DG_OK;
+    } catch (const dg::Error &e) {
+        g_last_error = e.message;
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "host allocation failed";
+        return DG_DEVICE;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return DG_DEVICE;
+    } catch (...) {
+        g_last_error = "unknown failure";
+        return DG_DEVICE;
+    }
+}
+
+// Makes `device` current for the scope and restores the caller's device.
+struct DeviceScope {
+    int previous = -1;
+    explicit DeviceScope(int device) {
+        DG_CUDA(cudaGetDevice(&previous));
+        if (previous != device) DG_CUDA(cudaSetDevice(device));
+    }
+    ~DeviceScope() {
+        int now = -1;
+        if (cudaGetDevice(&now) == cudaSuccess && now != previous && previous >= 0)
+            cudaSetDevice(previous);
+    }
+};
+
+size_t dtype_size(int32_t dtype) {
+    switch (dtype) {
+    case DG_U16: return 2;
+    case DG_U32:
+    case DG_I32:
+    case DG_F32: return 4;
+    case DG_F64: return 8;
+    default: dg::fail(DG_INVALID_INPUT, "unknown pixel dtype " + std::to_string(dtype));
+    }
+}
+
+// check_configuration (src/integration/cuda.rs:1001-1057), in its order.
+void check_config(const dg_geometry *g, const dg_method *m, int32_t dim1, int32_t dim2,
+                  int32_t n_radial, int32_t n_azimuthal) {
+    using dg::fail;
+    if (!g || !m) fail(DG_INVALID_INPUT, "geometry and method must not be NULL");
+    if (n_radial <= 0) fail(DG_INVALID_INPUT, "n_points must be between 1 and 2147483647");
+    if (n_azimuthal < 0) fail(DG_INVALID_INPUT, "n_azimuthal must not be negative");
+    if (n_azimuthal > 0 && int64_t(n_radial) * n_azimuthal > INT32_MAX)
+        fail(DG_INVALID_INPUT, "2D bin count must be in 1..=2147483647");
+    if (dim1 <= 0 || dim2 <= 0)
+        fail(DG_INVALID_INPUT, "image shape (" + std::to_string(dim1) + ", " +
+                                   std::to_string(dim2) + ") has a zero side");
+    if (int64_t(dim1) * dim2 > int64_t(INT32_MAX))
+        fail(DG_INVALID_INPUT, "image shape exceeds 2147483647 pixels");
+    if (m->max_batch_bytes < 0) fail(DG_INVALID_INPUT, "max_batch_bytes must be positive");
+    if (m->kind < DG_METHOD_COUNTING || m->kind > DG_METHOD_SUPERSAMPLED)
+        fail(DG_UNSUPPORTED, "unknown integration method");
+    if (m->kind == DG_METHOD_SUPERSAMPLED && m->n_ss <= 0)
+        fail(DG_INVALID_INPUT, "n_ss must be positive");
+    if (m->unit < DG_UNIT_TTH_RAD || m->unit > DG_UNIT_Q_NM)
+        fail(DG_INVALID_INPUT, "unknown radial unit");
+    if ((m->unit == DG_UNIT_Q_A || m->unit == DG_UNIT_Q_NM) && !(g->wavelength > 0.0))
+        fail(DG_INVALID_INPUT, "Wavelength must be positive for q conversion");
+    if (m->precision < DG_PRECISION_F32 || m->precision > DG_PRECISION_F64)
+        fail(DG_INVALID_INPUT, "unknown precision");
+    if (m->has_radial_range &&
+        !(std::isfinite(m->radial_min) && std::isfinite(m->radial_max) &&
+          m->radial_min < m->radial_max))
+        fail(DG_INVALID_INPUT, "radial_range must be finite with min < max");
+    if (m->has_polarization &&
+        !(m->polarization_factor >= -1.0 && m->polarization_factor <= 1.0))
+        fail(DG_INVALID_INPUT, "polarization_factor must lie in [-1, 1]");
+}
+
+void check_device(int32_t device) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        dg::fail(DG_UNAVAILABLE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count)
+        dg::fail(DG_UNAVAILABLE, "CUDA device " + std::to_string(device) + " does not exist (" +
+                                     std::to_string(count) + " visible)");
+}
+
+void check_frames(const dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                  uint32_t flags, const void *oi, const void *os, const void *od) {
+    using dg::fail;
+    if (!plan) fail(DG_INVALID_INPUT, "plan must not be NULL");
+    (void)dtype_size(dtype);
+    if (n_frames < 0) fail(DG_INVALID_INPUT, "frame count must not be negative");
+    if (flags & ~(DG_ERRORS | DG_AZIMUTHAL_STD)) fail(DG_INVALID_INPUT, "unknown flags");
+    if (n_frames == 0) return;
+    if (!frames) fail(DG_INVALID_INPUT, "frames must not be NULL");
+    if (!oi) fail(DG_INVALID_INPUT, "intensity output must not be NULL");
+    if ((flags & DG_ERRORS) && !os) fail(DG_INVALID_INPUT, "errors requested without an output");
+    if ((flags & DG_AZIMUTHAL_STD) && !od)
+        fail(DG_INVALID_INPUT, "azimuthal_std requested without an output");
+    if (flags & DG_AZIMUTHAL_STD) {
+        if (plan->n_azimuthal != 0)
+            fail(DG_UNSUPPORTED, "azimuthal_std is defined for 1D tables only");
+    }
+}
+
+}  // namespace
+
+int64_t dg_plan::device_bytes() const {
+    int64_t b = 0;
+    b += full.row_ptr.bytes() + full.col.bytes() + full.w.bytes();
+    b += table.row_ptr.bytes() + table.col.bytes() + table.w.bytes();
+    b += norm.bytes();
+    b += gather.seg.bytes() + gather.row_seg.bytes() + gather.entry.bytes() +
+         gather.entry_std.bytes() + gather.den.bytes() + gather.den_std.bytes() +
+         gather.valid_std.bytes() + gather.partial.bytes();
+    b += stage_in.bytes() + stage_out.bytes();
+    return b;
+}
+
+extern "C" {
+
+dg_status dg_plan_create(const dg_geometry *geometry, const dg_method *method,
+                         const uint8_t *mask, int32_t dim1, int32_t dim2, int32_t n_radial,
+                         int32_t n_azimuthal, const double *azimuthal_range, dg_plan **out) {
+    return guarded([&] {
+        if (!out) dg::fail(DG_INVALID_INPUT, "out must not be NULL");
+        *out = nullptr;
+        check_config(geometry, method, dim1, dim2, n_radial, n_azimuthal);
+        check_device(method->device);
+        DeviceScope scope(method->device);
+        auto plan = std::make_unique<dg_plan>();
+        plan->device = method->device;
+        plan->geometry = *geometry;
+        plan->method = *method;
+        plan->dim1 = dim1;
+        plan->dim2 = dim2;
+        plan->n_radial = n_radial;
+        plan->n_azimuthal = n_azimuthal;
+        plan->n_bins = n_azimuthal ? int64_t(n_radial) * n_azimuthal : n_radial;
+        DG_CUDA(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking));
+        cudaStream_t s = plan->stream;
+        cudaEvent_t e0, e1;
+        DG_CUDA(cudaEventCreate(&e0));
+        DG_CUDA(cudaEventCreate(&e1));
+        DG_CUDA(cudaEventRecord(e0, s));
+        dg::BuildResult built;
+        try {
+            dg::build_table(*geometry, *method, dim1, dim2, n_radial, n_azimuthal,
+                            azimuthal_range, s, built);
+            const int64_t npix = int64_t(dim1) * dim2;
+            dg::DeviceArray<uint8_t> d_mask;
+            bool any = false;
+            if (mask) any = std::any_of(mask, mask + npix, [](uint8_t v) { return v != 0; });
+            if (any) {
+                d_mask.alloc(size_t(npix));
+                DG_CUDA(cudaMemcpyAsync(d_mask.ptr, mask, size_t(npix), cudaMemcpyHostToDevice, s));
+            }
+            dg::compact_table(built.full, any ? d_mask.ptr : nullptr, int32_t(npix), s, plan->table);
+            dg::make_gather_table(plan->table, built.norm.ptr, 2048, s, plan->gather);
+            DG_CUDA(cudaEventRecord(e1, s));
+            DG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            DG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            plan->build_ms = ms;
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        plan->hist_min = built.hist_min;
+        plan->hist_step = built.hist_step;
+        plan->guard_corners = built.guard_corners;
+        plan->singular_pixels = built.singular_pixels;
+        plan->full_entries = built.full.nnz;
+        plan->radial = built.radial_centres;
+        plan->azimuthal = built.azimuthal_centres;
+        plan->norm = std::move(built.norm);
+        if (method->flags & DG_PLAN_KEEP_TABLES) plan->full = std::move(built.full);
+        // Chunk budget (src/integration/cuda.rs:137-158): min(1 GiB, free/2)
+        // unless given; one frame costs pixels * 8 (f64 worst case) plus its
+        // outputs.
+        size_t free_b = 0, total_b = 0;
+        DG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        int64_t budget = method->max_batch_bytes > 0
+                             ? method->max_batch_bytes
+                             : std::min<int64_t>(int64_t(1) << 30, int64_t(free_b / 2));
+        int64_t per_frame = int64_t(dim1) * dim2 * 8 + plan->n_bins * 24;
+        plan->max_batch_frames = budget / per_frame;
+        if (plan->max_batch_frames < 1) {
+            if (method->max_batch_bytes > 0)
+                dg::fail(DG_INVALID_INPUT, "max_batch_bytes is smaller than one frame");
+            dg::fail(DG_DEVICE, "not enough free device memory for one frame");
+        }
+        *out = plan.release();
+    });
+}
+
+dg_status dg_plan_destroy(dg_plan *plan) {
+    return guarded([&] {
+        if (!plan) return;
+        {
+            std::lock_guard<std::mutex> lock(plan->mu);
+            int prev = -1;
+            cudaGetDevice(&prev);
+            cudaSetDevice(plan->device);
+            if (plan->stream) cudaStreamSynchronize(plan->stream);
+            plan->full = dg::DeviceCsr();
+            plan->table = dg::DeviceCsr();
+            plan->norm.release();
+            plan->gather = dg::GatherTable();
+            plan->stage_in.release();
+            plan->stage_out.release();
+            if (plan->stream) cudaStreamDestroy(plan->stream);
+            plan->stream = nullptr;
+            if (prev >= 0) cudaSetDevice(prev);
+        }
+        delete plan;
+    });
+}
+
+dg_status dg_plan_query(const dg_plan *plan, dg_plan_info *out) {
+    return guarded([&] {
+        if (!plan || !out) dg::fail(DG_INVALID_INPUT, "plan and out must not be NULL");
+        std::memset(out, 0, sizeof *out);
+        out->dim1 = plan->dim1;
+        out->dim2 = plan->dim2;
+        out->n_radial = plan->n_radial;
+        out->n_azimuthal = plan->n_azimuthal;
+        out->table_entries = plan->table.nnz;
+        out->full_entries = plan->full_entries;
+        out->max_batch_frames = plan->max_batch_frames;
+        out->device = plan->device;
+        out->precision = plan->method.precision;
+        out->hist_min = plan->hist_min;
+        out->hist_step = plan->hist_step;
+        out->build_ms = plan->build_ms;
+        out->device_bytes = plan->device_bytes();
+        out->guard_corners = plan->guard_corners;
+        out->singular_pixels = plan->singular_pixels;
+    });
+}
+
+dg_status dg_plan_radial(const dg_plan *plan, double *out, int64_t n) {
+    return guarded([&] {
+        if (!plan || !out) dg::fail(DG_INVALID_INPUT, "plan and out must not be NULL");
+        if (n != int64_t(plan->radial.size()))
+            dg::fail(DG_INVALID_INPUT, "radial axis has " + std::to_string(plan->radial.size()) +
+                                           " values");
+        std::copy(plan->radial.begin(), plan->radial.end(), out);
+    });
+}
+
+dg_status dg_plan_azimuthal(const dg_plan *plan, double *out, int64_t n) {
+    return guarded([&] {
+        if (!plan || !out) dg::fail(DG_INVALID_INPUT, "plan and out must not be NULL");
+        if (n != int64_t(plan->azimuthal.size()))
+            dg::fail(DG_INVALID_INPUT, "azimuthal axis has " +
+                                           std::to_string(plan->azimuthal.size()) + " values");
+        std::copy(plan->azimuthal.begin(), plan->azimuthal.end(), out);
+    });
+}
+
+dg_status dg_plan_export_table(const dg_plan *cplan, int32_t which, int64_t *row_ptr,
+                               int32_t *col, double *weight, double *denominator) {
+    return guarded([&] {
+        if (!cplan) dg::fail(DG_INVALID_INPUT, "plan must not be NULL");
+        dg_plan *plan = const_cast<dg_plan *>(cplan);
+        std::lock_guard<std::mutex> lock(plan->mu);
+        const dg::DeviceCsr *t = nullptr;
+        if (which == 0) t = &plan->table;
+        else if (which == 1) {
+            if (!plan->full.row_ptr.ptr)
+                dg::fail(DG_INVALID_INPUT, "the unmasked table needs DG_PLAN_KEEP_TABLES");
+            t = &plan->full;
+        } else dg::fail(DG_INVALID_INPUT, "which must be 0 or 1");
+        DeviceScope scope(plan->device);
+        cudaStream_t s = plan->stream;
+        if (row_ptr)
+            DG_CUDA(cudaMemcpyAsync(row_ptr, t->row_ptr.ptr, size_t(t->n_rows + 1) * 8,
+                                    cudaMemcpyDeviceToHost, s));
+        if (col && t->nnz)
+            DG_CUDA(cudaMemcpyAsync(col, t->col.ptr, size_t(t->nnz) * 4, cudaMemcpyDeviceToHost, s));
+        if (weight && t->nnz)
+            DG_CUDA(cudaMemcpyAsync(weight, t->w.ptr, size_t(t->nnz) * 8, cudaMemcpyDeviceToHost, s));
+        if (denominator) {
+            if (which != 0) dg::fail(DG_INVALID_INPUT, "denominators exist for the masked table");
+            DG_CUDA(cudaMemcpyAsync(denominator, plan->gather.den.ptr, size_t(t->n_rows) * 8,
+                                    cudaMemcpyDeviceToHost, s));
+        }
+        DG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+dg_status dg_integrate_device(dg_plan *plan, const void *d_frames, int32_t dtype,
+                              int64_t n_frames, uint32_t flags, double *d_i, double *d_s,
+                              double *d_d, void *stream) {
+    return guarded([&] {
+        check_frames(plan, d_frames, dtype, n_frames, flags, d_i, d_s, d_d);
+        if (n_frames == 0) return;
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        dg::run_gather(plan->gather, d_frames, dtype, int64_t(plan->dim1) * plan->dim2, n_frames,
+                       flags, plan->method.precision, d_i, (flags & DG_ERRORS) ? d_s : nullptr,
+                       (flags & DG_AZIMUTHAL_STD) ? d_d : nullptr, s);
+    });
+}
+
+dg_status dg_integrate_device_plain(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                    int64_t n_frames, uint32_t flags, double *d_i, double *d_s,
+                                    double *d_d, void *stream) {
+    return guarded([&] {
+        check_frames(plan, d_frames, dtype, n_frames, flags, d_i, d_s, d_d);
+        if (n_frames == 0) return;
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        const int64_t npix = int64_t(plan->dim1) * plan->dim2;
+        const size_t es = dtype_size(dtype);
+        const int64_t nb = plan->n_bins;
+        for (int64_t f = 0; f < n_frames; ++f) {
+            const void *fp = static_cast<const unsigned char *>(d_frames) + f * npix * es;
+            dg::run_gather(plan->gather, fp, dtype, npix, 1, flags, plan->method.precision,
+                           d_i + f * nb, (flags & DG_ERRORS) ? d_s + f * nb : nullptr,
+                           (flags & DG_AZIMUTHAL_STD) ? d_d + f * nb : nullptr, s);
+        }
+    });
+}
+
+dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                       uint32_t flags, double *oi, double *os, double *od) {
+    return guarded([&] {
+        check_frames(plan, frames, dtype, n_frames, flags, oi, os, od);
+        if (n_frames == 0) return;
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        cudaStream_t s = plan->stream;
+        const int64_t npix = int64_t(plan->dim1) * plan->dim2;
+        const size_t es = dtype_size(dtype);
+        const int64_t nb = plan->n_bins;
+        const int64_t chunk = std::min<int64_t>(plan->max_batch_frames, n_frames);
+        const int nout = 1 + ((flags & DG_ERRORS) ? 1 : 0) + ((flags & DG_AZIMUTHAL_STD) ? 1 : 0);
+        if (plan->stage_in.count < size_t(chunk * npix * es)) {
+            plan->stage_in.release();
+            plan->stage_in.alloc(size_t(chunk * npix * es));
+        }
+        if (plan->stage_out.count < size_t(chunk * nb * nout)) {
+            plan->stage_out.release();
+            plan->stage_out.alloc(size_t(chunk * nb * nout));
+        }
+        for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
+            const int64_t nf = std::min<int64_t>(chunk, n_frames - f0);
+            DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr,
+                                    static_cast<const unsigned char *>(frames) + f0 * npix * es,
+                                    size_t(nf * npix * es), cudaMemcpyHostToDevice, s));
+            double *di = plan->stage_out.ptr;
+            double *ds = (flags & DG_ERRORS) ? di + nf * nb : nullptr;
+            double *dd = (flags & DG_AZIMUTHAL_STD) ? di + nf * nb * (ds ? 2 : 1) : nullptr;
+            dg::run_gather(plan->gather, plan->stage_in.ptr, dtype, npix, nf, flags,
+                           plan->method.precision, di, ds, dd, s);
+            DG_CUDA(cudaMemcpyAsync(oi + f0 * nb, di, size_t(nf * nb) * 8, cudaMemcpyDeviceToHost, s));
+            if (ds)
+                DG_CUDA(cudaMemcpyAsync(os + f0 * nb, ds, size_t(nf * nb) * 8,
+                                        cudaMemcpyDeviceToHost, s));
+            if (dd)
+                DG_CUDA(cudaMemcpyAsync(od + f0 * nb, dd, size_t(nf * nb) * 8,
+                                        cudaMemcpyDeviceToHost, s));
+        }
+        DG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+dg_status dg_plan_profile(dg_plan *plan, int32_t enable) {
+    return guarded([&] {
+        if (!plan) dg::fail(DG_INVALID_INPUT, "plan must not be NULL");
+        std::lock_guard<std::mutex> lock(plan->mu);
+        plan->gather.profile = enable != 0;
+    });
+}
+
+dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *gather_ms,
+                              int64_t *gather_launches, int64_t *launches) {
+    return guarded([&] {
+        if (!plan) dg::fail(DG_INVALID_INPUT, "plan must not be NULL");
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        dg::gather_kernel_time(plan->gather, reset != 0, gather_ms, gather_launches, launches);
+    });
+}
+
+dg_status dg_device_info_get(int32_t device, dg_device_info *out) {
+    return guarded([&] {
+        if (!out) dg::fail(DG_INVALID_INPUT, "out must not be NULL");
+        std::memset(out, 0, sizeof *out);
+        out->device = device;
+        check_device(device);
+        cudaDeviceProp p{};
+        DG_CUDA(cudaGetDeviceProperties(&p, device));
+        out->available = 1;
+        out->cc_major = p.major;
+        out->cc_minor = p.minor;
+        out->sm_count = p.multiProcessorCount;
+        out->total_memory_bytes = int64_t(p.totalGlobalMem);
+        int v = 0;
+        cudaDriverGetVersion(&v);
+        out->driver_version = v;
+        std::strncpy(out->name, p.name, sizeof(out->name) - 1);
+    });
+}
+
+int32_t dg_last_error(char *buf, size_t len) {
+    const std::string &m = g_last_error;
+    if (buf && len) {
+        size_t n = std::min(len - 1, m.size());
+        std::memcpy(buf, m.data(), n);
+        buf[n] = 0;
+    }
+    return int32_t(m.size());
+}
+
+}  // extern "C"

@@ -1,0 +1,220 @@
+// Internal declarations shared by the translation units of libdioptrin_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dioptrin_gpu.h"
+
+namespace dg {
+
+// Error carried from the point of failure to the C ABI, which stores the
+// message in the calling thread's last-error slot and returns the status.
+struct Error {
+    dg_status status;
+    std::string message;
+};
+
+[[noreturn]] void fail(dg_status status, const std::string &message);
+// Stores `message` as the calling thread's dg_last_error text.
+void set_last_error(const std::string &message);
+void check_cuda(cudaError_t err, const char *what);
+#define DG_CUDA(call) ::dg::check_cuda((call), #call)
+
+// Device allocation owned by a plan; freed with the plan.
+template <typename T>
+struct DeviceArray {
+    T *ptr = nullptr;
+    size_t count = 0;
+    DeviceArray() = default;
+    DeviceArray(const DeviceArray &) = delete;
+    DeviceArray &operator=(const DeviceArray &) = delete;
+    DeviceArray(DeviceArray &&o) noexcept : ptr(o.ptr), count(o.count) {
+        o.ptr = nullptr;
+        o.count = 0;
+    }
+    DeviceArray &operator=(DeviceArray &&o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            count = o.count;
+            o.ptr = nullptr;
+            o.count = 0;
+        }
+        return *this;
+    }
+    ~DeviceArray() { release(); }
+    void alloc(size_t n) {
+        release();
+        if (n == 0) n = 1;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&ptr), n * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            (void)cudaGetLastError();
+            fail(DG_DEVICE, "device allocation of " + std::to_string(n * sizeof(T)) +
+                                " bytes failed: " + cudaGetErrorString(e));
+        }
+        count = n;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+// Geometry scalars the device kernels need. Trigonometric constants and the
+// q scale are computed on the host with the C library so that they are the
+// same bits the reference computes (geometry.rs:640-660, integration.rs:147-158).
+struct GeomParams {
+    double pixel1, pixel2, distance, poni1, poni2;
+    double s1, c1, s2, c2, s3, c3;
+    double wavelength, q_scale;
+    int unit;
+    int has_pol;
+    double pol_factor;
+};
+
+GeomParams make_geom_params(const dg_geometry &g, const dg_method &m);
+
+// A CSR table in device memory, as produced by the builders (f64 weights,
+// the reference's Lut1d/Lut2d) or compacted for the gather.
+struct DeviceCsr {
+    int64_t n_rows = 0;
+    int64_t nnz = 0;
+    DeviceArray<int64_t> row_ptr;  // n_rows + 1
+    DeviceArray<int32_t> col;      // nnz
+    DeviceArray<double> w;         // nnz
+};
+
+struct BuildResult {
+    DeviceCsr full;                 // unmasked table
+    double hist_min = 0, hist_step = 0;
+    int64_t guard_corners = 0;
+    int64_t singular_pixels = 0;
+    DeviceArray<double> norm;       // per-pixel pol*sa (f64)
+    std::vector<double> radial_centres;
+    std::vector<double> azimuthal_centres;
+};
+
+// Device CSR construction (dg_build.cu).
+void build_table(const dg_geometry &g, const dg_method &m, int32_t dim1, int32_t dim2,
+                 int32_t n_radial, int32_t n_azimuthal, const double *azimuthal_range,
+                 cudaStream_t stream, BuildResult &out);
+// Order-preserving mask compaction (fixed_table) + strict f64 denominators.
+void compact_table(const DeviceCsr &full, const uint8_t *d_mask, int32_t n_pixels,
+                   cudaStream_t stream, DeviceCsr &out);
+void denominators(const DeviceCsr &table, const double *d_norm, cudaStream_t stream,
+                  double *d_den);
+
+// Gather-side table: packed entries + row segments (dg_gather.cu).
+struct GatherTable {
+    int32_t n_rows = 0;
+    int64_t nnz = 0;
+    int32_t n_segments = 0;
+    int32_t seg_len = 0;
+    DeviceArray<int4> seg;          // {row, begin, end, first_of_row}
+    DeviceArray<int32_t> row_seg;   // n_rows + 1: segments of row r
+    DeviceArray<int2> entry;        // {col, weight bits} for the I/sigma path
+    DeviceArray<float4> entry_std;  // {col bits, c, n, c/n} for the spread path
+    DeviceArray<double> den;        // strict f64 Σ w·norm
+    DeviceArray<double> den_std;    // Σ c·n over entries valid for the spread
+    DeviceArray<int32_t> valid_std; // entries valid for the spread, per row
+    DeviceArray<float> partial;     // scratch: per (segment, frame) double-word sums
+    int64_t partial_frames = 0;
+    // Optional CUDA-event timing of the gather launches (dg_plan_profile).
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    size_t events_used = 0;
+    int64_t launches = 0;  // every kernel launch of run_gather since the last reset
+    ~GatherTable() {
+        for (auto &e : events) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    }
+    GatherTable() = default;
+    GatherTable(const GatherTable &) = delete;
+    GatherTable &operator=(GatherTable &&o) noexcept {
+        if (this != &o) {
+            for (auto &e : events) {
+                cudaEventDestroy(e.first);
+                cudaEventDestroy(e.second);
+            }
+            n_rows = o.n_rows;
+            nnz = o.nnz;
+            n_segments = o.n_segments;
+            seg_len = o.seg_len;
+            seg = std::move(o.seg);
+            row_seg = std::move(o.row_seg);
+            entry = std::move(o.entry);
+            entry_std = std::move(o.entry_std);
+            den = std::move(o.den);
+            den_std = std::move(o.den_std);
+            valid_std = std::move(o.valid_std);
+            partial = std::move(o.partial);
+            partial_frames = o.partial_frames;
+            profile = o.profile;
+            events = std::move(o.events);
+            o.events.clear();
+            events_used = o.events_used;
+            launches = o.launches;
+        }
+        return *this;
+    }
+};
+
+// Sums the recorded gather-kernel event pairs (synchronising on the last);
+// reset clears them.
+void gather_kernel_time(GatherTable &t, bool reset, double *ms, int64_t *gather_launches,
+                        int64_t *launches);
+
+void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t seg_len,
+                       cudaStream_t stream, GatherTable &out);
+// Enqueues the batched gather for n_frames device-resident frames.
+void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
+                int64_t n_frames, uint32_t flags, int precision, double *d_i, double *d_sigma,
+                double *d_std, cudaStream_t stream);
+// Number of gather kernel launches run_gather enqueues (for launch counting).
+int gather_launches_per_call();
+
+// Exclusive scans (dg_scan.cu). `temp` sizing via scan_temp_bytes.
+size_t scan_temp_bytes(int64_t n);
+void exclusive_scan_i32_to_i64(const int32_t *in, int64_t *out, int64_t n, void *temp,
+                               cudaStream_t stream);
+void exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *temp,
+                        cudaStream_t stream);
+
+}  // namespace dg
+
+struct dg_plan {
+    std::mutex mu;
+    int32_t device = 0;
+    cudaStream_t stream = nullptr;
+    dg_geometry geometry{};
+    dg_method method{};
+    int32_t dim1 = 0, dim2 = 0, n_radial = 0, n_azimuthal = 0;
+    int64_t n_bins = 0;
+    double hist_min = 0, hist_step = 0;
+    double build_ms = 0;
+    int64_t guard_corners = 0, singular_pixels = 0;
+    int64_t full_entries = 0;
+    std::vector<double> radial, azimuthal;
+    dg::DeviceCsr full;      // kept with DG_PLAN_KEEP_TABLES
+    dg::DeviceCsr table;     // masked, f64 weights (export)
+    dg::DeviceArray<double> norm;
+    dg::GatherTable gather;
+    int64_t max_batch_frames = 0;
+    // staging for host-memory calls
+    dg::DeviceArray<unsigned char> stage_in;
+    dg::DeviceArray<double> stage_out;
+    int64_t device_bytes() const;
+    ~dg_plan() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};

@@ -1,0 +1,536 @@
+"""Python surface of the B200 integration path, mirroring the reference's
+Python bindings (dioptrin.pyi: ``Integrator`` :337, ``batch1d`` :845,
+``batch1d_iter`` :906, ``Cuda1dPlan`` :1358) so existing callers keep working.
+
+Every integration runs on the GPU through libdioptrin_b200.so; there is no
+CPU path. Without a usable device the calls raise ``CudaUnavailableError``,
+as the reference's CUDA plans do.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import threading
+from dataclasses import dataclass
+from typing import Iterable, Iterator, Optional, Sequence, Union
+
+import numpy as np
+
+from . import _native as N
+from ._native import CudaUnavailableError
+
+_DTYPES = {np.dtype(np.uint16): 0, np.dtype(np.uint32): 1, np.dtype(np.int32): 2,
+           np.dtype(np.float32): 3, np.dtype(np.float64): 4}
+
+
+def _dp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class Poni:
+    """Calibration (src/poni.rs:13-24), SI units, radians."""
+    pixel1: float = 0.0
+    pixel2: float = 0.0
+    distance: float = 0.0
+    poni1: float = 0.0
+    poni2: float = 0.0
+    rot1: float = 0.0
+    rot2: float = 0.0
+    rot3: float = 0.0
+    wavelength: float = 0.0
+
+    _KEYS = {"PixelSize1": "pixel1", "PixelSize2": "pixel2", "Distance": "distance",
+             "Poni1": "poni1", "Poni2": "poni2", "Rot1": "rot1", "Rot2": "rot2",
+             "Rot3": "rot3", "Wavelength": "wavelength"}
+
+    @classmethod
+    def load(cls, path: str) -> "Poni":
+        """Parse a v1 or v2 PONI file (Poni::load, src/poni.rs:79-137)."""
+        poni = cls()
+        with open(path) as f:
+            for line in f:
+                if line.lstrip().startswith("#") or ":" not in line:
+                    continue
+                key, value = (s.strip() for s in line.split(":", 1))
+                if key in cls._KEYS:
+                    setattr(poni, cls._KEYS[key], float(value))
+                elif key == "Detector_config":
+                    cfg = json.loads(value)
+                    if not isinstance(cfg, dict):
+                        raise ValueError("Detector_config must be a JSON object")
+                    for k in ("pixel1", "pixel2"):
+                        if cfg.get(k) is not None:
+                            setattr(poni, k, float(cfg[k]))
+        if poni.pixel1 == 0.0 or poni.pixel2 == 0.0:
+            raise ValueError(f"{path}: missing pixel sizes (pixel1/pixel2) in PONI file")
+        return poni
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "Poni":
+        return cls(**{k: float(d.get(k, 0.0)) for k in (
+            "pixel1", "pixel2", "distance", "poni1", "poni2", "rot1", "rot2", "rot3",
+            "wavelength")})
+
+    def _c(self) -> N.Geometry:
+        g = N.Geometry()
+        for k in ("pixel1", "pixel2", "distance", "poni1", "poni2", "rot1", "rot2", "rot3",
+                  "wavelength"):
+            setattr(g, k, float(getattr(self, k)))
+        return g
+
+
+class IntegrationResult:
+    """One integrated pattern (src/python/results.rs); lists like the
+    reference, with ``*_array`` NumPy views."""
+
+    def __init__(self, radial, intensity, errors=None, azimuthal_std=None, azimuthal=None,
+                 n_radial=None, n_azimuthal=None):
+        self.radial_array = None if radial is None else np.asarray(radial)
+        self.intensity_array = np.asarray(intensity)
+        self.errors_array = None if errors is None else np.asarray(errors)
+        self.azimuthal_std_array = None if azimuthal_std is None else np.asarray(azimuthal_std)
+        self.azimuthal_array = None if azimuthal is None else np.asarray(azimuthal)
+        self.n_radial = n_radial
+        self.n_azimuthal = n_azimuthal
+
+    radial = property(lambda s: None if s.radial_array is None else s.radial_array.tolist())
+    intensity = property(lambda s: s.intensity_array.tolist())
+    errors = property(lambda s: None if s.errors_array is None else s.errors_array.tolist())
+    azimuthal_std = property(
+        lambda s: None if s.azimuthal_std_array is None else s.azimuthal_std_array.tolist())
+    azimuthal = property(
+        lambda s: None if s.azimuthal_array is None else s.azimuthal_array.tolist())
+
+
+class BatchResult:
+    """One batch item (dioptrin.pyi:243-275)."""
+
+    def __init__(self, filename: str, result: Optional[IntegrationResult] = None,
+                 error: Optional[str] = None):
+        self.filename = filename
+        self.result = result
+        self.error = error
+
+    def is_ok(self) -> bool:
+        return self.error is None
+
+    def is_err(self) -> bool:
+        return self.error is not None
+
+
+def _frame_array(image) -> np.ndarray:
+    if isinstance(image, (str, bytes, os.PathLike)):
+        raise TypeError("file inputs are decoded by the caller; pass a 2D NumPy array")
+    a = np.asarray(image)
+    if a.dtype not in _DTYPES:
+        raise TypeError(f"unsupported dtype {a.dtype}; expected float64, float32, uint16, "
+                        "uint32 or int32")
+    if a.ndim != 2 or a.size == 0:
+        raise ValueError("image must be a non-empty 2D array")
+    if not a.flags.c_contiguous:
+        raise ValueError("image must be C-contiguous")
+    return a
+
+
+class Cuda1dPlan:
+    """A fixed-mask table resident in HBM (src/integration/cuda.rs:374-618).
+
+    Created by ``Integrator.prepare_cuda1d``. Calls on one plan are serialised
+    (a lock in the library); separate plans may run concurrently. The plan is
+    a snapshot: later changes to the Integrator do not affect it."""
+
+    def __init__(self, handle, shape, n_points, precision, device, n_azimuthal=0):
+        self._h = handle
+        self.shape = tuple(shape)
+        self.n_points = n_points
+        self.n_azimuthal = n_azimuthal
+        self.precision = precision
+        self.device = device
+        info = self.info()
+        self.table_entries = info.table_entries
+        self.max_batch_frames = info.max_batch_frames
+        rad = np.empty(n_points)
+        N.check(N.lib().dg_plan_radial(self._h, _dp(rad), n_points))
+        self._radial = rad
+        dev = N.DeviceInfo()
+        N.check(N.lib().dg_device_info_get(device, C.byref(dev)))
+        self.device_name = dev.name.decode()
+
+    @property
+    def radial(self) -> list:
+        return self._radial.tolist()
+
+    @property
+    def radial_array(self) -> np.ndarray:
+        return self._radial
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> N.PlanInfo:
+        info = N.PlanInfo()
+        N.check(N.lib().dg_plan_query(self._h, C.byref(info)))
+        return info
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            N.lib().dg_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def export_table(self, which: int = 0):
+        """(row_ptr, col, weight, denominator) of the masked (0) or unmasked
+        (1, needs keep_tables) table, for parity checks."""
+        info = self.info()
+        nnz = info.table_entries if which == 0 else info.full_entries
+        nb = self.n_points * max(1, self.n_azimuthal)
+        rp = np.empty(nb + 1, np.int64)
+        col = np.empty(max(nnz, 1), np.int32)
+        w = np.empty(max(nnz, 1))
+        den = np.empty(nb) if which == 0 else None
+        N.check(N.lib().dg_plan_export_table(
+            self._h, which, rp.ctypes.data_as(C.POINTER(C.c_int64)),
+            col.ctypes.data_as(C.POINTER(C.c_int32)), _dp(w), _dp(den)))
+        return rp, col[:nnz], w[:nnz], den
+
+    def integrate_stack(self, stack: np.ndarray, errors: bool = False,
+                        azimuthal_std: bool = False):
+        """Integrate (n, dim1, dim2) frames; returns (I, sigma, std) arrays of
+        shape (n, n_bins), sigma/std None when not requested."""
+        stack = np.ascontiguousarray(stack)
+        if stack.dtype not in _DTYPES:
+            raise TypeError(f"unsupported dtype {stack.dtype}")
+        if stack.ndim == 2:
+            stack = stack[None]
+        if tuple(stack.shape[1:]) != self.shape:
+            raise ValueError(f"frames of shape {stack.shape[1:]} do not match plan {self.shape}")
+        n = stack.shape[0]
+        nb = self.n_points * max(1, self.n_azimuthal)
+        flags = (N.DG_ERRORS if errors else 0) | (N.DG_AZIMUTHAL_STD if azimuthal_std else 0)
+        oi = np.empty((n, nb))
+        os_ = np.empty((n, nb)) if errors else None
+        od = np.empty((n, nb)) if azimuthal_std else None
+        N.check(N.lib().dg_integrate(self._h, stack.ctypes.data, _DTYPES[stack.dtype], n, flags,
+                                     _dp(oi), _dp(os_), _dp(od)))
+        return oi, os_, od
+
+    def integrate1d(self, image: np.ndarray, *, errors: bool = False,
+                    azimuthal_std: bool = False) -> IntegrationResult:
+        a = _frame_array(image)
+        i, s, d = self.integrate_stack(a, errors, azimuthal_std)
+        return IntegrationResult(self._radial, i[0], None if s is None else s[0],
+                                 None if d is None else d[0])
+
+    def batch1d(self, images, *, errors: bool = False,
+                azimuthal_std: bool = False) -> list:
+        if isinstance(images, np.ndarray) and images.ndim == 3:
+            stack = images
+        else:
+            arrays = [_frame_array(a) for a in images]
+            if not arrays:
+                return []
+            if len({a.dtype for a in arrays}) > 1:
+                raise TypeError("all images of one call must have the same dtype")
+            stack = np.stack(arrays)
+        i, s, d = self.integrate_stack(stack, errors, azimuthal_std)
+        return [IntegrationResult(self._radial, i[k], None if s is None else s[k],
+                                  None if d is None else d[k]) for k in range(len(i))]
+
+
+class BatchIterator(Iterator[BatchResult]):
+    """Streaming results in input order (src/batch/bounded.rs:172-420,
+    dioptrin.pyi:277-335): frames are gathered into device batches of up to
+    ``read_ahead`` as they arrive from the source."""
+
+    def __init__(self, integrator: "Integrator", images, n_points: int, errors: bool,
+                 azimuthal_std: bool, read_ahead: int = 32):
+        self._it = iter(images)
+        self._int = integrator
+        self._n = n_points
+        self._errors = errors
+        self._std = azimuthal_std
+        self._read_ahead = max(1, read_ahead)
+        self._pending: list = []
+        self.total = len(images) if hasattr(images, "__len__") else 0
+        self.completed = 0
+        self._index = 0
+        self._error: Optional[BaseException] = None
+
+    @property
+    def progress(self) -> Optional[float]:
+        return None if not self.total else self.completed / self.total
+
+    def __iter__(self) -> "BatchIterator":
+        return self
+
+    def _refill(self) -> None:
+        frames = []
+        while len(frames) < self._read_ahead:
+            try:
+                item = next(self._it)
+            except StopIteration:
+                break
+            except BaseException as e:  # surfaced at this item's position
+                self._error = e
+                break
+            frames.append(_frame_array(item))
+        if frames:
+            names = [f"array_{self._index + k}" for k in range(len(frames))]
+            self._index += len(frames)
+            results = self._int._batch_arrays(frames, self._n, self._errors, self._std)
+            self._pending.extend(BatchResult(n, r) for n, r in zip(names, results))
+
+    def __next__(self) -> BatchResult:
+        if not self._pending and self._error is None:
+            self._refill()
+        if self._pending:
+            self.completed += 1
+            return self._pending.pop(0)
+        if self._error is not None:
+            e, self._error = self._error, None
+            raise e
+        raise StopIteration
+
+
+class Integrator:
+    """Azimuthal integrator (src/integration.rs:278-573; Python class
+    src/python/integrator.rs:186). Integration runs on one CUDA device through
+    device-resident plans cached per image shape and bin count."""
+
+    def __init__(self, poni_path: Optional[str] = None, method: Optional[str] = None,
+                 polarization_factor: Optional[float] = None, n_ss: Optional[int] = None,
+                 unit: Optional[str] = None, radial_range=None, *, fast_math: bool = True,
+                 mask_mode: str = "fixed", sparse_layout: str = "csc", device: int = 0,
+                 precision: str = "f32_compensated", poni: Optional[Poni] = None):
+        self.poni = poni if poni is not None else Poni.load(poni_path)
+        self._method = "pixel_split"
+        self._n_ss = 5
+        self.set_method(method or "pixel_split", n_ss)
+        self._pol = None
+        self.set_polarization_factor(polarization_factor)
+        self._unit = "2th_rad"
+        self.set_unit(unit or "2th_rad")
+        self._radial_range = None
+        if radial_range is not None:
+            lo, hi = (float(v) for v in radial_range)
+            if not (np.isfinite(lo) and np.isfinite(hi) and lo < hi):
+                raise ValueError("radial_range must be finite with min < max")
+            self._radial_range = (lo, hi)
+        if mask_mode not in ("fixed", "dynamic"):
+            raise ValueError("mask_mode must be 'fixed' or 'dynamic'")
+        if mask_mode != "fixed":
+            raise ValueError("the device integrator requires mask_mode fixed")
+        if sparse_layout not in ("csc", "csr"):
+            raise ValueError("sparse_layout must be 'csc' or 'csr'")
+        if precision not in N.PRECISIONS:
+            raise ValueError(f"unknown CUDA precision {precision!r}; expected \"f32\", "
+                             "\"f32_compensated\" or \"f64\"")
+        self.fast_math = fast_math  # accepted for compatibility; the device order is fixed
+        self.mask_mode = mask_mode
+        self.sparse_layout = sparse_layout
+        self.device = device
+        self.precision = precision
+        self._mask: Optional[np.ndarray] = None
+        self._plans: dict = {}
+        self._lock = threading.Lock()
+
+    @classmethod
+    def from_poni_dict(cls, poni_dict: dict, method=None, polarization_factor=None, n_ss=None,
+                       unit=None, radial_range=None, **kw) -> "Integrator":
+        return cls(None, method, polarization_factor, n_ss, unit, radial_range,
+                   poni=Poni.from_dict(poni_dict), **kw)
+
+    # -- configuration (src/integration.rs:319-510) --
+    def set_method(self, method: str, n_ss: Optional[int] = None) -> None:
+        if method not in N.METHODS:
+            raise ValueError(f"unknown method {method!r}")
+        if n_ss is not None and n_ss <= 0:
+            raise ValueError("n_ss must be positive")
+        self._method = method
+        if n_ss is not None:
+            self._n_ss = int(n_ss)
+        self._invalidate()
+
+    @property
+    def method(self) -> str:
+        return self._method
+
+    def set_polarization_factor(self, factor: Optional[float]) -> None:
+        if factor is not None and not (-1.0 <= factor <= 1.0):
+            raise ValueError("polarization_factor must lie in [-1, 1]")
+        self._pol = None if factor is None else float(factor)
+        self._invalidate()
+
+    def set_unit(self, unit: str) -> None:
+        if unit not in N.UNITS:
+            raise ValueError(f"unknown unit {unit!r}")
+        if unit.startswith("q") and not self.poni.wavelength > 0:
+            raise ValueError("a q unit needs a positive PONI wavelength")
+        self._unit = unit
+        self._invalidate()
+
+    def get_unit(self) -> str:
+        return self._unit
+
+    def set_radial_range(self, radial_range) -> None:
+        self._radial_range = None if radial_range is None else tuple(map(float, radial_range))
+        self._invalidate()
+
+    def set_mask(self, mask: Optional[np.ndarray]) -> None:
+        if mask is None:
+            self.clear_mask()
+            return
+        if isinstance(mask, (str, bytes, os.PathLike)):
+            raise TypeError("mask files are decoded by the caller; pass a 2D array")
+        m = np.ascontiguousarray(np.asarray(mask) != 0, np.uint8)
+        if m.ndim != 2:
+            raise ValueError("mask must be 2D")
+        self._mask = m
+        self._invalidate()
+
+    def clear_mask(self) -> None:
+        self._mask = None
+        self._invalidate()
+
+    def _invalidate(self) -> None:
+        plans = getattr(self, "_plans", None)
+        if plans:
+            for p in plans.values():
+                p.close()
+            plans.clear()
+
+    # -- plans --
+    def _method_struct(self, precision: str, device: int, max_batch_bytes: int,
+                       keep_tables: bool) -> N.Method:
+        m = N.Method()
+        m.kind = N.METHODS[self._method]
+        m.n_ss = self._n_ss
+        m.unit = N.UNITS[self._unit]
+        m.has_polarization = 0 if self._pol is None else 1
+        m.polarization_factor = 0.0 if self._pol is None else self._pol
+        m.has_radial_range = 0 if self._radial_range is None else 1
+        if self._radial_range is not None:
+            m.radial_min, m.radial_max = self._radial_range
+        m.precision = N.PRECISIONS[precision]
+        m.device = device
+        m.max_batch_bytes = max_batch_bytes
+        m.flags = N.DG_PLAN_KEEP_TABLES if keep_tables else 0
+        return m
+
+    def prepare_cuda1d(self, shape, n_points: int, *, precision: str = "f32_compensated",
+                       device: int = 0, max_batch_bytes: Optional[int] = None,
+                       keep_tables: bool = False) -> Cuda1dPlan:
+        """Integrator::prepare_cuda1d (src/integration/cuda.rs:1089): the
+        table is built on the device and kept there."""
+        if precision not in N.PRECISIONS:
+            raise ValueError(f"unknown CUDA precision {precision!r}")
+        if device < 0:
+            raise OverflowError("device must be non-negative")
+        dim1, dim2 = (int(v) for v in shape)
+        if max_batch_bytes is not None and max_batch_bytes <= 0:
+            raise ValueError("max_batch_bytes must be positive")
+        if self._mask is not None and self._mask.shape != (dim1, dim2):
+            raise ValueError(f"image shape ({dim1}, {dim2}) does not match mask shape "
+                             f"{self._mask.shape}")
+        m = self._method_struct(precision, device, max_batch_bytes or 0, keep_tables)
+        h = C.c_void_p()
+        mask = (None if self._mask is None
+                else self._mask.ctypes.data_as(C.POINTER(C.c_uint8)))
+        N.check(N.lib().dg_plan_create(C.byref(self.poni._c()), C.byref(m), mask, dim1, dim2,
+                                       int(n_points), 0, None, C.byref(h)))
+        return Cuda1dPlan(h, (dim1, dim2), int(n_points), precision, device)
+
+    def _plan(self, shape, n_points: int) -> Cuda1dPlan:
+        key = (tuple(shape), int(n_points))
+        with self._lock:
+            p = self._plans.get(key)
+            if p is None:
+                p = self.prepare_cuda1d(shape, n_points, precision=self.precision,
+                                        device=self.device)
+                self._plans[key] = p
+            return p
+
+    # -- integration (src/integration/methods.rs) --
+    def integrate1d(self, image, n_points: int, errors: bool = False, *,
+                    azimuthal_std: bool = False) -> IntegrationResult:
+        if n_points <= 0:
+            raise ValueError("n_points must be positive")
+        a = _frame_array(image)
+        return self._plan(a.shape, n_points).integrate1d(a, errors=errors,
+                                                         azimuthal_std=azimuthal_std)
+
+    def integrate1d_with_errors(self, image, n_points: int) -> IntegrationResult:
+        return self.integrate1d(image, n_points, True)
+
+    def integrate1d_with_azimuthal_std(self, image, n_points: int,
+                                       errors: bool = False) -> IntegrationResult:
+        return self.integrate1d(image, n_points, errors, azimuthal_std=True)
+
+    def _batch_arrays(self, arrays: Sequence[np.ndarray], n_points: int, errors: bool,
+                      azimuthal_std: bool) -> list:
+        out: list = [None] * len(arrays)
+        groups: dict = {}
+        for k, a in enumerate(arrays):
+            groups.setdefault((a.shape, a.dtype), []).append(k)
+        for (shape, _), idx in groups.items():
+            plan = self._plan(shape, n_points)
+            res = plan.batch1d(np.stack([arrays[k] for k in idx]), errors=errors,
+                               azimuthal_std=azimuthal_std)
+            for k, r in zip(idx, res):
+                out[k] = r
+        return out
+
+    def batch1d(self, images, n_points: int, errors: bool = False,
+                num_workers: Optional[int] = None, num_threads: Optional[int] = None, *,
+                azimuthal_std: bool = False) -> list:
+        """Integrator.batch1d (src/python/integrator.rs:1867): arrays are
+        integrated as device batches; results keep the input order."""
+        if isinstance(images, (str, bytes, os.PathLike)):
+            raise TypeError("images must be a list; wrap one path in a list")
+        if n_points <= 0:
+            raise ValueError("n_points must be positive")
+        arrays = [_frame_array(a) for a in images]
+        results = self._batch_arrays(arrays, n_points, errors, azimuthal_std)
+        return [BatchResult(f"array_{k}", r) for k, r in enumerate(results)]
+
+    def batch1d_iter(self, images, n_points: int, errors: bool = False,
+                     num_workers: Optional[int] = None, num_threads: Optional[int] = None, *,
+                     azimuthal_std: bool = False) -> BatchIterator:
+        """Integrator.batch1d_iter (src/python/integrator.rs:2211)."""
+        if isinstance(images, (str, bytes, os.PathLike)):
+            raise TypeError("images must be a list or iterable; wrap one path in a list")
+        if n_points <= 0:
+            raise ValueError("n_points must be positive")
+        if isinstance(images, list):
+            for a in images:
+                _frame_array(a)
+        return BatchIterator(self, images, n_points, errors, azimuthal_std,
+                             read_ahead=num_workers or 32)
+
+
+def cuda_info(device: int = 0) -> dict:
+    """cuda_info (src/integration/cuda.rs:262-329) as a dict."""
+    try:
+        info = N.DeviceInfo()
+        st = N.lib().dg_device_info_get(device, C.byref(info))
+    except CudaUnavailableError as e:
+        return {"compiled": False, "available": False, "reason": str(e), "device": device}
+    if st != N.DG_OK:
+        return {"compiled": True, "available": False, "reason": N.last_error(), "device": device}
+    return {"compiled": True, "available": True, "reason": None, "device": device,
+            "device_name": info.name.decode(), "compute_capability": (info.cc_major,
+                                                                      info.cc_minor),
+            "sm_count": info.sm_count, "total_memory_bytes": info.total_memory_bytes,
+            "driver_version": info.driver_version}
+
+
+def cuda_available(device: int = 0) -> bool:
+    return bool(cuda_info(device).get("available"))

@@ -1,0 +1,75 @@
+"""Python handle on the library's request loop (dg_server_* in
+include/dioptrin_gpu.h): continuous batching of single-frame requests over
+device-resident plans held in an HBM cache bounded by bytes."""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from .integrator import _DTYPES, Integrator, _dp
+
+
+class RequestLoop:
+    def __init__(self, device: int = 0, cache_bytes: int = 60 << 30,
+                 max_inflight_frames: int = 512, max_coalesce: int = 64, poll_us: int = 100):
+        cfg = N.ServerConfig(device, max_inflight_frames, cache_bytes, max_coalesce, poll_us)
+        self._h = C.c_void_p()
+        N.check(N.lib().dg_server_create(C.byref(cfg), C.byref(self._h)))
+        self._bins: dict = {}
+        self._shapes: dict = {}
+
+    def register(self, key: int, integrator: Integrator, shape, n_points: int,
+                 precision: str = "f32_compensated") -> None:
+        """Registers (or re-registers, after a PONI change) a plan under key."""
+        dim1, dim2 = shape
+        m = integrator._method_struct(precision, 0, 0, False)
+        mask = (None if integrator._mask is None
+                else integrator._mask.ctypes.data_as(C.POINTER(C.c_uint8)))
+        N.check(N.lib().dg_server_register(self._h, key, C.byref(integrator.poni._c()),
+                                           C.byref(m), mask, dim1, dim2, n_points, 0, None))
+        self._bins[key] = n_points
+        self._shapes[key] = (dim1, dim2)
+
+    def submit(self, key: int, frame: np.ndarray, errors: bool = False,
+               azimuthal_std: bool = False, wait_ms: int = 10000) -> int:
+        a = np.ascontiguousarray(frame)
+        if a.dtype not in _DTYPES:
+            raise TypeError(f"unsupported dtype {a.dtype}")
+        if a.shape != self._shapes[key]:
+            raise ValueError("frame shape does not match the registered plan")
+        flags = (N.DG_ERRORS if errors else 0) | (N.DG_AZIMUTHAL_STD if azimuthal_std else 0)
+        t = C.c_uint64()
+        N.check(N.lib().dg_server_submit(self._h, key, a.ctypes.data, _DTYPES[a.dtype], flags,
+                                         wait_ms, C.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int, key: int, errors: bool = False, azimuthal_std: bool = False,
+             wait_ms: int = 10000):
+        """Returns (intensity, sigma, std, latency_us) for a ticket."""
+        nb = self._bins[key]
+        oi = np.empty(nb)
+        os_ = np.empty(nb) if errors else None
+        od = np.empty(nb) if azimuthal_std else None
+        lat = C.c_double()
+        N.check(N.lib().dg_server_poll(self._h, ticket, wait_ms, _dp(oi), _dp(os_), _dp(od),
+                                       C.byref(lat)))
+        return oi, os_, od, lat.value
+
+    def stats(self) -> dict:
+        s = N.ServerStats()
+        N.check(N.lib().dg_server_stats_get(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in N.ServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            N.lib().dg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,223 @@
+/*
+ * dioptrin_gpu.h — C ABI of the B200 lookup-table integration library.
+ *
+ * Plain pointers and sizes only. A plan is the device-resident snapshot of
+ * one integrator configuration (geometry, method, unit, radial range,
+ * polarisation, mask) for one image shape and bin count: its CSR table is
+ * built on the GPU and kept in HBM until the plan is destroyed.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths are inside the reference crate, CPrescher/Dioptrin v0.20.1).
+ */
+#ifndef DIOPTRIN_GPU_H
+#define DIOPTRIN_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DG_EXPORT __attribute__((visibility("default")))
+#else
+#define DG_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: the five CudaError variants (src/integration/cuda.rs:218-237)
+ * plus a timeout for the request loop's bounded waits. */
+typedef enum dg_status {
+    DG_OK = 0,
+    DG_NOT_COMPILED = 1, /* CudaError::NotCompiled */
+    DG_UNAVAILABLE = 2,  /* CudaError::Unavailable: no device / no such ordinal */
+    DG_UNSUPPORTED = 3,  /* CudaError::Unsupported: method, mask mode, table size */
+    DG_INVALID_INPUT = 4,/* CudaError::InvalidInput: shapes, sizes, budgets */
+    DG_DEVICE = 5,       /* CudaError::Device: driver error, out of memory */
+    DG_TIMEOUT = 6       /* a bounded wait expired (request loop, device spin) */
+} dg_status;
+
+/* IntegrationMethod (src/integration.rs:222-236). */
+enum {
+    DG_METHOD_COUNTING = 0,
+    DG_METHOD_PIXEL_SPLIT = 1,
+    DG_METHOD_PYFAI_FULL = 2,
+    DG_METHOD_SUPERSAMPLED = 3
+};
+
+/* RadialUnit (src/integration.rs:115-128). */
+enum { DG_UNIT_TTH_RAD = 0, DG_UNIT_TTH_DEG = 1, DG_UNIT_Q_A = 2, DG_UNIT_Q_NM = 3 };
+
+/* Pixel types a plan accepts (CudaPixel, src/integration/cuda.rs:354-367). */
+enum { DG_U16 = 0, DG_U32 = 1, DG_I32 = 2, DG_F32 = 3, DG_F64 = 4 };
+
+/* CudaPrecision (src/integration/cuda.rs:64-73). Weights are stored in FP32
+ * in every mode; F32_COMPENSATED accumulates with double-word FP32 sums, F64
+ * accumulates in FP64. */
+enum { DG_PRECISION_F32 = 0, DG_PRECISION_F32_COMPENSATED = 1, DG_PRECISION_F64 = 2 };
+
+/* Integration flags. */
+#define DG_ERRORS 1u        /* propagated Poisson sigma (integrate1d_with_errors) */
+#define DG_AZIMUTHAL_STD 2u /* weighted population spread (integrate1d_with_azimuthal_std) */
+
+/* Plan-creation flags. */
+#define DG_PLAN_KEEP_TABLES 1u /* keep the unmasked f64 CSR for dg_plan_export_table */
+
+/* Poni (src/poni.rs:13-24); SI units, angles in radians. */
+typedef struct dg_geometry {
+    double pixel1, pixel2, distance, poni1, poni2, rot1, rot2, rot3, wavelength;
+} dg_geometry;
+
+/* Integrator configuration captured by a plan (src/integration.rs:278-297,
+ * Cuda1dOptions src/integration/cuda.rs:118-211). */
+typedef struct dg_method {
+    int32_t kind;              /* DG_METHOD_* */
+    int32_t n_ss;              /* subpixels per side for DG_METHOD_SUPERSAMPLED */
+    int32_t unit;              /* DG_UNIT_* */
+    int32_t has_polarization;  /* with_polarization_factor was called */
+    double polarization_factor;
+    int32_t has_radial_range;  /* with_radial_range */
+    double radial_min, radial_max;
+    int32_t precision;         /* DG_PRECISION_* */
+    int32_t device;            /* CUDA ordinal */
+    int64_t max_batch_bytes;   /* chunk budget for host-memory calls; 0 = automatic */
+    uint32_t flags;            /* DG_PLAN_* */
+} dg_method;
+
+typedef struct dg_plan dg_plan;
+
+/* Replaces Integrator::prepare_cuda1d (src/integration/cuda.rs:1089-1103) and
+ * prepare_cuda2d (:1111-1157). n_azimuthal == 0 selects 1D. azimuthal_range is
+ * NULL or two doubles (radians). mask is NULL or dim1*dim2 bytes, nonzero =
+ * masked (src/mask.rs:4-9). Checks run in the reference's order
+ * (src/integration/cuda.rs:1071-1088): configuration, shape, device, build. */
+DG_EXPORT dg_status dg_plan_create(const dg_geometry *geometry, const dg_method *method,
+                         const uint8_t *mask, int32_t dim1, int32_t dim2, int32_t n_radial,
+                         int32_t n_azimuthal, const double *azimuthal_range, dg_plan **out);
+
+/* Replaces Drop for Cuda1dPlan (src/integration/cuda.rs:374-386). NULL is a no-op. */
+DG_EXPORT dg_status dg_plan_destroy(dg_plan *plan);
+
+typedef struct dg_plan_info {
+    int32_t dim1, dim2, n_radial, n_azimuthal;
+    int64_t table_entries;   /* Cuda1dPlan::table_entries (masked table) */
+    int64_t full_entries;    /* entries before mask compaction */
+    int64_t max_batch_frames;/* Cuda1dPlan::max_batch_frames */
+    int32_t device, precision;
+    double hist_min, hist_step;
+    double build_ms;         /* device CSR build, event-timed */
+    int64_t device_bytes;    /* HBM held by the plan */
+    int64_t guard_corners;   /* corners within the FP64 guard band of a bin edge */
+    int64_t singular_pixels; /* pixels integrated by detector-plane sampling */
+} dg_plan_info;
+
+/* Replaces Cuda1dPlan::{shape, n_points, table_entries, max_batch_frames,
+ * device} (src/integration/cuda.rs:420-470). */
+DG_EXPORT dg_status dg_plan_query(const dg_plan *plan, dg_plan_info *out);
+
+/* Radial (and for 2D azimuthal) bin centres; Cuda1dPlan::radial
+ * (src/integration/cuda.rs:455-460). n must equal the bin count. */
+DG_EXPORT dg_status dg_plan_radial(const dg_plan *plan, double *out, int64_t n);
+DG_EXPORT dg_status dg_plan_azimuthal(const dg_plan *plan, double *out, int64_t n);
+
+/* Copies a table to host memory for parity checks. which = 0: the masked
+ * table the gather uses (fixed_csr_parts, src/lut/prepared.rs:194-202), with
+ * its f64 denominators; which = 1: the unmasked table (needs
+ * DG_PLAN_KEEP_TABLES). row_ptr has n_bins+1 entries, col/weight
+ * *_entries; any pointer may be NULL to skip it. weight is the f64 weight the
+ * builder produced (1.0 for counting tables). */
+DG_EXPORT dg_status dg_plan_export_table(const dg_plan *plan, int32_t which, int64_t *row_ptr,
+                               int32_t *col, double *weight, double *denominator);
+
+/* Replaces Cuda1dPlan::integrate_frames / integrate_stack
+ * (src/integration/cuda.rs:499-564) and Cuda2dPlan::integrate_*_into
+ * (:770-863): n_frames row-major frames stacked in HOST memory, results to
+ * HOST arrays of n_frames * n_bins doubles (out_sigma needs DG_ERRORS,
+ * out_std DG_AZIMUTHAL_STD; pass NULL otherwise). Frames are copied to the
+ * device in chunks of at most max_batch_frames. Results do not depend on how
+ * frames are chunked or batched. */
+DG_EXPORT dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                       uint32_t flags, double *out_intensity, double *out_sigma,
+                       double *out_std);
+
+/* Same with frames and results already in DEVICE memory of the plan's GPU,
+ * enqueued on `stream` (a cudaStream_t; NULL = the plan's own stream). No
+ * synchronisation: the caller owns completion. */
+DG_EXPORT dg_status dg_integrate_device(dg_plan *plan, const void *d_frames, int32_t dtype,
+                              int64_t n_frames, uint32_t flags, double *d_intensity,
+                              double *d_sigma, double *d_std, void *stream);
+
+/* One-frame-per-launch form of dg_integrate_device: one gather launch per
+ * frame, the table re-read for every frame. The plain GPU path the batched
+ * kernel is measured against. */
+DG_EXPORT dg_status dg_integrate_device_plain(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                    int64_t n_frames, uint32_t flags, double *d_intensity,
+                                    double *d_sigma, double *d_std, void *stream);
+
+/* Kernel timing for roofline reports; the reference times its CUDA phases
+ * with events in src/integration/cuda/bench.rs:139-196. With enable != 0,
+ * every gather-kernel launch of the plan is bracketed by CUDA events on the
+ * stream it runs on. dg_plan_kernel_time waits for the last recorded event and
+ * returns the summed gather-kernel time, the number of gather launches and the
+ * number of all kernel launches since the last reset. */
+DG_EXPORT dg_status dg_plan_profile(dg_plan *plan, int32_t enable);
+DG_EXPORT dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *gather_ms,
+                                        int64_t *gather_launches, int64_t *launches);
+
+/* Request loop (continuous batching across plans). Replaces the reference's
+ * bounded streaming executor (src/batch/bounded.rs:56-420) for device work:
+ * requests are admitted while slots and HBM allow, same-plan requests are
+ * coalesced into one launch, results come back through dg_server_poll. */
+typedef struct dg_server dg_server;
+
+typedef struct dg_server_config {
+    int32_t device;
+    int32_t max_inflight_frames; /* admission slots */
+    int64_t cache_bytes;         /* HBM budget of the plan cache */
+    int32_t max_coalesce;        /* most frames one launch takes */
+    int32_t poll_us;             /* worker idle wait */
+} dg_server_config;
+
+typedef struct dg_server_stats {
+    int64_t submitted, completed, failed, launches, coalesced_frames;
+    int64_t plan_builds, plan_hits, plan_evictions, cache_bytes;
+} dg_server_stats;
+
+DG_EXPORT dg_status dg_server_create(const dg_server_config *config, dg_server **out);
+DG_EXPORT dg_status dg_server_destroy(dg_server *server);
+/* Registers a plan configuration under `key` (built on first use, rebuilt
+ * when evicted). Replaces re-preparing a Cuda1dPlan per geometry. */
+DG_EXPORT dg_status dg_server_register(dg_server *server, uint64_t key, const dg_geometry *geometry,
+                             const dg_method *method, const uint8_t *mask, int32_t dim1,
+                             int32_t dim2, int32_t n_radial, int32_t n_azimuthal,
+                             const double *azimuthal_range);
+/* Queues one frame (host memory, copied before return) for plan `key`;
+ * returns a ticket. DG_TIMEOUT if no slot frees within wait_ms. */
+DG_EXPORT dg_status dg_server_submit(dg_server *server, uint64_t key, const void *frame, int32_t dtype,
+                           uint32_t flags, int32_t wait_ms, uint64_t *ticket);
+/* Waits up to wait_ms for `ticket`; fills n_bins doubles per requested
+ * output and the request's latency in microseconds (submit to result). */
+DG_EXPORT dg_status dg_server_poll(dg_server *server, uint64_t ticket, int32_t wait_ms,
+                         double *out_intensity, double *out_sigma, double *out_std,
+                         double *latency_us);
+DG_EXPORT dg_status dg_server_stats_get(dg_server *server, dg_server_stats *out);
+
+/* Device description; cuda_info (src/integration/cuda.rs:262-329). */
+typedef struct dg_device_info {
+    int32_t available;
+    int32_t device;
+    int32_t cc_major, cc_minor;
+    int32_t sm_count;
+    int64_t total_memory_bytes;
+    int32_t driver_version;
+    char name[128];
+} dg_device_info;
+DG_EXPORT dg_status dg_device_info_get(int32_t device, dg_device_info *out);
+
+/* Message of the calling thread's last failed call; returns its length. */
+DG_EXPORT int32_t dg_last_error(char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -23,7 +23,8 @@ DG_PLAN_KEEP_TABLES = 1
 EXPORTS = [
     "dg_plan_create", "dg_plan_destroy", "dg_plan_query", "dg_plan_radial",
     "dg_plan_azimuthal", "dg_plan_export_table", "dg_integrate", "dg_integrate_device",
-    "dg_integrate_device_plain", "dg_plan_profile", "dg_plan_kernel_time", "dg_server_create", "dg_server_destroy",
+    "dg_integrate_device_plain", "dg_plan_profile", "dg_plan_kernel_time", "dg_eval_math",
+    "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
     "dg_device_info_get", "dg_last_error",
 ]
@@ -111,6 +112,7 @@ def lib():
                                          vp]
         L.dg_plan_profile.argtypes = [vp, C.c_int32]
         L.dg_plan_kernel_time.argtypes = [vp, C.c_int32, pd, P(C.c_int64), P(C.c_int64)]
+        L.dg_eval_math.argtypes = [C.c_int32, vp, vp, C.c_int64, vp]
         L.dg_server_create.argtypes = [P(ServerConfig), P(vp)]
         L.dg_server_destroy.argtypes = [vp]
         L.dg_server_register.argtypes = [vp, C.c_uint64, P(Geometry), P(Method), P(C.c_uint8),

@@ -434,6 +434,25 @@ dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *gather_ms,
     });
 }
 
+dg_status dg_eval_math(int32_t which, const double *d_a, const double *d_b, int64_t n,
+                       double *d_out) {
+    return guarded([&] {
+        if (n < 0) dg::fail(DG_INVALID_INPUT, "n must not be negative");
+        if (n > 0 && (!d_a || !d_out || ((which == 0 || which == 2) && !d_b)))
+            dg::fail(DG_INVALID_INPUT, "arrays must not be NULL");
+        cudaStream_t s = nullptr;
+        DG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        try {
+            dg::eval_math(which, d_a, d_b, n, d_out, s);
+            DG_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
+    });
+}
+
 dg_status dg_device_info_get(int32_t device, dg_device_info *out) {
     return guarded([&] {
         if (!out) dg::fail(DG_INVALID_INPUT, "out must not be NULL");

@@ -3,12 +3,14 @@
 // Compiled with -fmad=false: every a*b+c below is a separate multiply and
 // add, in C's left-to-right order, which is the order the reference's Rust
 // evaluates (Rust never contracts to FMA unless mul_add is written). Double
-// division and sqrt are IEEE round-to-nearest on the device; atan2/sin/cos are
-// CUDA's FP64 library functions (a few ulp from glibc), so corner values can
-// differ from the CPU reference in the last bits. Table indices depend on them
-// only through floor((r - min)/step) and the clip areas; the build counts the
-// corners that lie within a guard band of a bin edge (guard_corners) so a
-// build that could disagree with the CPU in an index is visible.
+// division and sqrt are IEEE round-to-nearest on the device, and atan2 and sin
+// are the correctly rounded double-double versions of dg_ddmath.cuh, so a
+// corner's 2-theta and chi are the bits the C library gives the reference
+// (cos, used only for the polarisation factor, is CUDA's). Table indices
+// depend on corners through floor((r - min)/step) and through clip areas,
+// whose shoelace sums amplify a last-bit change of a corner ~1e5-fold; the
+// build also counts the corners that lie within a guard band of a bin edge
+// (guard_corners), where any remaining difference could show.
 //
 // Every builder is count -> exclusive scan -> fill, first into a pixel-major
 // list of (pixel, bin, weight) contributions, then transposed into CSR rows by
@@ -22,6 +24,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "dg_ddmath.cuh"
 #include "dg_internal.h"
 
 namespace dg {
@@ -77,7 +80,7 @@ __device__ __forceinline__ double to_unit(const GeomParams &g, double tth) {
     switch (g.unit) {
     case DG_UNIT_TTH_DEG: return tth * (180.0 / kPi);
     case DG_UNIT_Q_A:
-    case DG_UNIT_Q_NM: return g.q_scale * sin(tth * 0.5);
+    case DG_UNIT_Q_NM: return g.q_scale * ddm::cr_sin(tth * 0.5);
     default: return tth;
     }
 }
@@ -88,8 +91,8 @@ __device__ __forceinline__ void radial_chi(const GeomParams &g, double d1, doubl
                                            double &chi) {
     double x, y, z;
     sample_xyz(g, d1 * g.pixel1 - g.poni1, d2 * g.pixel2 - g.poni2, x, y, z);
-    r = to_unit(g, atan2(sqrt(y * y + x * x), z));
-    chi = atan2(x, y);
+    r = to_unit(g, ddm::cr_atan2(sqrt(y * y + x * x), z));
+    chi = ddm::cr_atan2(x, y);
 }
 
 // Corner grid (geometry.rs:229-278): corner (i, j) at i * pixel - poni.
@@ -101,8 +104,8 @@ __global__ void k_corners(GeomParams g, int dim1, int dim2, double *__restrict__
         int64_t i = k / (dim2 + 1), j = k % (dim2 + 1);
         double x, y, z;
         sample_xyz(g, double(i) * g.pixel1 - g.poni1, double(j) * g.pixel2 - g.poni2, x, y, z);
-        rc[k] = to_unit(g, atan2(sqrt(y * y + x * x), z));
-        ac[k] = atan2(x, y);
+        rc[k] = to_unit(g, ddm::cr_atan2(sqrt(y * y + x * x), z));
+        ac[k] = ddm::cr_atan2(x, y);
     }
 }
 
@@ -119,8 +122,8 @@ __global__ void k_centres(GeomParams g, int dim1, int dim2, double *__restrict__
         double d2 = (double(j) + 0.5) * g.pixel2 - g.poni2;
         double x, y, z;
         sample_xyz(g, d1, d2, x, y, z);
-        double tth = atan2(sqrt(y * y + x * x), z);
-        double az = atan2(x, y);
+        double tth = ddm::cr_atan2(sqrt(y * y + x * x), z);
+        double az = ddm::cr_atan2(x, y);
         double cosa = g.distance / sqrt(d1 * d1 + d2 * d2 + g.distance * g.distance);
         double sa = cosa * (cosa * cosa);
         double pol = 1.0;
@@ -1058,6 +1061,34 @@ void compact_table(const DeviceCsr &full, const uint8_t *d_mask, int32_t n_pixel
 void denominators(const DeviceCsr &t, const double *d_norm, cudaStream_t s, double *d_den) {
     k_denominators<<<grid_for(t.n_rows, 128), 128, 0, s>>>(t.row_ptr.ptr, t.n_rows, t.col.ptr,
                                                            t.w.ptr, d_norm, d_den);
+    DG_CUDA(cudaGetLastError());
+}
+
+}  // namespace dg
+
+namespace dg {
+namespace {
+
+__global__ void k_eval_math(int which, const double *__restrict__ a, const double *__restrict__ b,
+                            int64_t n, double *__restrict__ out) {
+    for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n;
+         k += int64_t(gridDim.x) * blockDim.x) {
+        switch (which) {
+        case 0: out[k] = ddm::cr_atan2(a[k], b[k]); break;
+        case 1: out[k] = ddm::cr_sin(a[k]); break;
+        case 2: out[k] = atan2(a[k], b[k]); break;
+        default: out[k] = sin(a[k]); break;
+        }
+    }
+}
+
+}  // namespace
+
+void eval_math(int which, const double *a, const double *b, int64_t n, double *out,
+               cudaStream_t s) {
+    if (which < 0 || which > 3) fail(DG_INVALID_INPUT, "unknown function");
+    if (n <= 0) return;
+    k_eval_math<<<grid_for(n), 256, 0, s>>>(which, a, b, n, out);
     DG_CUDA(cudaGetLastError());
 }
 

@@ -111,6 +111,10 @@ void compact_table(const DeviceCsr &full, const uint8_t *d_mask, int32_t n_pixel
                    cudaStream_t stream, DeviceCsr &out);
 void denominators(const DeviceCsr &table, const double *d_norm, cudaStream_t stream,
                   double *d_den);
+// Device FP64 primitives on arrays: 0 correctly rounded atan2(a, b), 1 its
+// sin(a), 2 CUDA atan2, 3 CUDA sin.
+void eval_math(int which, const double *a, const double *b, int64_t n, double *out,
+               cudaStream_t stream);
 
 // Gather-side table: packed entries + row segments (dg_gather.cu).
 struct GatherTable {

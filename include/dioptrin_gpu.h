@@ -164,6 +164,15 @@ DG_EXPORT dg_status dg_plan_profile(dg_plan *plan, int32_t enable);
 DG_EXPORT dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *gather_ms,
                                         int64_t *gather_launches, int64_t *launches);
 
+/* Evaluates one FP64 primitive of the device table builders on n values in
+ * DEVICE memory of the current device, for parity checks against the C
+ * library the reference calls (f64::atan2 and f64::sin, geometry.rs:684-692,
+ * integration.rs:167): which = 0 the builders' correctly rounded atan2(a, b),
+ * 1 their correctly rounded sin(a), 2 CUDA's atan2, 3 CUDA's sin. b is unused
+ * for sin. Synchronous. */
+DG_EXPORT dg_status dg_eval_math(int32_t which, const double *d_a, const double *d_b,
+                                 int64_t n, double *d_out);
+
 /* Request loop (continuous batching across plans). Replaces the reference's
  * bounded streaming executor (src/batch/bounded.rs:56-420) for device work:
  * requests are admitted while slots and HBM allow, same-plan requests are

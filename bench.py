@@ -208,7 +208,10 @@ def main():
     od = torch.empty_like(oi)
     flags = (N.DG_ERRORS if w.errors else 0) | (N.DG_AZIMUTHAL_STD if w.azimuthal_std else 0)
     dtype_code = {"uint16": 0, "uint32": 1, "int32": 2, "float32": 3, "float64": 4}[w.dtype]
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: its handle is what the library launches on, so the
+    # CUDA events below bracket exactly the library's kernels.
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
 
     def step(fn=L.dg_integrate_device, nf=n_frames):
         N.check(fn(plan.handle, C.c_void_p(frames.data_ptr()), dtype_code, nf, flags,

@@ -31,6 +31,11 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// Detector rows per gather strip (see dg_gather.cu): small enough that a
+// unit's bins cover a few kilobytes of each frame, large enough that a bin's
+// ring is cut into few segments.
+constexpr int32_t kStripRows = 128;
+
 }  // namespace
 
 void dg::set_last_error(const std::string &message) { g_last_error = message; }
@@ -154,8 +159,10 @@ int64_t dg_plan::device_bytes() const {
     b += full.row_ptr.bytes() + full.col.bytes() + full.w.bytes();
     b += table.row_ptr.bytes() + table.col.bytes() + table.w.bytes();
     b += norm.bytes();
-    b += gather.seg.bytes() + gather.row_seg.bytes() + gather.entry.bytes() +
+    b += gather.seg.bytes() + gather.unit.bytes() + gather.row_seg.bytes() +
+         gather.seg_ids.bytes() + gather.first_valid.bytes() + gather.entry.bytes() +
          gather.entry_std.bytes() + gather.den.bytes() + gather.den_std.bytes() +
+         gather.den_f32.bytes() +
          gather.valid_std.bytes() + gather.partial.bytes();
     b += stage_in.bytes() + stage_out.bytes();
     return b;
@@ -200,7 +207,8 @@ dg_status dg_plan_create(const dg_geometry *geometry, const dg_method *method,
                 DG_CUDA(cudaMemcpyAsync(d_mask.ptr, mask, size_t(npix), cudaMemcpyHostToDevice, s));
             }
             dg::compact_table(built.full, any ? d_mask.ptr : nullptr, int32_t(npix), s, plan->table);
-            dg::make_gather_table(plan->table, built.norm.ptr, 2048, s, plan->gather);
+            dg::make_gather_table(plan->table, built.norm.ptr, dim1, dim2, kStripRows, s,
+                                  plan->gather);
             DG_CUDA(cudaEventRecord(e1, s));
             DG_CUDA(cudaEventSynchronize(e1));
             float ms = 0;

@@ -1,19 +1,27 @@
 // Per-frame gather: CSR (bins x pixels) times a stack of frames.
 //
-// Layout. The masked table is cut into row segments of at most `seg_len`
-// entries (a row never shares a segment with another row). One CTA owns one
-// segment: it stages the segment's packed entries in shared memory once and
-// then sweeps every frame of the call over them, so the table crosses HBM
-// once per call however many frames there are. Warps take frames four at a
-// time; a lane reads one staged entry (col, weight[, norm, weight/norm]) and
-// applies it to four frames, gathering the four pixel values with independent
-// loads. Pixels shared by neighbouring bins are read by neighbouring segments
-// at nearly the same time, so the second read is served by L2.
+// Layout. The masked table is cut into segments: a segment is a run of one
+// row's entries whose pixels lie in one strip of `strip_rows` detector rows
+// (rows list pixels in ascending order, so this is a contiguous range), split
+// further to at most kSegMax entries. Within a strip, the segments of
+// neighbouring rows are grouped into units of at most kWarps segments and
+// unit_cap entries. One CTA owns one unit: it stages the unit's packed entries
+// in shared memory once and sweeps every frame of the call over them, so the
+// table crosses HBM once per call however many frames there are. Neighbouring
+// bins share most pixels (a split pixel falls in ~2.6 bins), and a unit's
+// bins cover the same strip of the detector: warps take (segment, frame
+// group) tasks in frame-major order, so at any time the CTA's warps read the
+// same few kilobytes of the same frames and the repeats are served by L1
+// instead of each costing an L2 sector.
+//
+// A lane reads one staged entry (col, weight[, norm, weight/norm]) and
+// applies it to kFramesPerPass frames, gathering the pixel values with
+// independent loads.
 //
 // Arithmetic. Sums are FP32 products accumulated in short plain-FP32 blocks
 // (at most kFlush terms per lane) that are folded into a double-word (hi, lo)
-// FP32 accumulator with TwoSum, then merged across lanes with TwoSum and across
-// segments in a fixed order in the finalize pass, which divides in FP64. The
+// FP32 accumulator with TwoSum; each lane's double-word sum is exact in FP64,
+// and lanes, then segments, are added in FP64 in a fixed order. The
 // reduction order depends only on the table, never on how many frames a call
 // carries, so one frame alone and the same frame inside a batch give
 // bit-identical results.
@@ -21,7 +29,8 @@
 // Azimuthal spread (azimuthal.rs:48-118): with x = s/n, w = c*n and origin
 // o = x of the row's first valid entry, t = s - o*n (one FMA) gives
 // w*(x - o) = c*t and w*(x - o)^2 = (c/n)*t*t, so the shifted moments
-// A = sum c*t and B = sum (c/n)*t*t need no division per pixel and
+// B = sum (c/n)*t*t needs no division per pixel, A = sum c*t equals
+// S - o*sum(c*n) and is formed once per row in the finalize, and
 // m2 = B - A^2 / sum(w).
 #include <algorithm>
 #include <type_traits>
@@ -35,13 +44,31 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kFramesPerPass = 4;
 constexpr int kFlush = 16;
+constexpr int kUnroll = 4;  // entries per lane per step; kFlush is a multiple
+constexpr int kSegMax = 1024;
+constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
 enum Mode { kIntensity = 0, kErrors = 1, kSpread = 2 };
 
-template <int MODE>
+template <typename P>
+constexpr bool is_float_px() {
+    return std::is_same<P, float>::value || std::is_same<P, double>::value;
+}
+
+// Accumulators per (segment, frame): S = sum c*s, then V = sum c^2*max(s,0),
+// then for the spread B = sum (c/n)*t^2, then for float pixels the weight
+// c*n and the count of non-finite pixels. The spread's first moment
+// A = sum c*t = S - o*sum c*n is formed in the finalize.
+template <int MODE, typename P>
 struct NAcc {
-    static constexpr int value = MODE == kIntensity ? 1 : MODE == kErrors ? 2 : 6;
+    static constexpr int value =
+        MODE == kIntensity ? 1 : MODE == kErrors ? 2 : (is_float_px<P>() ? 5 : 3);
 };
+
+template <typename P>
+constexpr bool is_unsigned_px() {
+    return std::is_same<P, uint16_t>::value || std::is_same<P, uint32_t>::value;
+}
 
 // Double-word FP32 accumulator with a plain FP32 block in front.
 struct AccDW {
@@ -82,36 +109,69 @@ __device__ __forceinline__ float load_px<double>(const double *__restrict__ f, u
     return __double2float_rn(__ldg(f + i));
 }
 
+// Origin o = s/n of the row's first valid entry in this frame
+// (azimuthal.rs:80-82): entries that are statically invalid carry c = 0, and
+// for float pixels a non-finite value moves on to the next entry.
 template <typename P>
-constexpr bool is_float_px() {
-    return std::is_same<P, float>::value || std::is_same<P, double>::value;
+__device__ __forceinline__ float row_origin(const float4 *__restrict__ entry_std, int first,
+                                            int row_end, const P *__restrict__ frame) {
+    if (first < 0) return 0.f;
+    int k = first;
+    float4 e = entry_std[k];
+    float s = load_px<P>(frame, uint32_t(__float_as_int(e.x)));
+    if (is_float_px<P>()) {
+        while (!isfinite(s) && ++k < row_end) {
+            e = entry_std[k];
+            if (e.y > 0.f) s = load_px<P>(frame, uint32_t(__float_as_int(e.x)));
+        }
+    }
+    return __fdiv_rn(s, e.z);
 }
 
-// One CTA per segment; see the file comment.
+// One CTA per unit; see the file comment.
 template <int MODE, typename P>
 __global__ void __launch_bounds__(kThreads)
-    k_gather(const int4 *__restrict__ segs, const int2 *__restrict__ entry,
-             const float4 *__restrict__ entry_std, const int32_t *__restrict__ first_valid,
-             const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_segments,
-             float *__restrict__ partial) {
-    constexpr int NA = NAcc<MODE>::value;
+    k_gather(const int2 *__restrict__ units, const int4 *__restrict__ segs,
+             const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
+             const int32_t *__restrict__ first_valid, const P *__restrict__ frames,
+             int64_t n_pixels, int n_frames, int n_segments, double *__restrict__ partial) {
+    constexpr int NA = NAcc<MODE, P>::value;
     extern __shared__ __align__(16) unsigned char smem[];
-    const int4 sg = segs[blockIdx.x];
-    const int row = sg.x, begin = sg.y, len = sg.z - sg.y;
+    __shared__ int s_off[kWarps + 1];
+    const int2 un = units[blockIdx.x];
+    const int seg0 = un.x, nseg = un.y;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-    // Stage the segment's entries (16-byte vector copies).
-    if (MODE == kSpread) {
-        float4 *st = reinterpret_cast<float4 *>(smem);
-        for (int j = threadIdx.x; j < len; j += kThreads) st[j] = entry_std[begin + j];
-    } else {
-        int2 *st = reinterpret_cast<int2 *>(smem);
-        for (int j = threadIdx.x; j < len; j += kThreads) st[j] = entry[begin + j];
+    if (threadIdx.x == 0) {
+        int o = 0;
+        for (int i = 0; i < nseg; ++i) {
+            s_off[i] = o;
+            const int4 sg = segs[seg0 + i];
+            o += sg.z - sg.y;
+        }
+        s_off[nseg] = o;
+    }
+    __syncthreads();
+    // Stage the unit's entries (16- or 8-byte vector copies, segment by segment).
+    for (int i = 0; i < nseg; ++i) {
+        const int4 sg = segs[seg0 + i];
+        const int len = sg.z - sg.y, off = s_off[i];
+        if (MODE == kSpread) {
+            float4 *st = reinterpret_cast<float4 *>(smem) + off;
+            for (int j = threadIdx.x; j < len; j += kThreads) st[j] = entry_std[sg.y + j];
+        } else {
+            int2 *st = reinterpret_cast<int2 *>(smem) + off;
+            for (int j = threadIdx.x; j < len; j += kThreads) st[j] = entry[sg.y + j];
+        }
     }
     __syncthreads();
 
     const int groups = (n_frames + kFramesPerPass - 1) / kFramesPerPass;
-    for (int grp = warp; grp < groups; grp += kWarps) {
+    const int tasks = groups * nseg;
+    // Frame-major task order: the CTA's warps work on the same frames at once.
+    for (int task = warp; task < tasks; task += kWarps) {
+        const int grp = task / nseg, si = task - grp * nseg;
+        const int4 sg = segs[seg0 + si];
+        const int row = sg.x, len = sg.z - sg.y, off = s_off[si];
         const int f0 = grp * kFramesPerPass;
         const P *fr[kFramesPerPass];
         bool fv[kFramesPerPass];
@@ -122,26 +182,10 @@ __global__ void __launch_bounds__(kThreads)
         }
         float origin[kFramesPerPass];
         if (MODE == kSpread) {
-            // o = s/n of the row's first valid entry (azimuthal.rs:80-82).
             const int fvi = first_valid[row];
 #pragma unroll
-            for (int q = 0; q < kFramesPerPass; ++q) {
-                origin[q] = 0.f;
-                if (fvi >= 0) {
-                    int k = fvi;
-                    float4 e = entry_std[k];
-                    float s = load_px<P>(fr[q], uint32_t(__float_as_int(e.x)));
-                    if (is_float_px<P>()) {
-                        // Skip entries whose pixel is not finite in this frame.
-                        const int row_end = sg.w;
-                        while (!isfinite(s) && ++k < row_end) {
-                            e = entry_std[k];
-                            if (e.y > 0.f) s = load_px<P>(fr[q], uint32_t(__float_as_int(e.x)));
-                        }
-                    }
-                    origin[q] = __fdiv_rn(s, e.z);
-                }
-            }
+            for (int q = 0; q < kFramesPerPass; ++q)
+                origin[q] = row_origin<P>(entry_std, fvi, sg.w, fr[q]);
         }
         AccDW acc[kFramesPerPass][NA];
 #pragma unroll
@@ -149,44 +193,69 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
             for (int a = 0; a < NA; ++a) acc[q][a].zero();
 
+        // kUnroll entries per lane per step: all their pixel loads are issued
+        // before any is used. Slots past the end read pixel 0 with weight 0.
         int since = 0;
-        for (int j = lane; j < len; j += 32) {
+        for (int j0 = lane; j0 < len; j0 += 32 * kUnroll) {
             if (MODE == kSpread) {
-                const float4 e = reinterpret_cast<const float4 *>(smem)[j];
-                const uint32_t col = uint32_t(__float_as_int(e.x));
-                const float c = e.y, n = e.z, cr = e.w;
-                const float c2 = __fmul_rn(c, c);
-                float s[kFramesPerPass];
+                float4 e[kUnroll];
 #pragma unroll
-                for (int q = 0; q < kFramesPerPass; ++q) s[q] = load_px<P>(fr[q], col);
+                for (int u = 0; u < kUnroll; ++u) {
+                    const int j = j0 + 32 * u;
+                    e[u] = j < len ? reinterpret_cast<const float4 *>(smem)[off + j]
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                float s[kUnroll][kFramesPerPass];
 #pragma unroll
-                for (int q = 0; q < kFramesPerPass; ++q) {
-                    float v = s[q];
-                    if (is_float_px<P>() && !isfinite(v)) {
-                        acc[q][4].add(__fmul_rn(c, n));
-                        acc[q][5].add(c > 0.f ? 1.f : 0.f);
-                        continue;
+                for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+                    for (int q = 0; q < kFramesPerPass; ++q)
+                        s[u][q] = load_px<P>(fr[q], uint32_t(__float_as_int(e[u].x)));
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    const float c = e[u].y, n = e[u].z, cr = e[u].w;
+                    const float c2 = __fmul_rn(c, c);
+#pragma unroll
+                    for (int q = 0; q < kFramesPerPass; ++q) {
+                        float v = s[u][q];
+                        if (is_float_px<P>() && !isfinite(v)) {
+                            acc[q][NA - 2].add(__fmul_rn(c, n));
+                            acc[q][NA - 1].add(c > 0.f ? 1.f : 0.f);
+                            continue;
+                        }
+                        acc[q][0].fma(c, v);
+                        acc[q][1].fma(c2, is_unsigned_px<P>() ? v : fmaxf(v, 0.f));
+                        const float t = __fmaf_rn(-origin[q], n, v);
+                        acc[q][2].fma(__fmul_rn(cr, t), t);
                     }
-                    acc[q][0].fma(c, v);
-                    acc[q][1].fma(c2, fmaxf(v, 0.f));
-                    const float t = __fmaf_rn(-origin[q], n, v);
-                    acc[q][2].fma(c, t);
-                    acc[q][3].fma(__fmul_rn(cr, t), t);
                 }
             } else {
-                const int2 e = reinterpret_cast<const int2 *>(smem)[j];
-                const uint32_t col = uint32_t(e.x);
-                const float c = __int_as_float(e.y);
-                float s[kFramesPerPass];
+                int2 e[kUnroll];
 #pragma unroll
-                for (int q = 0; q < kFramesPerPass; ++q) s[q] = load_px<P>(fr[q], col);
+                for (int u = 0; u < kUnroll; ++u) {
+                    const int j = j0 + 32 * u;
+                    e[u] = j < len ? reinterpret_cast<const int2 *>(smem)[off + j] : make_int2(0, 0);
+                }
+                float s[kUnroll][kFramesPerPass];
 #pragma unroll
-                for (int q = 0; q < kFramesPerPass; ++q) {
-                    acc[q][0].fma(c, s[q]);
-                    if (MODE == kErrors) acc[q][1].fma(__fmul_rn(c, c), fmaxf(s[q], 0.f));
+                for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+                    for (int q = 0; q < kFramesPerPass; ++q)
+                        s[u][q] = load_px<P>(fr[q], uint32_t(e[u].x));
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    const float c = __int_as_float(e[u].y);
+#pragma unroll
+                    for (int q = 0; q < kFramesPerPass; ++q) {
+                        acc[q][0].fma(c, s[u][q]);
+                        if (MODE == kErrors)
+                            acc[q][1].fma(__fmul_rn(c, c),
+                                          is_unsigned_px<P>() ? s[u][q] : fmaxf(s[u][q], 0.f));
+                    }
                 }
             }
-            if (++since == kFlush) {
+            since += kUnroll;
+            if (since == kFlush) {
                 since = 0;
 #pragma unroll
                 for (int q = 0; q < kFramesPerPass; ++q)
@@ -198,53 +267,57 @@ __global__ void __launch_bounds__(kThreads)
         for (int q = 0; q < kFramesPerPass; ++q)
 #pragma unroll
             for (int a = 0; a < NA; ++a) acc[q][a].flush();
-        // Fixed butterfly-free tree: lane i takes lane i + o for o = 16..1.
+        // Each lane's double-word sum is exact in FP64; the lanes are then
+        // folded by a fixed FP64 tree: lane i takes lane i + o for o = 16..1.
+        double d[kFramesPerPass][NA];
+#pragma unroll
+        for (int q = 0; q < kFramesPerPass; ++q)
+#pragma unroll
+            for (int a = 0; a < NA; ++a) d[q][a] = double(acc[q][a].hi) + double(acc[q][a].lo);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
             for (int q = 0; q < kFramesPerPass; ++q)
 #pragma unroll
-                for (int a = 0; a < NA; ++a) {
-                    float h2 = __shfl_down_sync(0xffffffffu, acc[q][a].hi, o);
-                    float l2 = __shfl_down_sync(0xffffffffu, acc[q][a].lo, o);
-                    acc[q][a].merge(h2, l2);
-                }
+                for (int a = 0; a < NA; ++a)
+                    d[q][a] = __dadd_rn(d[q][a], __shfl_down_sync(0xffffffffu, d[q][a], o));
         if (lane == 0) {
 #pragma unroll
             for (int q = 0; q < kFramesPerPass; ++q) {
                 if (!fv[q]) continue;
-                float *out = partial + (int64_t(f0 + q) * n_segments + blockIdx.x) * (2 * NA);
+                double *out = partial + (int64_t(f0 + q) * n_segments + seg0 + si) * NA;
 #pragma unroll
-                for (int a = 0; a < NA; ++a) {
-                    out[2 * a] = acc[q][a].hi;
-                    out[2 * a + 1] = acc[q][a].lo;
-                }
+                for (int a = 0; a < NA; ++a) out[a] = d[q][a];
             }
         }
     }
 }
 
-// One thread per (frame, row): fold the row's segment partials in order and
-// normalise in FP64 (normalize_bin, prepared.rs:985-996; the spread's
-// closing formulas, azimuthal.rs:96-104).
-template <int MODE>
-__global__ void k_finalize(const float *__restrict__ partial, const int32_t *__restrict__ row_seg,
+// One thread per (frame, row): fold the row's segment partials in strip
+// order in FP64 and normalise (normalize_bin, prepared.rs:985-996; the
+// spread's closing formulas, azimuthal.rs:96-104).
+template <int MODE, typename P>
+__global__ void k_finalize(const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
+                           const int32_t *__restrict__ seg_ids, const int4 *__restrict__ segs,
                            const double *__restrict__ den, const double *__restrict__ den_std,
-                           const int32_t *__restrict__ valid_std, int n_rows, int n_segments,
-                           int n_frames, double *__restrict__ out_i, double *__restrict__ out_s,
+                           const double *__restrict__ den_f32,
+                           const int32_t *__restrict__ valid_std,
+                           const int32_t *__restrict__ first_valid,
+                           const float4 *__restrict__ entry_std, const P *__restrict__ frames,
+                           int64_t n_pixels, int n_rows, int n_segments, int n_frames,
+                           double *__restrict__ out_i, double *__restrict__ out_s,
                            double *__restrict__ out_d) {
-    constexpr int NA = NAcc<MODE>::value;
+    constexpr int NA = NAcc<MODE, P>::value;
     int64_t id = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
     if (id >= int64_t(n_rows) * n_frames) return;
     int f = int(id / n_rows), r = int(id % n_rows);
-    AccDW acc[NA];
-    for (int a = 0; a < NA; ++a) acc[a].zero();
-    for (int sgi = row_seg[r]; sgi < row_seg[r + 1]; ++sgi) {
-        const float *p = partial + (int64_t(f) * n_segments + sgi) * (2 * NA);
-        for (int a = 0; a < NA; ++a) acc[a].merge(p[2 * a], p[2 * a + 1]);
-    }
     double v[NA];
-    for (int a = 0; a < NA; ++a) v[a] = double(acc[a].hi) + double(acc[a].lo);
+    for (int a = 0; a < NA; ++a) v[a] = 0.0;
+    const int k0 = row_seg[r], k1 = row_seg[r + 1];
+    for (int k = k0; k < k1; ++k) {
+        const double *p = partial + (int64_t(f) * n_segments + seg_ids[k]) * NA;
+        for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[a]);
+    }
     int64_t o = int64_t(f) * n_rows + r;
     if (MODE != kSpread) {
         double n = den[r];
@@ -255,19 +328,28 @@ __global__ void k_finalize(const float *__restrict__ partial, const int32_t *__r
         }
         return;
     }
-    int valid = valid_std[r] - int(acc[5].hi + acc[5].lo + 0.5f);
-    double sw = den_std[r] - v[4];
+    int valid = valid_std[r];
+    double sw = den_std[r], wf = den_f32[r];
+    if (NA == 5) {
+        valid -= int(v[4] + 0.5);
+        sw -= v[3];
+        wf -= v[3];
+    }
     if (valid <= 0 || !(sw > 0.0)) {
         out_i[o] = 0.0;
         if (out_s) out_s[o] = 0.0;
         out_d[o] = __longlong_as_double(0x7ff8000000000000ll);
         return;
     }
+    // A = sum c*(s - o*n) = S - o * sum c*n over the same FP32 weights.
+    const int row_end = k0 < k1 ? segs[seg_ids[k0]].w : 0;
+    const float org = row_origin<P>(entry_std, first_valid[r], row_end, frames + int64_t(f) * n_pixels);
+    const double a1 = v[0] - double(org) * wf;
     out_i[o] = v[0] / sw;
     if (out_s) out_s[o] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
-    double mean = v[2] / sw;
-    double m2 = v[3] - mean * v[2];
-    double q = m2 / sw;
+    const double mean = a1 / sw;
+    const double m2 = v[2] - mean * a1;
+    const double q = m2 / sw;
     out_d[o] = sqrt(q > 0.0 ? q : 0.0);
 }
 
@@ -277,10 +359,11 @@ __global__ void k_pack(const int64_t *__restrict__ row_ptr, int n_rows,
                        const int32_t *__restrict__ col, const double *__restrict__ w,
                        const double *__restrict__ norm, int2 *__restrict__ entry,
                        float4 *__restrict__ entry_std, double *__restrict__ den_std,
-                       int32_t *__restrict__ valid_std, int32_t *__restrict__ first_valid) {
+                       double *__restrict__ den_f32, int32_t *__restrict__ valid_std,
+                       int32_t *__restrict__ first_valid) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
-    double sw = 0.0;
+    double sw = 0.0, swf = 0.0;
     int valid = 0, first = -1;
     for (int64_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
         int32_t j = col[k];
@@ -294,35 +377,77 @@ __global__ void k_pack(const int64_t *__restrict__ row_ptr, int n_rows,
                                    ok ? __double2float_rn(c / n) : 0.f);
         if (ok) {
             sw += ww;
+            swf += double(cf) * double(nf);
             ++valid;
             if (first < 0) first = int(k);
         }
     }
     den_std[r] = sw;
+    den_f32[r] = swf;
     valid_std[r] = valid;
     first_valid[r] = first;
+}
+
+// bounds[r * (n_strips + 1) + s]: first entry of row r whose pixel lies in
+// strip s or later (columns within a row are ascending).
+__global__ void k_strip_bounds(const int64_t *__restrict__ row_ptr, int n_rows,
+                               const int32_t *__restrict__ col, int n_strips, int64_t strip_px,
+                               int32_t *__restrict__ bounds) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    int64_t b = row_ptr[r], e = row_ptr[r + 1];
+    int32_t *out = bounds + int64_t(r) * (n_strips + 1);
+    for (int s = 0; s <= n_strips; ++s) {
+        int64_t key = int64_t(s) * strip_px, lo = b, hi = e;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (int64_t(col[mid]) < key) lo = mid + 1;
+            else hi = mid;
+        }
+        out[s] = int32_t(lo);
+    }
 }
 
 template <typename P>
 void launch_typed(GatherTable &t, const void *frames, int64_t n_pixels, int n_frames, int mode,
                   cudaStream_t s) {
-    const int threads = kThreads;
-    const size_t smem = size_t(t.seg_len) * (mode == kSpread ? 16 : 8);
+    const size_t smem = size_t(t.unit_cap) * (mode == kSpread ? 16 : 8);
     const P *fp = static_cast<const P *>(frames);
+    const int32_t *fv = t.first_valid.ptr;
     if (mode == kSpread) {
-        k_gather<kSpread, P><<<t.n_segments, threads, smem, s>>>(
-            t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.row_seg.ptr + t.n_rows + 1, fp, n_pixels,
-            n_frames, t.n_segments, t.partial.ptr);
+        k_gather<kSpread, P><<<t.n_units, kThreads, smem, s>>>(
+            t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, fv, fp, n_pixels, n_frames,
+            t.n_segments, t.partial.ptr);
     } else if (mode == kErrors) {
-        k_gather<kErrors, P><<<t.n_segments, threads, smem, s>>>(
-            t.seg.ptr, t.entry.ptr, t.entry_std.ptr, nullptr, fp, n_pixels, n_frames,
+        k_gather<kErrors, P><<<t.n_units, kThreads, smem, s>>>(
+            t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, fv, fp, n_pixels, n_frames,
             t.n_segments, t.partial.ptr);
     } else {
-        k_gather<kIntensity, P><<<t.n_segments, threads, smem, s>>>(
-            t.seg.ptr, t.entry.ptr, t.entry_std.ptr, nullptr, fp, n_pixels, n_frames,
+        k_gather<kIntensity, P><<<t.n_units, kThreads, smem, s>>>(
+            t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, fv, fp, n_pixels, n_frames,
             t.n_segments, t.partial.ptr);
     }
     DG_CUDA(cudaGetLastError());
+}
+
+template <int MODE, typename P>
+void launch_finalize(GatherTable &t, const void *frames, int64_t n_pixels, int nf, double *oi,
+                     double *os, double *od, cudaStream_t s) {
+    const int64_t total = int64_t(t.n_rows) * nf;
+    const unsigned blocks = unsigned((total + 255) / 256);
+    k_finalize<MODE, P><<<blocks, 256, 0, s>>>(
+        t.partial.ptr, t.row_seg.ptr, t.seg_ids.ptr, t.seg.ptr, t.den.ptr, t.den_std.ptr,
+        t.den_f32.ptr, t.valid_std.ptr, t.first_valid.ptr, t.entry_std.ptr,
+        static_cast<const P *>(frames), n_pixels, t.n_rows, t.n_segments, nf, oi, os, od);
+    DG_CUDA(cudaGetLastError());
+}
+
+template <typename P>
+void finalize_typed(GatherTable &t, int mode, const void *frames, int64_t n_pixels, int nf,
+                    double *oi, double *os, double *od, cudaStream_t s) {
+    if (mode == kSpread) launch_finalize<kSpread, P>(t, frames, n_pixels, nf, oi, os, od, s);
+    else if (mode == kErrors) launch_finalize<kErrors, P>(t, frames, n_pixels, nf, oi, os, od, s);
+    else launch_finalize<kIntensity, P>(t, frames, n_pixels, nf, oi, os, od, s);
 }
 
 }  // namespace
@@ -332,62 +457,106 @@ int gather_launches_per_call() { return 2; }
 void gather_kernel_time(GatherTable &t, bool reset, double *ms, int64_t *gather_launches,
                         int64_t *launches) {
     double total = 0.0;
-    if (t.events_used) DG_CUDA(cudaEventSynchronize(t.events[t.events_used - 1].second));
-    for (size_t i = 0; i < t.events_used; ++i) {
+    EventPool &p = t.events;
+    if (p.used) DG_CUDA(cudaEventSynchronize(p.events[p.used - 1].second));
+    for (size_t i = 0; i < p.used; ++i) {
         float m = 0.f;
-        DG_CUDA(cudaEventElapsedTime(&m, t.events[i].first, t.events[i].second));
+        DG_CUDA(cudaEventElapsedTime(&m, p.events[i].first, p.events[i].second));
         total += m;
     }
     if (ms) *ms = total;
-    if (gather_launches) *gather_launches = int64_t(t.events_used);
+    if (gather_launches) *gather_launches = int64_t(p.used);
     if (launches) *launches = t.launches;
     if (reset) {
-        t.events_used = 0;
+        p.used = 0;
         t.launches = 0;
     }
 }
 
-void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t seg_len,
-                       cudaStream_t s, GatherTable &out) {
+void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1, int32_t dim2,
+                       int32_t strip_rows, cudaStream_t s, GatherTable &out) {
     out.n_rows = int32_t(table.n_rows);
     out.nnz = table.nnz;
-    out.seg_len = seg_len;
+    out.unit_cap = kUnitCap;
+    out.strip_rows = strip_rows;
     out.entry.alloc(size_t(table.nnz));
     out.entry_std.alloc(size_t(table.nnz));
     out.den.alloc(size_t(table.n_rows));
     out.den_std.alloc(size_t(table.n_rows));
+    out.den_f32.alloc(size_t(table.n_rows));
     out.valid_std.alloc(size_t(table.n_rows));
+    out.first_valid.alloc(size_t(table.n_rows));
     denominators(table, d_norm, s, out.den.ptr);
-    // Segments: rows cut into pieces of at most seg_len entries, on the host
-    // from the row pointers (a few thousand to a few hundred thousand rows).
-    std::vector<int64_t> rp(size_t(table.n_rows) + 1);
-    DG_CUDA(cudaMemcpyAsync(rp.data(), table.row_ptr.ptr, rp.size() * 8, cudaMemcpyDeviceToHost,
-                            s));
+    const unsigned rb = unsigned((table.n_rows + 127) / 128);
+    if (table.n_rows > 0)
+        k_pack<<<rb, 128, 0, s>>>(table.row_ptr.ptr, int(table.n_rows), table.col.ptr, table.w.ptr,
+                                  d_norm, out.entry.ptr, out.entry_std.ptr, out.den_std.ptr,
+                                  out.den_f32.ptr, out.valid_std.ptr, out.first_valid.ptr);
+    DG_CUDA(cudaGetLastError());
+
+    // Segments: (row, strip) runs from per-row strip bounds found on the
+    // device; grouped into units on the host (a few hundred thousand at most).
+    const int n_strips = (dim1 + strip_rows - 1) / strip_rows;
+    const int64_t nb = table.n_rows;
+    DeviceArray<int32_t> bounds;
+    bounds.alloc(size_t(nb * (n_strips + 1)));
+    if (nb > 0)
+        k_strip_bounds<<<rb, 128, 0, s>>>(table.row_ptr.ptr, int(nb), table.col.ptr, n_strips,
+                                          int64_t(strip_rows) * dim2, bounds.ptr);
+    DG_CUDA(cudaGetLastError());
+    std::vector<int32_t> hb(size_t(nb * (n_strips + 1)));
+    std::vector<int64_t> rp(size_t(nb) + 1);
+    if (!hb.empty())
+        DG_CUDA(cudaMemcpyAsync(hb.data(), bounds.ptr, hb.size() * 4, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaMemcpyAsync(rp.data(), table.row_ptr.ptr, rp.size() * 8, cudaMemcpyDeviceToHost, s));
     DG_CUDA(cudaStreamSynchronize(s));
+
     std::vector<int4> segs;
-    std::vector<int32_t> row_seg(size_t(table.n_rows) + 1);
-    for (int64_t r = 0; r < table.n_rows; ++r) {
-        row_seg[size_t(r)] = int32_t(segs.size());
-        for (int64_t b = rp[size_t(r)]; b < rp[size_t(r) + 1]; b += seg_len) {
-            int64_t e = std::min<int64_t>(b + seg_len, rp[size_t(r) + 1]);
-            segs.push_back(make_int4(int(r), int(b), int(e), int(rp[size_t(r) + 1])));
+    std::vector<int2> units;
+    std::vector<int32_t> seg_count(size_t(nb), 0);
+    for (int st = 0; st < n_strips; ++st) {
+        int unit_first = int(segs.size()), unit_entries = 0;
+        auto close_unit = [&]() {
+            if (int(segs.size()) > unit_first)
+                units.push_back(make_int2(unit_first, int(segs.size()) - unit_first));
+            unit_first = int(segs.size());
+            unit_entries = 0;
+        };
+        for (int64_t r = 0; r < nb; ++r) {
+            const int32_t *b = hb.data() + r * (n_strips + 1);
+            for (int32_t lo = b[st]; lo < b[st + 1]; lo += kSegMax) {
+                int32_t hi = std::min<int32_t>(lo + kSegMax, b[st + 1]);
+                int len = hi - lo;
+                if (int(segs.size()) - unit_first == kWarps || unit_entries + len > kUnitCap)
+                    close_unit();
+                segs.push_back(make_int4(int(r), lo, hi, int(rp[size_t(r) + 1])));
+                unit_entries += len;
+                seg_count[size_t(r)]++;
+            }
         }
+        close_unit();
     }
-    row_seg[size_t(table.n_rows)] = int32_t(segs.size());
+    // Row -> its segments, in strip order (the finalize's fixed fold order).
+    std::vector<int32_t> row_seg(size_t(nb) + 1, 0), seg_ids(segs.size());
+    for (int64_t r = 0; r < nb; ++r) row_seg[size_t(r) + 1] = row_seg[size_t(r)] + seg_count[size_t(r)];
+    std::vector<int32_t> fill(row_seg.begin(), row_seg.end() - 1);
+    for (size_t i = 0; i < segs.size(); ++i) seg_ids[size_t(fill[size_t(segs[i].x)]++)] = int32_t(i);
     out.n_segments = int32_t(segs.size());
+    out.n_units = int32_t(units.size());
     out.seg.alloc(std::max<size_t>(segs.size(), 1));
-    if (!segs.empty())
+    out.unit.alloc(std::max<size_t>(units.size(), 1));
+    out.seg_ids.alloc(std::max<size_t>(seg_ids.size(), 1));
+    out.row_seg.alloc(row_seg.size());
+    if (!segs.empty()) {
         DG_CUDA(cudaMemcpyAsync(out.seg.ptr, segs.data(), segs.size() * sizeof(int4),
                                 cudaMemcpyHostToDevice, s));
-    // row_seg followed by first_valid (n_rows) in one allocation.
-    out.row_seg.alloc(size_t(2 * table.n_rows + 1));
+        DG_CUDA(cudaMemcpyAsync(out.unit.ptr, units.data(), units.size() * sizeof(int2),
+                                cudaMemcpyHostToDevice, s));
+        DG_CUDA(cudaMemcpyAsync(out.seg_ids.ptr, seg_ids.data(), seg_ids.size() * 4,
+                                cudaMemcpyHostToDevice, s));
+    }
     DG_CUDA(cudaMemcpyAsync(out.row_seg.ptr, row_seg.data(), row_seg.size() * 4,
                             cudaMemcpyHostToDevice, s));
-    k_pack<<<unsigned((table.n_rows + 127) / 128), 128, 0, s>>>(
-        table.row_ptr.ptr, int(table.n_rows), table.col.ptr, table.w.ptr, d_norm, out.entry.ptr,
-        out.entry_std.ptr, out.den_std.ptr, out.valid_std.ptr,
-        out.row_seg.ptr + table.n_rows + 1);
-    DG_CUDA(cudaGetLastError());
     DG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -396,28 +565,28 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
                 double *d_std, cudaStream_t s) {
     (void)precision;
     if (n_frames <= 0) return;
+    if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
     const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
                                                                                 : kIntensity;
-    const int na = mode == kSpread ? 6 : mode == kErrors ? 2 : 1;
     // Frames per launch bounded by the partial-sum scratch (256 frames).
     const int64_t chunk = 256;
-    const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 2 * 6;
+    const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 5;
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
-    if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
     const size_t esize = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
     for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
         const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
         const void *fp = static_cast<const unsigned char *>(d_frames) + f0 * n_pixels * esize;
-        if (t.n_segments > 0) {
+        if (t.n_units > 0) {
             std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
             if (t.profile) {
-                if (t.events_used == t.events.size()) {
+                EventPool &p = t.events;
+                if (p.used == p.events.size()) {
                     std::pair<cudaEvent_t, cudaEvent_t> e{};
                     DG_CUDA(cudaEventCreate(&e.first));
                     DG_CUDA(cudaEventCreate(&e.second));
-                    t.events.push_back(e);
+                    p.events.push_back(e);
                 }
-                ev = &t.events[t.events_used++];
+                ev = &p.events[p.used++];
                 DG_CUDA(cudaEventRecord(ev->first, s));
             }
             ++t.launches;
@@ -430,28 +599,19 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
             }
             if (ev) DG_CUDA(cudaEventRecord(ev->second, s));
         }
-        const int64_t total = int64_t(t.n_rows) * nf;
-        const unsigned blocks = unsigned((total + 255) / 256);
         double *oi = d_i + f0 * t.n_rows;
         double *os = d_sigma ? d_sigma + f0 * t.n_rows : nullptr;
         double *od = d_std ? d_std + f0 * t.n_rows : nullptr;
-        if (total > 0) {
+        if (t.n_rows > 0) {
             ++t.launches;
-            if (mode == kSpread)
-                k_finalize<kSpread><<<blocks, 256, 0, s>>>(t.partial.ptr, t.row_seg.ptr, t.den.ptr,
-                                                           t.den_std.ptr, t.valid_std.ptr, t.n_rows,
-                                                           t.n_segments, nf, oi, os, od);
-            else if (mode == kErrors)
-                k_finalize<kErrors><<<blocks, 256, 0, s>>>(t.partial.ptr, t.row_seg.ptr, t.den.ptr,
-                                                           t.den_std.ptr, t.valid_std.ptr, t.n_rows,
-                                                           t.n_segments, nf, oi, os, od);
-            else
-                k_finalize<kIntensity><<<blocks, 256, 0, s>>>(
-                    t.partial.ptr, t.row_seg.ptr, t.den.ptr, t.den_std.ptr, t.valid_std.ptr,
-                    t.n_rows, t.n_segments, nf, oi, os, od);
-            DG_CUDA(cudaGetLastError());
+            switch (dtype) {
+            case DG_U16: finalize_typed<uint16_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            case DG_U32: finalize_typed<uint32_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            case DG_I32: finalize_typed<int32_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            case DG_F32: finalize_typed<float>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            case DG_F64: finalize_typed<double>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            }
         }
-        (void)na;
     }
 }
 

@@ -116,61 +116,65 @@ void denominators(const DeviceCsr &table, const double *d_norm, cudaStream_t str
 void eval_math(int which, const double *a, const double *b, int64_t n, double *out,
                cudaStream_t stream);
 
-// Gather-side table: packed entries + row segments (dg_gather.cu).
-struct GatherTable {
-    int32_t n_rows = 0;
-    int64_t nnz = 0;
-    int32_t n_segments = 0;
-    int32_t seg_len = 0;
-    DeviceArray<int4> seg;          // {row, begin, end, first_of_row}
-    DeviceArray<int32_t> row_seg;   // n_rows + 1: segments of row r
-    DeviceArray<int2> entry;        // {col, weight bits} for the I/sigma path
-    DeviceArray<float4> entry_std;  // {col bits, c, n, c/n} for the spread path
-    DeviceArray<double> den;        // strict f64 Σ w·norm
-    DeviceArray<double> den_std;    // Σ c·n over entries valid for the spread
-    DeviceArray<int32_t> valid_std; // entries valid for the spread, per row
-    DeviceArray<float> partial;     // scratch: per (segment, frame) double-word sums
-    int64_t partial_frames = 0;
-    // Optional CUDA-event timing of the gather launches (dg_plan_profile).
-    bool profile = false;
+// Pairs of CUDA events, created on demand and destroyed with the pool.
+struct EventPool {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
-    size_t events_used = 0;
-    int64_t launches = 0;  // every kernel launch of run_gather since the last reset
-    ~GatherTable() {
+    size_t used = 0;
+    EventPool() = default;
+    EventPool(const EventPool &) = delete;
+    EventPool &operator=(const EventPool &) = delete;
+    EventPool(EventPool &&o) noexcept : events(std::move(o.events)), used(o.used) {
+        o.events.clear();
+        o.used = 0;
+    }
+    EventPool &operator=(EventPool &&o) noexcept {
+        if (this != &o) {
+            destroy();
+            events = std::move(o.events);
+            used = o.used;
+            o.events.clear();
+            o.used = 0;
+        }
+        return *this;
+    }
+    ~EventPool() { destroy(); }
+    void destroy() {
         for (auto &e : events) {
             cudaEventDestroy(e.first);
             cudaEventDestroy(e.second);
         }
+        events.clear();
+        used = 0;
     }
-    GatherTable() = default;
-    GatherTable(const GatherTable &) = delete;
-    GatherTable &operator=(GatherTable &&o) noexcept {
-        if (this != &o) {
-            for (auto &e : events) {
-                cudaEventDestroy(e.first);
-                cudaEventDestroy(e.second);
-            }
-            n_rows = o.n_rows;
-            nnz = o.nnz;
-            n_segments = o.n_segments;
-            seg_len = o.seg_len;
-            seg = std::move(o.seg);
-            row_seg = std::move(o.row_seg);
-            entry = std::move(o.entry);
-            entry_std = std::move(o.entry_std);
-            den = std::move(o.den);
-            den_std = std::move(o.den_std);
-            valid_std = std::move(o.valid_std);
-            partial = std::move(o.partial);
-            partial_frames = o.partial_frames;
-            profile = o.profile;
-            events = std::move(o.events);
-            o.events.clear();
-            events_used = o.events_used;
-            launches = o.launches;
-        }
-        return *this;
-    }
+};
+
+// Gather-side table (dg_gather.cu). The masked table is cut into segments,
+// each a run of one row's entries whose pixels lie in one strip of detector
+// rows; segments of the same strip and neighbouring rows are grouped into
+// units, one CTA each, so a CTA's warps read the same detector region.
+struct GatherTable {
+    int32_t n_rows = 0;
+    int64_t nnz = 0;
+    int32_t n_segments = 0;
+    int32_t n_units = 0;
+    int32_t unit_cap = 0;             // most entries one unit stages in shared memory
+    int32_t strip_rows = 0;           // detector rows per strip
+    DeviceArray<int4> seg;            // {row, begin, end, row end}
+    DeviceArray<int2> unit;           // {first segment, segment count}
+    DeviceArray<int32_t> row_seg;     // n_rows + 1: row r's segments are
+    DeviceArray<int32_t> seg_ids;     //   seg_ids[row_seg[r] .. row_seg[r+1]) in strip order
+    DeviceArray<int32_t> first_valid; // first entry valid for the spread, per row (-1: none)
+    DeviceArray<int2> entry;          // {col, weight bits} for the I/sigma path
+    DeviceArray<float4> entry_std;    // {col bits, c, n, c/n} for the spread path
+    DeviceArray<double> den;          // strict f64 sum w*norm
+    DeviceArray<double> den_std;      // sum c*n over entries valid for the spread
+    DeviceArray<double> den_f32;      // the same sum over the FP32-rounded c and n
+    DeviceArray<int32_t> valid_std;   // entries valid for the spread, per row
+    DeviceArray<double> partial;      // scratch: per (frame, segment) FP64 sums
+    // Optional CUDA-event timing of the gather launches (dg_plan_profile).
+    bool profile = false;
+    EventPool events;
+    int64_t launches = 0;  // every kernel launch of run_gather since the last reset
 };
 
 // Sums the recorded gather-kernel event pairs (synchronising on the last);
@@ -178,8 +182,8 @@ struct GatherTable {
 void gather_kernel_time(GatherTable &t, bool reset, double *ms, int64_t *gather_launches,
                         int64_t *launches);
 
-void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t seg_len,
-                       cudaStream_t stream, GatherTable &out);
+void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1,
+                       int32_t dim2, int32_t strip_rows, cudaStream_t stream, GatherTable &out);
 // Enqueues the batched gather for n_frames device-resident frames.
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                 int64_t n_frames, uint32_t flags, int precision, double *d_i, double *d_sigma,

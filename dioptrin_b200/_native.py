@@ -23,7 +23,8 @@ DG_PLAN_KEEP_TABLES = 1
 EXPORTS = [
     "dg_plan_create", "dg_plan_destroy", "dg_plan_query", "dg_plan_radial",
     "dg_plan_azimuthal", "dg_plan_export_table", "dg_integrate", "dg_integrate_device",
-    "dg_integrate_device_plain", "dg_plan_profile", "dg_plan_kernel_time", "dg_eval_math",
+    "dg_integrate_device_plain", "dg_integrate_device_noalloc", "dg_plan_profile",
+    "dg_plan_kernel_time", "dg_eval_math",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
     "dg_device_info_get", "dg_last_error",
@@ -107,7 +108,8 @@ def lib():
         L.dg_plan_azimuthal.argtypes = [vp, pd, C.c_int64]
         L.dg_plan_export_table.argtypes = [vp, C.c_int32, P(C.c_int64), P(C.c_int32), pd, pd]
         L.dg_integrate.argtypes = [vp, vp, C.c_int32, C.c_int64, C.c_uint32, pd, pd, pd]
-        for name in ("dg_integrate_device", "dg_integrate_device_plain"):
+        for name in ("dg_integrate_device", "dg_integrate_device_plain",
+                     "dg_integrate_device_noalloc"):
             getattr(L, name).argtypes = [vp, vp, C.c_int32, C.c_int64, C.c_uint32, vp, vp, vp,
                                          vp]
         L.dg_plan_profile.argtypes = [vp, C.c_int32]

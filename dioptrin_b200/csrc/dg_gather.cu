@@ -616,3 +616,161 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
 }
 
 }  // namespace dg
+
+// ---------------------------------------------------------------------------
+// Allocation-free integration (dg_integrate_device_noalloc).
+//
+// For callers that must not allocate device memory while they integrate: a
+// real-time acquisition loop with a fixed memory budget, a host thread that
+// may not enter the CUDA allocator, or code running where cudaMalloc is not
+// permitted. dg_integrate_device allocates its per-segment partial sums on
+// first use; this variant keeps them in one fixed array in the library
+// instead, so after the plan exists nothing is allocated. The plan itself is
+// created beforehand with dg_plan_create, which does allocate.
+//
+// The array is a file-scope __device__ variable of kNoAllocScratchBytes. Host
+// code cannot use its name as a device address, so its address is obtained
+// with cudaGetSymbolAddress once per device, with that device current, on
+// the first call on that device; make that first call before any stream
+// capture. Every call on a device shares the one array: calls that overlap on
+// the GPU (from different streams or threads) race on it, so serialise them.
+// Every partial sum the finalize reads is written by the gather kernel of the
+// same call, so nothing needs clearing between calls.
+namespace dg {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
+constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_partial[kNoAllocScratchDoubles];
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// The array's device address on `device` (current), resolved once.
+double *noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices)
+        fail(DG_UNSUPPORTED, "device ordinal beyond the allocation-free path's table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partial);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            fail(DG_DEVICE, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
+                                cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[device] = static_cast<double *>(p);
+    }
+    return g_noalloc_ptr[device];
+}
+
+template <typename P>
+void noalloc_launch(const GatherTable &t, double *partial, const void *frames, int64_t n_pixels,
+                    int nf, int mode, double *oi, double *os, double *od, cudaStream_t s) {
+    const P *fp = static_cast<const P *>(frames);
+    if (t.n_units > 0) {
+        const size_t smem = size_t(t.unit_cap) * (mode == kSpread ? 16 : 8);
+        if (mode == kSpread)
+            k_gather<kSpread, P><<<t.n_units, kThreads, smem, s>>>(
+                t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp,
+                n_pixels, nf, t.n_segments, partial);
+        else if (mode == kErrors)
+            k_gather<kErrors, P><<<t.n_units, kThreads, smem, s>>>(
+                t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp,
+                n_pixels, nf, t.n_segments, partial);
+        else
+            k_gather<kIntensity, P><<<t.n_units, kThreads, smem, s>>>(
+                t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp,
+                n_pixels, nf, t.n_segments, partial);
+        DG_CUDA(cudaGetLastError());
+    }
+    if (t.n_rows > 0) {
+        const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);
+#define DG_NOALLOC_FINALIZE(M)                                                                 \
+    k_finalize<M, P><<<blocks, 256, 0, s>>>(                                                   \
+        partial, t.row_seg.ptr, t.seg_ids.ptr, t.seg.ptr, t.den.ptr, t.den_std.ptr,           \
+        t.den_f32.ptr, t.valid_std.ptr, t.first_valid.ptr, t.entry_std.ptr, fp, n_pixels,      \
+        t.n_rows, t.n_segments, nf, oi, os, od)
+        if (mode == kSpread) DG_NOALLOC_FINALIZE(kSpread);
+        else if (mode == kErrors) DG_NOALLOC_FINALIZE(kErrors);
+        else DG_NOALLOC_FINALIZE(kIntensity);
+#undef DG_NOALLOC_FINALIZE
+        DG_CUDA(cudaGetLastError());
+    }
+}
+
+}  // namespace
+}  // namespace dg
+
+extern "C" dg_status dg_integrate_device_noalloc(dg_plan *plan, const void *d_frames,
+                                                 int32_t dtype, int64_t n_frames, uint32_t flags,
+                                                 double *d_i, double *d_s, double *d_d,
+                                                 void *stream) {
+    using namespace dg;
+    try {
+        if (!plan) fail(DG_INVALID_INPUT, "plan must not be NULL");
+        if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
+        if (n_frames < 0) fail(DG_INVALID_INPUT, "frame count must not be negative");
+        if (flags & ~(DG_ERRORS | DG_AZIMUTHAL_STD)) fail(DG_INVALID_INPUT, "unknown flags");
+        if (n_frames == 0) return DG_OK;
+        if (!d_frames || !d_i) fail(DG_INVALID_INPUT, "frames and intensity must not be NULL");
+        if ((flags & DG_ERRORS) && !d_s) fail(DG_INVALID_INPUT, "errors requested without an output");
+        if ((flags & DG_AZIMUTHAL_STD) && !d_d)
+            fail(DG_INVALID_INPUT, "azimuthal_std requested without an output");
+        if ((flags & DG_AZIMUTHAL_STD) && plan->n_azimuthal != 0)
+            fail(DG_UNSUPPORTED, "azimuthal_std is defined for 1D tables only");
+        std::lock_guard<std::mutex> lock(plan->mu);
+        int previous = -1;
+        DG_CUDA(cudaGetDevice(&previous));
+        if (previous != plan->device) DG_CUDA(cudaSetDevice(plan->device));
+        struct Restore {
+            int dev;
+            ~Restore() {
+                int now = -1;
+                if (dev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != dev) cudaSetDevice(dev);
+            }
+        } restore{previous};
+        double *scratch = noalloc_scratch(plan->device);
+        const GatherTable &t = plan->gather;
+        const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
+                                                                                    : kIntensity;
+        const bool fpx = dtype == DG_F32 || dtype == DG_F64;
+        const int na = mode == kIntensity ? 1 : mode == kErrors ? 2 : (fpx ? 5 : 3);
+        const int64_t per_frame = std::max<int64_t>(1, t.n_segments) * na;
+        const int64_t chunk = std::min<int64_t>(int64_t(kNoAllocScratchDoubles) / per_frame, 256);
+        if (chunk < 1)
+            fail(DG_UNSUPPORTED,
+                 "this plan needs " + std::to_string(per_frame * 8) +
+                     " bytes of partial sums per frame; the allocation-free path holds " +
+                     std::to_string(kNoAllocScratchBytes) + " bytes (use dg_integrate_device)");
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        const int64_t npix = int64_t(plan->dim1) * plan->dim2;
+        const size_t es = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
+        for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
+            const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
+            const void *fp = static_cast<const unsigned char *>(d_frames) + f0 * npix * int64_t(es);
+            double *oi = d_i + f0 * t.n_rows;
+            double *os = (flags & DG_ERRORS) ? d_s + f0 * t.n_rows : nullptr;
+            double *od = (flags & DG_AZIMUTHAL_STD) ? d_d + f0 * t.n_rows : nullptr;
+            switch (dtype) {
+            case DG_U16: noalloc_launch<uint16_t>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
+            case DG_U32: noalloc_launch<uint32_t>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
+            case DG_I32: noalloc_launch<int32_t>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
+            case DG_F32: noalloc_launch<float>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
+            case DG_F64: noalloc_launch<double>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
+            }
+        }
+        return DG_OK;
+    } catch (const Error &e) {
+        set_last_error(e.message);
+        return e.status;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return DG_DEVICE;
+    } catch (...) {
+        set_last_error("unknown failure");
+        return DG_DEVICE;
+    }
+}

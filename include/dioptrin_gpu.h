@@ -147,6 +147,24 @@ DG_EXPORT dg_status dg_integrate_device(dg_plan *plan, const void *d_frames, int
                               int64_t n_frames, uint32_t flags, double *d_intensity,
                               double *d_sigma, double *d_std, void *stream);
 
+/* Allocation-free form of dg_integrate_device; it has no counterpart in the
+ * reference. For callers that may not allocate device memory while they
+ * integrate (a real-time acquisition loop with a fixed memory budget, a thread
+ * that must not enter the CUDA allocator): dg_integrate_device allocates its
+ * partial sums on first use, this call keeps them in one fixed 32 MiB array
+ * that every GPU loading the library holds until the process exits. It calls
+ * no cudaMalloc or cudaFree; the plan (from dg_plan_create, which does
+ * allocate) and the frames and results are the caller's. A plan whose partial
+ * sums for a single frame exceed the array is rejected with
+ * DG_UNSUPPORTED. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make it before any stream capture. All
+ * calls on a device share the array, so calls that overlap on the GPU race:
+ * serialise them. Results equal dg_integrate_device's. */
+DG_EXPORT dg_status dg_integrate_device_noalloc(dg_plan *plan, const void *d_frames,
+                                                int32_t dtype, int64_t n_frames, uint32_t flags,
+                                                double *d_intensity, double *d_sigma,
+                                                double *d_std, void *stream);
+
 /* One-frame-per-launch form of dg_integrate_device: one gather launch per
  * frame, the table re-read for every frame. The plain GPU path the batched
  * kernel is measured against. */

@@ -24,7 +24,7 @@ EXPORTS = [
     "dg_plan_create", "dg_plan_destroy", "dg_plan_query", "dg_plan_radial",
     "dg_plan_azimuthal", "dg_plan_export_table", "dg_integrate", "dg_integrate_device",
     "dg_integrate_device_plain", "dg_integrate_device_noalloc", "dg_plan_profile",
-    "dg_plan_kernel_time", "dg_eval_math",
+    "dg_plan_kernel_time", "dg_plan_autotune", "dg_plan_variant", "dg_eval_math",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
     "dg_device_info_get", "dg_last_error",
@@ -114,6 +114,9 @@ def lib():
                                          vp]
         L.dg_plan_profile.argtypes = [vp, C.c_int32]
         L.dg_plan_kernel_time.argtypes = [vp, C.c_int32, pd, P(C.c_int64), P(C.c_int64)]
+        L.dg_plan_autotune.argtypes = [vp, vp, C.c_int32, C.c_int64, C.c_uint32, vp,
+                                       P(C.c_int32), pd, C.c_int32]
+        L.dg_plan_variant.argtypes = [vp, C.c_int32, P(C.c_int32), P(C.c_int32)]
         L.dg_eval_math.argtypes = [C.c_int32, vp, vp, C.c_int64, vp]
         L.dg_server_create.argtypes = [P(ServerConfig), P(vp)]
         L.dg_server_destroy.argtypes = [vp]

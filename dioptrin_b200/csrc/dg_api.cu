@@ -442,6 +442,40 @@ dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *gather_ms,
     });
 }
 
+dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype, int64_t n_frames,
+                           uint32_t flags, void *stream, int32_t *variant, double *ms,
+                           int32_t n_ms) {
+    return guarded([&] {
+        if (!plan) dg::fail(DG_INVALID_INPUT, "plan must not be NULL");
+        if (flags & ~uint32_t(DG_ERRORS | DG_AZIMUTHAL_STD)) dg::fail(DG_INVALID_INPUT, "unknown flags");
+        if (n_frames <= 0 || !d_frames)
+            dg::fail(DG_INVALID_INPUT, "autotuning needs device frames (n_frames >= 1)");
+        if ((flags & DG_AZIMUTHAL_STD) && plan->n_azimuthal != 0)
+            dg::fail(DG_UNSUPPORTED, "azimuthal_std is defined for 1D tables only");
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        std::vector<double> each;
+        const int v = dg::autotune_gather(plan->gather, d_frames, dtype,
+                                          int64_t(plan->dim1) * plan->dim2, n_frames, flags, s,
+                                          &each);
+        if (variant) *variant = v;
+        for (int32_t i = 0; ms && i < n_ms && size_t(i) < each.size(); ++i) ms[i] = each[size_t(i)];
+    });
+}
+
+dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current, int32_t *count) {
+    return guarded([&] {
+        if (!plan) dg::fail(DG_INVALID_INPUT, "plan must not be NULL");
+        std::lock_guard<std::mutex> lock(plan->mu);
+        if (set >= dg::gather_variant_count())
+            dg::fail(DG_INVALID_INPUT, "gather mapping " + std::to_string(set) + " does not exist");
+        if (set >= 0) plan->gather.variant = set;
+        if (current) *current = plan->gather.variant;
+        if (count) *count = dg::gather_variant_count();
+    });
+}
+
 dg_status dg_eval_math(int32_t which, const double *d_a, const double *d_b, int64_t n,
                        double *d_out) {
     return guarded([&] {

@@ -14,9 +14,10 @@
 // same few kilobytes of the same frames and the repeats are served by L1
 // instead of each costing an L2 sector.
 //
-// A lane reads one staged entry (col, weight[, norm, weight/norm]) and
-// applies it to kFramesPerPass frames, gathering the pixel values with
-// independent loads.
+// A task is (segment, group of kFrameLanes frames); lane (frame, slice)
+// reads every kSlices-th staged entry (col, weight[, norm, weight/norm]) and
+// gathers that pixel of its frame, kUnroll independent loads at a time; the
+// kSlices lanes of a frame then fold their sums.
 //
 // Arithmetic. Sums are FP32 products accumulated in short plain-FP32 blocks
 // (at most kFlush terms per lane) that are folded into a double-word (hi, lo)
@@ -42,9 +43,11 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kFramesPerPass = 4;
-constexpr int kFlush = 16;
-constexpr int kUnroll = 4;  // entries per lane per step; kFlush is a multiple
+constexpr int kFlush = 16;  // terms per lane between double-word folds
+// Gather lane mappings a plan chooses from (launch_gather), as
+// (entry slices per frame group, frames per lane, entries per lane per step):
+// 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2).
+constexpr int kVariantCount = 5;
 constexpr int kSegMax = 1024;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
@@ -128,14 +131,50 @@ __device__ __forceinline__ float row_origin(const float4 *__restrict__ entry_std
     return __fdiv_rn(s, e.z);
 }
 
-// One CTA per unit; see the file comment.
-template <int MODE, typename P>
+// Reduce-scatter of V values (a power of two, <= 32) across the 32 lanes of
+// a warp by a fixed butterfly: after the call, lanes 2i and 2i+1 (V = 16),
+// or lanes with (lane >> log2(32/V)) == i in general, hold value i summed over
+// all lanes. IEEE addition is commutative, so the result does not depend on
+// which partner adds which.
+template <int V>
+__device__ __forceinline__ double reduce_scatter(double (&v)[V], int lane) {
+    int cur = V;
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        if (cur > 1) {
+            const bool hi = (lane & m) != 0;
+            const int half = cur / 2;
+#pragma unroll
+            for (int i = 0; i < V / 2; ++i) {
+                if (i < half) {
+                    const double send = hi ? v[i] : v[i + half];
+                    const double keep = hi ? v[i + half] : v[i];
+                    v[i] = __dadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, m));
+                }
+            }
+            cur = half;
+        } else {
+            v[0] = __dadd_rn(v[0], __shfl_xor_sync(0xffffffffu, v[0], m));
+        }
+    }
+    return v[0];
+}
+
+// One CTA per unit; see the file comment. Template parameters choose the
+// lane mapping: SLICES lanes split a segment's entries (lane sl takes entries
+// sl, sl + SLICES, ...), 32 / SLICES lane groups take different frames, and
+// each lane carries FPL frames, so a task is (segment, 32 / SLICES * FPL
+// frames). U entries per lane per step have all their loads in flight.
+template <int MODE, typename P, int SLICES, int FPL, int U>
 __global__ void __launch_bounds__(kThreads)
     k_gather(const int2 *__restrict__ units, const int4 *__restrict__ segs,
              const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
              const int32_t *__restrict__ first_valid, const P *__restrict__ frames,
              int64_t n_pixels, int n_frames, int n_segments, double *__restrict__ partial) {
     constexpr int NA = NAcc<MODE, P>::value;
+    constexpr int GROUPS = 32 / SLICES;         // frame lane groups per warp
+    constexpr int TASK_FRAMES = GROUPS * FPL;  // frames per task
+    static_assert(kFlush % U == 0, "flush cadence must be a multiple of the unroll");
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_off[kWarps + 1];
     const int2 un = units[blockIdx.x];
@@ -165,59 +204,68 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
 
-    const int groups = (n_frames + kFramesPerPass - 1) / kFramesPerPass;
-    const int tasks = groups * nseg;
+    const int sl = lane % SLICES, fg = lane / SLICES;
+    const int groups = (n_frames + TASK_FRAMES - 1) / TASK_FRAMES;
+    int grp = 0, si = warp;
     // Frame-major task order: the CTA's warps work on the same frames at once.
-    for (int task = warp; task < tasks; task += kWarps) {
-        const int grp = task / nseg, si = task - grp * nseg;
+    for (;; si += kWarps) {
+        while (si >= nseg) {
+            si -= nseg;
+            ++grp;
+        }
+        if (grp >= groups) break;
         const int4 sg = segs[seg0 + si];
         const int row = sg.x, len = sg.z - sg.y, off = s_off[si];
-        const int f0 = grp * kFramesPerPass;
-        const P *fr[kFramesPerPass];
-        bool fv[kFramesPerPass];
+        const int fbase = grp * TASK_FRAMES + fg * FPL;
+        const P *fr[FPL];
+        bool fv[FPL];
 #pragma unroll
-        for (int q = 0; q < kFramesPerPass; ++q) {
-            fv[q] = f0 + q < n_frames;
-            fr[q] = frames + int64_t(fv[q] ? f0 + q : f0) * n_pixels;
+        for (int q = 0; q < FPL; ++q) {
+            fv[q] = fbase + q < n_frames;
+            fr[q] = frames + int64_t(fv[q] ? fbase + q : 0) * n_pixels;
         }
-        float origin[kFramesPerPass];
-        if (MODE == kSpread) {
-            const int fvi = first_valid[row];
+        float origin[FPL];
 #pragma unroll
-            for (int q = 0; q < kFramesPerPass; ++q)
-                origin[q] = row_origin<P>(entry_std, fvi, sg.w, fr[q]);
-        }
-        AccDW acc[kFramesPerPass][NA];
+        for (int q = 0; q < FPL; ++q)
+            origin[q] = MODE == kSpread ? row_origin<P>(entry_std, first_valid[row], sg.w, fr[q])
+                                        : 0.f;
+        AccDW acc[FPL][NA];
 #pragma unroll
-        for (int q = 0; q < kFramesPerPass; ++q)
+        for (int q = 0; q < FPL; ++q)
 #pragma unroll
             for (int a = 0; a < NA; ++a) acc[q][a].zero();
 
-        // kUnroll entries per lane per step: all their pixel loads are issued
-        // before any is used. Slots past the end read pixel 0 with weight 0.
-        int since = 0;
-        for (int j0 = lane; j0 < len; j0 += 32 * kUnroll) {
+        // One step: U entries of this lane, all loads issued before use.
+        // CHECK is true only for the last, partial step, whose entries past
+        // the segment end contribute zero without touching the frame.
+        auto step = [&](int j0, auto check) {
+            constexpr bool CHECK = decltype(check)::value;
             if (MODE == kSpread) {
-                float4 e[kUnroll];
+                float4 e[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    const int j = j0 + 32 * u;
-                    e[u] = j < len ? reinterpret_cast<const float4 *>(smem)[off + j]
-                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int u = 0; u < U; ++u) {
+                    const int j = j0 + SLICES * u;
+                    if (CHECK)
+                        e[u] = j < len ? reinterpret_cast<const float4 *>(smem)[off + j]
+                                       : make_float4(0.f, 0.f, 1.f, 0.f);
+                    else
+                        e[u] = reinterpret_cast<const float4 *>(smem)[off + j];
                 }
-                float s[kUnroll][kFramesPerPass];
+                float sv[U][FPL];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int q = 0; q < kFramesPerPass; ++q)
-                        s[u][q] = load_px<P>(fr[q], uint32_t(__float_as_int(e[u].x)));
+                    for (int q = 0; q < FPL; ++q)
+                        sv[u][q] = !CHECK || j0 + SLICES * u < len
+                                       ? load_px<P>(fr[q], uint32_t(__float_as_int(e[u].x)))
+                                       : 0.f;
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     const float c = e[u].y, n = e[u].z, cr = e[u].w;
                     const float c2 = __fmul_rn(c, c);
 #pragma unroll
-                    for (int q = 0; q < kFramesPerPass; ++q) {
-                        float v = s[u][q];
+                    for (int q = 0; q < FPL; ++q) {
+                        const float v = sv[u][q];
                         if (is_float_px<P>() && !isfinite(v)) {
                             acc[q][NA - 2].add(__fmul_rn(c, n));
                             acc[q][NA - 1].add(c > 0.f ? 1.f : 0.f);
@@ -230,64 +278,97 @@ __global__ void __launch_bounds__(kThreads)
                     }
                 }
             } else {
-                int2 e[kUnroll];
+                int2 e[U];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    const int j = j0 + 32 * u;
-                    e[u] = j < len ? reinterpret_cast<const int2 *>(smem)[off + j] : make_int2(0, 0);
+                for (int u = 0; u < U; ++u) {
+                    const int j = j0 + SLICES * u;
+                    if (CHECK)
+                        e[u] = j < len ? reinterpret_cast<const int2 *>(smem)[off + j]
+                                       : make_int2(0, 0);
+                    else
+                        e[u] = reinterpret_cast<const int2 *>(smem)[off + j];
                 }
-                float s[kUnroll][kFramesPerPass];
+                float sv[U][FPL];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                    for (int q = 0; q < kFramesPerPass; ++q)
-                        s[u][q] = load_px<P>(fr[q], uint32_t(e[u].x));
+                    for (int q = 0; q < FPL; ++q)
+                        sv[u][q] = !CHECK || j0 + SLICES * u < len
+                                       ? load_px<P>(fr[q], uint32_t(e[u].x))
+                                       : 0.f;
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
+                for (int u = 0; u < U; ++u) {
                     const float c = __int_as_float(e[u].y);
+                    const float c2 = __fmul_rn(c, c);
 #pragma unroll
-                    for (int q = 0; q < kFramesPerPass; ++q) {
-                        acc[q][0].fma(c, s[u][q]);
+                    for (int q = 0; q < FPL; ++q) {
+                        acc[q][0].fma(c, sv[u][q]);
                         if (MODE == kErrors)
-                            acc[q][1].fma(__fmul_rn(c, c),
-                                          is_unsigned_px<P>() ? s[u][q] : fmaxf(s[u][q], 0.f));
+                            acc[q][1].fma(c2, is_unsigned_px<P>() ? sv[u][q] : fmaxf(sv[u][q], 0.f));
                     }
                 }
             }
-            since += kUnroll;
+        };
+        int since = 0;
+        const int full = len / (SLICES * U) * (SLICES * U);
+        int j0 = sl;
+        for (; j0 < full; j0 += SLICES * U) {
+            step(j0, std::false_type{});
+            since += U;
             if (since == kFlush) {
                 since = 0;
 #pragma unroll
-                for (int q = 0; q < kFramesPerPass; ++q)
+                for (int q = 0; q < FPL; ++q)
 #pragma unroll
                     for (int a = 0; a < NA; ++a) acc[q][a].flush();
             }
         }
+        if (full < len) step(j0, std::true_type{});
 #pragma unroll
-        for (int q = 0; q < kFramesPerPass; ++q)
+        for (int q = 0; q < FPL; ++q)
 #pragma unroll
             for (int a = 0; a < NA; ++a) acc[q][a].flush();
-        // Each lane's double-word sum is exact in FP64; the lanes are then
-        // folded by a fixed FP64 tree: lane i takes lane i + o for o = 16..1.
-        double d[kFramesPerPass][NA];
+
+        // Each lane's double-word sums are exact in FP64; the SLICES lanes of
+        // a frame group are added by a fixed tree.
+        if constexpr (SLICES == 32) {
+            constexpr int V0 = FPL * NA;
+            constexpr int V = V0 <= 1 ? 1 : V0 <= 2 ? 2 : V0 <= 4 ? 4 : V0 <= 8 ? 8 : V0 <= 16 ? 16 : 32;
+            double d[V];
 #pragma unroll
-        for (int q = 0; q < kFramesPerPass; ++q)
+            for (int i = 0; i < V; ++i) d[i] = 0.0;
 #pragma unroll
-            for (int a = 0; a < NA; ++a) d[q][a] = double(acc[q][a].hi) + double(acc[q][a].lo);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int q = 0; q < kFramesPerPass; ++q)
+            for (int q = 0; q < FPL; ++q)
 #pragma unroll
                 for (int a = 0; a < NA; ++a)
-                    d[q][a] = __dadd_rn(d[q][a], __shfl_down_sync(0xffffffffu, d[q][a], o));
-        if (lane == 0) {
+                    d[q * NA + a] = double(acc[q][a].hi) + double(acc[q][a].lo);
+            const double mine = reduce_scatter<V>(d, lane);
+            const int idx = lane / (32 / V);
+            if (lane % (32 / V) == 0 && idx < V0) {
+                const int q = idx / NA, a = idx % NA;
+                if (fbase + q < n_frames)
+                    partial[(int64_t(fbase + q) * n_segments + seg0 + si) * NA + a] = mine;
+            }
+        } else {
+            double d[FPL][NA];
 #pragma unroll
-            for (int q = 0; q < kFramesPerPass; ++q) {
-                if (!fv[q]) continue;
-                double *out = partial + (int64_t(f0 + q) * n_segments + seg0 + si) * NA;
+            for (int q = 0; q < FPL; ++q)
 #pragma unroll
-                for (int a = 0; a < NA; ++a) out[a] = d[q][a];
+                for (int a = 0; a < NA; ++a) {
+                    double x = double(acc[q][a].hi) + double(acc[q][a].lo);
+#pragma unroll
+                    for (int o = SLICES / 2; o > 0; o >>= 1)
+                        x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));
+                    d[q][a] = x;
+                }
+            if (sl == 0) {
+#pragma unroll
+                for (int q = 0; q < FPL; ++q) {
+                    if (!fv[q]) continue;
+                    double *out = partial + (int64_t(fbase + q) * n_segments + seg0 + si) * NA;
+#pragma unroll
+                    for (int a = 0; a < NA; ++a) out[a] = d[q][a];
+                }
             }
         }
     }
@@ -408,26 +489,33 @@ __global__ void k_strip_bounds(const int64_t *__restrict__ row_ptr, int n_rows,
     }
 }
 
+// Launches lane-mapping variant `variant` of the gather (kVariantCount) with
+// its partial sums in `partial`.
+template <int MODE, typename P>
+void launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pixels, int nf,
+                   double *partial, cudaStream_t s) {
+    const size_t smem = size_t(t.unit_cap) * (MODE == kSpread ? 16 : 8);
+#define DG_GATHER_ARGS                                                                        \
+    t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp, n_pixels, nf, \
+        t.n_segments, partial
+    switch (variant) {
+    case 0: k_gather<MODE, P, 32, 4, 4><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
+    case 1: k_gather<MODE, P, 32, 2, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
+    case 2: k_gather<MODE, P, 8, 2, 4><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
+    case 3: k_gather<MODE, P, 4, 1, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
+    default: k_gather<MODE, P, 16, 4, 2><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
+    }
+#undef DG_GATHER_ARGS
+    DG_CUDA(cudaGetLastError());
+}
+
 template <typename P>
 void launch_typed(GatherTable &t, const void *frames, int64_t n_pixels, int n_frames, int mode,
                   cudaStream_t s) {
-    const size_t smem = size_t(t.unit_cap) * (mode == kSpread ? 16 : 8);
     const P *fp = static_cast<const P *>(frames);
-    const int32_t *fv = t.first_valid.ptr;
-    if (mode == kSpread) {
-        k_gather<kSpread, P><<<t.n_units, kThreads, smem, s>>>(
-            t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, fv, fp, n_pixels, n_frames,
-            t.n_segments, t.partial.ptr);
-    } else if (mode == kErrors) {
-        k_gather<kErrors, P><<<t.n_units, kThreads, smem, s>>>(
-            t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, fv, fp, n_pixels, n_frames,
-            t.n_segments, t.partial.ptr);
-    } else {
-        k_gather<kIntensity, P><<<t.n_units, kThreads, smem, s>>>(
-            t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, fv, fp, n_pixels, n_frames,
-            t.n_segments, t.partial.ptr);
-    }
-    DG_CUDA(cudaGetLastError());
+    if (mode == kSpread) launch_gather<kSpread, P>(t, t.variant, fp, n_pixels, n_frames, t.partial.ptr, s);
+    else if (mode == kErrors) launch_gather<kErrors, P>(t, t.variant, fp, n_pixels, n_frames, t.partial.ptr, s);
+    else launch_gather<kIntensity, P>(t, t.variant, fp, n_pixels, n_frames, t.partial.ptr, s);
 }
 
 template <int MODE, typename P>
@@ -615,6 +703,73 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
     }
 }
 
+namespace {
+
+template <typename P>
+void launch_mode(GatherTable &t, int variant, int mode, const void *frames, int64_t n_pixels,
+                 int nf, cudaStream_t s) {
+    const P *fp = static_cast<const P *>(frames);
+    if (mode == kSpread) launch_gather<kSpread, P>(t, variant, fp, n_pixels, nf, t.partial.ptr, s);
+    else if (mode == kErrors) launch_gather<kErrors, P>(t, variant, fp, n_pixels, nf, t.partial.ptr, s);
+    else launch_gather<kIntensity, P>(t, variant, fp, n_pixels, nf, t.partial.ptr, s);
+}
+
+}  // namespace
+
+int gather_variant_count() { return kVariantCount; }
+
+int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
+                    int64_t n_frames, uint32_t flags, cudaStream_t s,
+                    std::vector<double> *each) {
+    if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
+    if (n_frames <= 0) fail(DG_INVALID_INPUT, "autotuning needs at least one frame");
+    const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
+                                                                                : kIntensity;
+    const int nf = int(std::min<int64_t>(n_frames, 256));
+    const int64_t need = std::max<int64_t>(1, t.n_segments) * 256 * 5;
+    if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+    if (each) each->assign(size_t(kVariantCount), 0.0);
+    if (t.n_units == 0) return t.variant;
+    cudaEvent_t a = nullptr, b = nullptr;
+    DG_CUDA(cudaEventCreate(&a));
+    DG_CUDA(cudaEventCreate(&b));
+    int best = t.variant;
+    float best_t = 3.4e38f;
+    try {
+        for (int v = 0; v < kVariantCount; ++v) {
+            float vt = 3.4e38f;
+            for (int rep = 0; rep < 4; ++rep) {
+                DG_CUDA(cudaEventRecord(a, s));
+                switch (dtype) {
+                case DG_U16: launch_mode<uint16_t>(t, v, mode, d_frames, n_pixels, nf, s); break;
+                case DG_U32: launch_mode<uint32_t>(t, v, mode, d_frames, n_pixels, nf, s); break;
+                case DG_I32: launch_mode<int32_t>(t, v, mode, d_frames, n_pixels, nf, s); break;
+                case DG_F32: launch_mode<float>(t, v, mode, d_frames, n_pixels, nf, s); break;
+                case DG_F64: launch_mode<double>(t, v, mode, d_frames, n_pixels, nf, s); break;
+                }
+                DG_CUDA(cudaEventRecord(b, s));
+                DG_CUDA(cudaEventSynchronize(b));
+                float ms = 0.f;
+                DG_CUDA(cudaEventElapsedTime(&ms, a, b));
+                if (rep > 0 && ms < vt) vt = ms;  // first launch warms caches
+            }
+            if (each) (*each)[size_t(v)] = vt;
+            if (vt < best_t) {
+                best_t = vt;
+                best = v;
+            }
+        }
+    } catch (...) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        throw;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    t.variant = best;
+    return best;
+}
+
 }  // namespace dg
 
 // ---------------------------------------------------------------------------
@@ -671,20 +826,9 @@ void noalloc_launch(const GatherTable &t, double *partial, const void *frames, i
                     int nf, int mode, double *oi, double *os, double *od, cudaStream_t s) {
     const P *fp = static_cast<const P *>(frames);
     if (t.n_units > 0) {
-        const size_t smem = size_t(t.unit_cap) * (mode == kSpread ? 16 : 8);
-        if (mode == kSpread)
-            k_gather<kSpread, P><<<t.n_units, kThreads, smem, s>>>(
-                t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp,
-                n_pixels, nf, t.n_segments, partial);
-        else if (mode == kErrors)
-            k_gather<kErrors, P><<<t.n_units, kThreads, smem, s>>>(
-                t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp,
-                n_pixels, nf, t.n_segments, partial);
-        else
-            k_gather<kIntensity, P><<<t.n_units, kThreads, smem, s>>>(
-                t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp,
-                n_pixels, nf, t.n_segments, partial);
-        DG_CUDA(cudaGetLastError());
+        if (mode == kSpread) launch_gather<kSpread, P>(t, t.variant, fp, n_pixels, nf, partial, s);
+        else if (mode == kErrors) launch_gather<kErrors, P>(t, t.variant, fp, n_pixels, nf, partial, s);
+        else launch_gather<kIntensity, P>(t, t.variant, fp, n_pixels, nf, partial, s);
     }
     if (t.n_rows > 0) {
         const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);

@@ -171,6 +171,7 @@ struct GatherTable {
     DeviceArray<double> den_f32;      // the same sum over the FP32-rounded c and n
     DeviceArray<int32_t> valid_std;   // entries valid for the spread, per row
     DeviceArray<double> partial;      // scratch: per (frame, segment) FP64 sums
+    int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
     bool profile = false;
     EventPool events;
@@ -190,6 +191,13 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
                 double *d_std, cudaStream_t stream);
 // Number of gather kernel launches run_gather enqueues (for launch counting).
 int gather_launches_per_call();
+// Lane-mapping variants of the gather, and the per-plan autotuner: times each
+// variant's gather launch on the given frames and keeps the fastest in
+// t.variant (returned; `each` receives every variant's time in ms).
+int gather_variant_count();
+int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
+                    int64_t n_frames, uint32_t flags, cudaStream_t stream,
+                    std::vector<double> *each);
 
 // Exclusive scans (dg_scan.cu). `temp` sizing via scan_temp_bytes.
 size_t scan_temp_bytes(int64_t n);

@@ -222,6 +222,42 @@ class Cuda1dPlan:
                                      _dp(oi), _dp(os_), _dp(od)))
         return oi, os_, od
 
+    def autotune(self, frames, *, errors: bool = False, azimuthal_std: bool = False):
+        """Time every lane mapping of the gather on `frames` (a CUDA tensor
+        of shape (n, dim1, dim2) on the plan's device) and keep the fastest
+        for this plan. Returns (mapping index, [launch ms of every mapping])."""
+        if getattr(frames, "is_cuda", False) is not True:
+            raise TypeError("autotune takes device-resident frames (a CUDA tensor)")
+        import torch
+        codes = {torch.uint16: 0, torch.uint32: 1, torch.int32: 2, torch.float32: 3,
+                 torch.float64: 4}
+        if frames.dtype not in codes:
+            raise TypeError(f"unsupported dtype {frames.dtype}")
+        frames = frames.contiguous()
+        if tuple(frames.shape[-2:]) != self.shape:
+            raise ValueError(f"frames of shape {tuple(frames.shape[-2:])} do not match plan "
+                             f"{self.shape}")
+        n = frames.numel() // (self.shape[0] * self.shape[1])
+        flags = (N.DG_ERRORS if errors else 0) | (N.DG_AZIMUTHAL_STD if azimuthal_std else 0)
+        count = C.c_int32(0)
+        N.check(N.lib().dg_plan_variant(self._h, -1, None, C.byref(count)))
+        v, ms = C.c_int32(0), (C.c_double * count.value)()
+        stream = torch.cuda.current_stream(frames.device).cuda_stream
+        N.check(N.lib().dg_plan_autotune(self._h, C.c_void_p(frames.data_ptr()),
+                                         codes[frames.dtype], n, flags, C.c_void_p(stream),
+                                         C.byref(v), ms, count.value))
+        return v.value, list(ms)
+
+    @property
+    def gather_variant(self) -> int:
+        cur = C.c_int32(0)
+        N.check(N.lib().dg_plan_variant(self._h, -1, C.byref(cur), None))
+        return cur.value
+
+    @gather_variant.setter
+    def gather_variant(self, v: int) -> None:
+        N.check(N.lib().dg_plan_variant(self._h, int(v), None, None))
+
     def integrate1d(self, image: np.ndarray, *, errors: bool = False,
                     azimuthal_std: bool = False) -> IntegrationResult:
         a = _frame_array(image)

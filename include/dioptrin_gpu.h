@@ -182,6 +182,26 @@ DG_EXPORT dg_status dg_plan_profile(dg_plan *plan, int32_t enable);
 DG_EXPORT dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *gather_ms,
                                         int64_t *gather_launches, int64_t *launches);
 
+/* Per-plan autotuner of the gather's launch shape; it has no counterpart in
+ * the reference, whose gather kernels run one fixed shape
+ * (src/integration/cuda/device.rs). The gather has several lane mappings
+ * (entry slices per frame group, frames per lane, entries in flight per
+ * lane). dg_plan_autotune times each on up to 256 of the given DEVICE frames
+ * (dtype, flags as dg_integrate_device) on `stream` (NULL: the plan's own),
+ * keeps the fastest for every later call of the plan and returns it in
+ * *variant (may be NULL); ms (may be NULL) receives the launch time of each
+ * mapping in mapping order, n_ms entries at most.
+ * Synchronous. The mappings round differently within the stated tolerance;
+ * one plan's results are reproducible between calls made with the same
+ * mapping. dg_plan_variant reads the plan's mapping into *current and the
+ * number of mappings into *count (either may be NULL) and, when set >= 0,
+ * selects mapping `set` first. */
+DG_EXPORT dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                     int64_t n_frames, uint32_t flags, void *stream,
+                                     int32_t *variant, double *ms, int32_t n_ms);
+DG_EXPORT dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current,
+                                    int32_t *count);
+
 /* Evaluates one FP64 primitive of the device table builders on n values in
  * DEVICE memory of the current device, for parity checks against the C
  * library the reference calls (f64::atan2 and f64::sin, geometry.rs:684-692,

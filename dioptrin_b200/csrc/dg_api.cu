@@ -34,7 +34,7 @@ thread_local std::string g_last_error;
 // Detector rows per gather strip (see dg_gather.cu): small enough that a
 // unit's bins cover a few kilobytes of each frame, large enough that a bin's
 // ring is cut into few segments.
-constexpr int32_t kStripRows = 128;
+constexpr int32_t kStripRows = 32;
 
 }  // namespace
 
@@ -152,6 +152,18 @@ void check_frames(const dg_plan *plan, const void *frames, int32_t dtype, int64_
     }
 }
 
+// Device arrays must be aligned to their element size (the kernels load
+// pixels with naturally aligned loads and asynchronous 4-byte copies).
+void check_device_alignment(const void *frames, int32_t dtype, const void *oi, const void *os,
+                            const void *od) {
+    const uintptr_t es = uintptr_t(dtype_size(dtype));
+    if (reinterpret_cast<uintptr_t>(frames) % es)
+        dg::fail(DG_INVALID_INPUT, "device frames must be aligned to the pixel size");
+    for (const void *o : {oi, os, od})
+        if (reinterpret_cast<uintptr_t>(o) % 8)
+            dg::fail(DG_INVALID_INPUT, "device outputs must be 8-byte aligned");
+}
+
 }  // namespace
 
 int64_t dg_plan::device_bytes() const {
@@ -163,7 +175,9 @@ int64_t dg_plan::device_bytes() const {
          gather.seg_ids.bytes() + gather.first_valid.bytes() + gather.entry.bytes() +
          gather.entry_std.bytes() + gather.den.bytes() + gather.den_std.bytes() +
          gather.den_f32.bytes() +
-         gather.valid_std.bytes() + gather.partial.bytes();
+         gather.valid_std.bytes() + gather.partial.bytes() + gather.fl_unit.bytes() +
+         gather.fl_px.bytes() + gather.fl_pair_a.bytes() + gather.fl_pair_b.bytes() +
+         gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes();
     b += stage_in.bytes() + stage_out.bytes();
     return b;
 }
@@ -351,6 +365,7 @@ dg_status dg_integrate_device(dg_plan *plan, const void *d_frames, int32_t dtype
     return guarded([&] {
         check_frames(plan, d_frames, dtype, n_frames, flags, d_i, d_s, d_d);
         if (n_frames == 0) return;
+        check_device_alignment(d_frames, dtype, d_i, d_s, d_d);
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
@@ -366,6 +381,7 @@ dg_status dg_integrate_device_plain(dg_plan *plan, const void *d_frames, int32_t
     return guarded([&] {
         check_frames(plan, d_frames, dtype, n_frames, flags, d_i, d_s, d_d);
         if (n_frames == 0) return;
+        check_device_alignment(d_frames, dtype, d_i, d_s, d_d);
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
@@ -452,6 +468,7 @@ dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype, i
             dg::fail(DG_INVALID_INPUT, "autotuning needs device frames (n_frames >= 1)");
         if ((flags & DG_AZIMUTHAL_STD) && plan->n_azimuthal != 0)
             dg::fail(DG_UNSUPPORTED, "azimuthal_std is defined for 1D tables only");
+        check_device_alignment(d_frames, dtype, nullptr, nullptr, nullptr);
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
@@ -470,6 +487,9 @@ dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current, int32_t 
         std::lock_guard<std::mutex> lock(plan->mu);
         if (set >= dg::gather_variant_count())
             dg::fail(DG_INVALID_INPUT, "gather mapping " + std::to_string(set) + " does not exist");
+        if (set >= 0 && !dg::gather_variant_available(plan->gather, set))
+            dg::fail(DG_UNSUPPORTED, "gather mapping " + std::to_string(set) +
+                                         " is not available for this plan");
         if (set >= 0) plan->gather.variant = set;
         if (current) *current = plan->gather.variant;
         if (count) *count = dg::gather_variant_count();

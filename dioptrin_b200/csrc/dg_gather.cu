@@ -34,6 +34,7 @@
 // S - o*sum(c*n) and is formed once per row in the finalize, and
 // m2 = B - A^2 / sum(w).
 #include <algorithm>
+#include <climits>
 #include <type_traits>
 
 #include "dg_internal.h"
@@ -44,11 +45,13 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kFlush = 16;  // terms per lane between double-word folds
-// Gather lane mappings a plan chooses from (launch_gather), as
-// (entry slices per frame group, frames per lane, entries per lane per step):
-// 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2).
-constexpr int kVariantCount = 5;
-constexpr int kSegMax = 1024;
+// Gather lane mappings a plan chooses from (launch_gather). Entry-lane
+// mappings, as (entry slices per frame group, frames per lane, entries per
+// lane per step): 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2);
+// frame-lane mappings (k_gather_fl), 2 CTAs per SM (5) or 1 CTA per SM with
+// the next frames prefetched while the current ones are summed (6).
+constexpr int kVariantCount = 7;
+constexpr int kSegMax = 256;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
 enum Mode { kIntensity = 0, kErrors = 1, kSpread = 2 };
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(kThreads)
             if (lane % (32 / V) == 0 && idx < V0) {
                 const int q = idx / NA, a = idx % NA;
                 if (fbase + q < n_frames)
-                    partial[(int64_t(fbase + q) * n_segments + seg0 + si) * NA + a] = mine;
+                    partial[(int64_t(seg0 + si) * NA + a) * n_frames + fbase + q] = mine;
             }
         } else {
             double d[FPL][NA];
@@ -365,10 +368,522 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
                 for (int q = 0; q < FPL; ++q) {
                     if (!fv[q]) continue;
-                    double *out = partial + (int64_t(fbase + q) * n_segments + seg0 + si) * NA;
 #pragma unroll
-                    for (int a = 0; a < NA; ++a) out[a] = d[q][a];
+                    for (int a = 0; a < NA; ++a)
+                        partial[(int64_t(seg0 + si) * NA + a) * n_frames + fbase + q] = d[q][a];
                 }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Frame-lane gather. Lane = frame: for 32 frames at a time, a unit's distinct
+// pixels (at most kFlDCap, listed at plan time) are staged in shared memory,
+// 4-byte pixel types by cp.async and the others converted to FP32 on the way,
+// frame rows kFlStride words apart (odd, so the 32 lanes reading one pixel of
+// their own frames hit 32 banks). Every lane of a warp walks the same entries
+// against its own frame, so a frame's sums need no cross-lane reduction.
+//
+// Entries go in pairs, {index 0, index 1, c0, c1} and for the spread
+// {n0, n1, c0/n0, c1/n1}, their columns rewritten at plan time as indices
+// into the unit's pixel list; a segment of odd length ends with a padding
+// entry of weight 0 whose index names column kFlDCap, which staging never
+// writes and which holds 0. Sums use packed FP32x2 arithmetic: the even
+// entries of a segment accumulate in one half, the odd ones in the other,
+// each in a double-word accumulator folded every kFlFlushPairs pairs.
+//
+// A unit's pairs are cut into kWarps equal pieces, one per warp. A segment
+// inside one piece is written straight to the partial sums; a piece's first
+// and last segments go to shared-memory slots, and the slots of a segment
+// cut by piece boundaries are added in warp order. Results depend on the
+// table alone, not on the frames around them in a batch.
+
+constexpr int kFlSegs = 32;               // segments per frame-lane unit, at most
+constexpr int kFlECap = 1152;             // entries per frame-lane unit before padding
+constexpr int kFlDCap = 576;              // distinct pixels per frame-lane unit
+constexpr int kFlPairCap = (kFlECap + kFlSegs) / 2;
+constexpr int kFlStride = kFlDCap + 1;    // odd; column kFlDCap stays 0
+constexpr int kFlSlots = 2 * kWarps;      // first and last segment of each piece
+constexpr int kFlFlushPairs = 16;         // pairs per lane between double-word folds
+constexpr int kFlSortMax = 2048;          // keys one unit sorts at plan time
+static_assert(kFlECap + kFlSegs <= kFlSortMax, "frame-lane units must fit the plan-time sort");
+static_assert(kFlSegs <= 32, "the unit set-up scans segment lengths in one warp");
+static_assert(kSegMax <= kFlDCap, "a single segment must fit a frame-lane unit");
+
+template <typename P>
+using StagedPx = typename std::conditional<sizeof(P) == 4, P, float>::type;
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Packed FP32x2 arithmetic (round to nearest, per element as the scalar
+// operations).
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk(float a, float b) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 upk(f2 v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// Two double-word FP32 accumulators (even and odd entries) with a plain
+// FP32 block in front; the fold is AccDW::flush on each half.
+struct Acc2 {
+    f2 p, hi, lo;
+    __device__ __forceinline__ void zero() { p = hi = lo = 0ull; }
+    __device__ __forceinline__ void flush() {
+        const f2 s = add2(hi, p);
+        const f2 bp = sub2(s, hi);
+        const f2 e = add2(sub2(hi, sub2(s, bp)), sub2(p, bp));
+        hi = s;
+        lo = add2(lo, e);
+        p = 0ull;
+    }
+    // Both halves' exact sums added in FP64 (even + odd).
+    __device__ __forceinline__ double value() const {
+        const float2 h = upk(hi), l = upk(lo);
+        return __dadd_rn(double(h.x) + double(l.x), double(h.y) + double(l.y));
+    }
+};
+
+// Dynamic shared memory of k_gather_fl: entry pairs, pixel list, one or
+// (double-buffered) two sets of 32 frame rows, piece-boundary slots.
+template <int MODE, typename P, bool DB>
+constexpr size_t fl_smem_bytes() {
+    return size_t(kFlPairCap) * (MODE == kSpread ? 32 : 16) + size_t(kFlDCap) * 4 +
+           size_t(DB ? 64 : 32) * kFlStride * 4 + size_t(kFlSlots) * NAcc<MODE, P>::value * 32 * 8;
+}
+
+template <int MODE, typename P, int U2, bool DB>
+__global__ void __launch_bounds__(kThreads, DB ? 1 : 2)
+    k_gather_fl(const int4 *__restrict__ units, const int4 *__restrict__ segs,
+                const int32_t *__restrict__ unit_px, const float4 *__restrict__ pair_a,
+                const float4 *__restrict__ pair_b, const float4 *__restrict__ entry_std,
+                const int32_t *__restrict__ first_valid, const int32_t *__restrict__ seg_org,
+                const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_segments,
+                double *__restrict__ partial) {
+    using S = StagedPx<P>;
+    constexpr int NA = NAcc<MODE, P>::value;
+    constexpr bool SPREAD = MODE == kSpread;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_off[kFlSegs + 1], s_first[kFlSegs], s_rend[kFlSegs], s_oidx[kFlSegs];
+    __shared__ float s_on[kFlSegs];
+    __shared__ int s_sa[kWarps], s_sb[kWarps];
+    __shared__ int s_nb, s_bseg[kFlSlots], s_bwlo[kFlSlots], s_bwhi[kFlSlots];
+    float4 *s_pa = reinterpret_cast<float4 *>(smem);
+    float4 *s_pb = s_pa + kFlPairCap;
+    int32_t *s_px = reinterpret_cast<int32_t *>(smem + size_t(kFlPairCap) * (SPREAD ? 32 : 16));
+    S *s_buf = reinterpret_cast<S *>(s_px + kFlDCap);
+    double *s_red = reinterpret_cast<double *>(s_buf + (DB ? 64 : 32) * kFlStride);
+
+    const int4 un = units[blockIdx.x];
+    const int seg0 = un.x, nseg = un.y, D = un.w;
+    const int64_t poff = un.z;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (warp == 0) {
+        int plen = 0;
+        if (lane < nseg) {
+            const int4 sg = segs[seg0 + lane];
+            plen = (sg.z - sg.y + 1) & ~1;
+            const int first = first_valid[sg.x];
+            s_first[lane] = first;
+            s_rend[lane] = sg.w;
+            if (SPREAD) {
+                s_oidx[lane] = seg_org[seg0 + lane];
+                s_on[lane] = first >= 0 ? entry_std[first].z : 1.f;
+            }
+        }
+        int inc = plen;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane < nseg) s_off[lane + 1] = inc;
+        if (lane == 0) s_off[0] = 0;
+    }
+    __syncthreads();
+    const int np = s_off[nseg] >> 1;
+    for (int j = tid; j < np; j += kThreads) {
+        s_pa[j] = pair_a[poff + j];
+        if (SPREAD) s_pb[j] = pair_b[poff + j];
+    }
+    for (int j = tid; j < D; j += kThreads) s_px[j] = unit_px[int64_t(blockIdx.x) * kFlDCap + j];
+    for (int j = tid; j < (DB ? 64 : 32) * kFlStride; j += kThreads) s_buf[j] = S(0);
+    // This warp's piece [lo, hi) (entries; pair aligned) and the segments
+    // sa..sb it meets.
+    const int lo = 2 * int(int64_t(warp) * np / kWarps);
+    const int hi = 2 * int(int64_t(warp + 1) * np / kWarps);
+    int sa = 0, sb = -1;
+    if (lo < hi) {
+        while (s_off[sa + 1] <= lo) ++sa;
+        sb = sa;
+        while (s_off[sb + 1] < hi) ++sb;
+    }
+    if (lane == 0) {
+        s_sa[warp] = sa;
+        s_sb[warp] = sb;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        // Segments at piece boundaries, ascending, with their warps.
+        int nb = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            if (s_sb[w] < 0) continue;
+            for (int e = 0; e < 2; ++e) {
+                const int b = e == 0 ? s_sa[w] : s_sb[w];
+                if (e == 1 && b == s_sa[w]) break;
+                if (nb > 0 && s_bseg[nb - 1] == b) {
+                    s_bwhi[nb - 1] = w;
+                } else {
+                    s_bseg[nb] = b;
+                    s_bwlo[nb] = w;
+                    s_bwhi[nb] = w;
+                    ++nb;
+                }
+            }
+        }
+        s_nb = nb;
+    }
+    __syncthreads();
+
+    // Stage pixel s_px[k] of frames f0.. into frame rows of `buf`; rows of
+    // frames past the end keep stale values (their lanes are never written
+    // out). 4-byte pixels are copied asynchronously as one commit group.
+    auto stage = [&](int f0, S *buf) {
+        const int nv = min(32, n_frames - f0);
+        for (int k = tid; k < D; k += kThreads) {
+            const P *src = frames + int64_t(f0) * n_pixels + s_px[k];
+            S *dst = buf + k;
+            if constexpr (sizeof(P) == 4) {
+#pragma unroll 8
+                for (int f = 0; f < nv; ++f) cp_async4(dst + f * kFlStride, src + int64_t(f) * n_pixels);
+            } else {
+#pragma unroll 8
+                for (int f = 0; f < nv; ++f)
+                    dst[f * kFlStride] = load_px<P>(src + int64_t(f) * n_pixels, 0u);
+            }
+        }
+        if constexpr (sizeof(P) == 4) asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    const int groups = (n_frames + 31) / 32;
+    if (DB) stage(0, s_buf);
+    for (int g = 0; g < groups; ++g) {
+        const int f0 = g * 32;
+        const int nv = min(32, n_frames - f0);
+        S *cur = DB && (g & 1) ? s_buf + 32 * kFlStride : s_buf;
+        if (!DB) {
+            stage(f0, cur);
+            if constexpr (sizeof(P) == 4) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        } else if (g + 1 < groups) {
+            // Prefetch the next group into the other buffer, last read by the
+            // previous group's compute (finished at its closing barrier).
+            stage(f0 + 32, (g & 1) ? s_buf : s_buf + 32 * kFlStride);
+            if constexpr (sizeof(P) == 4) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            if constexpr (sizeof(P) == 4) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+        const S *px = cur + lane * kFlStride;
+
+        for (int i = sa; i <= sb; ++i) {
+            const int p0 = max(lo, s_off[i]) >> 1, p1 = min(hi, s_off[i + 1]) >> 1;
+            // Origin o = s/n of the row's first valid entry (row_origin): its
+            // pixel is staged with the unit's; a non-finite float pixel there
+            // sends the lane to the row's next entries in global memory.
+            float org = 0.f;
+            if constexpr (SPREAD) {
+                const float so = float(px[s_oidx[i]]);
+                org = __fdiv_rn(so, s_on[i]);
+                if (is_float_px<P>() && !isfinite(so)) {
+                    const int fi = min(f0 + lane, n_frames - 1);
+                    org = row_origin<P>(entry_std, s_first[i], s_rend[i],
+                                        frames + int64_t(fi) * n_pixels);
+                }
+            }
+            const f2 norg = pk(-org, -org);
+            Acc2 acc[NA];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) acc[a].zero();
+
+            // UU pairs from p, all shared-memory reads issued before use.
+            auto body = [&](int p, auto unroll) {
+                constexpr int UU = decltype(unroll)::value;
+                float4 ea[UU], eb[UU];
+#pragma unroll
+                for (int u = 0; u < UU; ++u) {
+                    ea[u] = s_pa[p + u];
+                    if constexpr (SPREAD) eb[u] = s_pb[p + u];
+                }
+                float v0[UU], v1[UU];
+#pragma unroll
+                for (int u = 0; u < UU; ++u) {
+                    v0[u] = float(px[__float_as_int(ea[u].x)]);
+                    v1[u] = float(px[__float_as_int(ea[u].y)]);
+                }
+#pragma unroll
+                for (int u = 0; u < UU; ++u) {
+                    const f2 c = pk(ea[u].z, ea[u].w);
+                    if constexpr (SPREAD && is_float_px<P>()) {
+                      if (!(isfinite(v0[u]) && isfinite(v1[u]))) {
+                        // A non-finite pixel adds its weight c*n to the
+                        // spread's excluded sums instead (azimuthal.rs:68-70).
+                        const bool ok0 = isfinite(v0[u]), ok1 = isfinite(v1[u]);
+                        const float x0 = ok0 ? v0[u] : 0.f, x1 = ok1 ? v1[u] : 0.f;
+                        const f2 ce = pk(ok0 ? ea[u].z : 0.f, ok1 ? ea[u].w : 0.f);
+                        const f2 x = pk(x0, x1), n = pk(eb[u].x, eb[u].y);
+                        const f2 cre = pk(ok0 ? eb[u].z : 0.f, ok1 ? eb[u].w : 0.f);
+                        acc[0].p = fma2(ce, x, acc[0].p);
+                        acc[1].p = fma2(mul2(ce, ce), pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f)), acc[1].p);
+                        const f2 t = fma2(norg, n, x);
+                        acc[2].p = fma2(mul2(cre, t), t, acc[2].p);
+                        acc[NA - 2].p = add2(acc[NA - 2].p,
+                                             pk(ok0 ? 0.f : __fmul_rn(ea[u].z, eb[u].x),
+                                                ok1 ? 0.f : __fmul_rn(ea[u].w, eb[u].y)));
+                        acc[NA - 1].p = add2(acc[NA - 1].p, pk(!ok0 && ea[u].z > 0.f ? 1.f : 0.f,
+                                                               !ok1 && ea[u].w > 0.f ? 1.f : 0.f));
+                        continue;
+                      }
+                    }
+                    const f2 x = pk(v0[u], v1[u]);
+                    acc[0].p = fma2(c, x, acc[0].p);
+                    if constexpr (MODE != kIntensity) {
+                        const f2 xp = is_unsigned_px<P>()
+                                          ? x
+                                          : pk(fmaxf(v0[u], 0.f), fmaxf(v1[u], 0.f));
+                        acc[1].p = fma2(mul2(c, c), xp, acc[1].p);
+                    }
+                    if constexpr (SPREAD) {
+                        const f2 n = pk(eb[u].x, eb[u].y), cr = pk(eb[u].z, eb[u].w);
+                        const f2 t = fma2(norg, n, x);
+                        acc[2].p = fma2(mul2(cr, t), t, acc[2].p);
+                    }
+                }
+            };
+            int p = p0, since = 0;
+            for (; p + U2 <= p1; p += U2) {
+                body(p, std::integral_constant<int, U2>{});
+                since += U2;
+                if (since == kFlFlushPairs) {
+                    since = 0;
+#pragma unroll
+                    for (int a = 0; a < NA; ++a) acc[a].flush();
+                }
+            }
+            for (; p < p1; ++p) body(p, std::integral_constant<int, 1>{});
+            double val[NA];
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                acc[a].flush();
+                val[a] = acc[a].value();
+            }
+            if (i != sa && i != sb) {
+                if (lane < nv) {
+#pragma unroll
+                    for (int a = 0; a < NA; ++a)
+                        partial[(int64_t(seg0 + i) * NA + a) * n_frames + f0 + lane] = val[a];
+                }
+            } else {
+                const int slot = 2 * warp + (i == sa ? 0 : 1);
+#pragma unroll
+                for (int a = 0; a < NA; ++a) s_red[(slot * NA + a) * 32 + lane] = val[a];
+            }
+        }
+        __syncthreads();
+
+        // Segments at piece boundaries: their pieces added in warp order.
+        const int items = s_nb * NA * 32;
+        for (int idx = tid; idx < items; idx += kThreads) {
+            const int f = idx & 31, rest = idx >> 5;
+            const int a = rest % NA, bi = rest / NA;
+            const int b = s_bseg[bi];
+            double v = 0.0;
+            for (int w = s_bwlo[bi]; w <= s_bwhi[bi]; ++w) {
+                const int slot = 2 * w + (b == s_sa[w] ? 0 : 1);
+                v = __dadd_rn(v, s_red[(slot * NA + a) * 32 + f]);
+            }
+            if (f < nv) partial[(int64_t(seg0 + b) * NA + a) * n_frames + f0 + f] = v;
+        }
+    }
+}
+
+// Frame-lane units at plan time: one CTA per unit sorts the unit's pixel
+// indices and its segments' origin pixels (bitonic, kFlSortMax keys),
+// writes each segment's origin index into seg_org (kFlDCap, the zero column,
+// for a row without valid entries), counts the distinct ones into out_d
+// and, with fill (and D <= kFlDCap), writes the distinct list and the
+// unit's entry pairs: A {index 0, index 1, c0, c1} with the table's FP32
+// weights, B {n0, n1, c0/n0, c1/n1} and, when pair_as is given, A with the
+// spread's weights (0 for entries the spread excludes).
+__global__ void __launch_bounds__(256)
+    k_fl_units(const int4 *__restrict__ units, const int4 *__restrict__ segs,
+               const int32_t *__restrict__ col, const int32_t *__restrict__ first_valid,
+               int fill, int32_t *__restrict__ out_d, int32_t *__restrict__ unit_px,
+               const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
+               float4 *__restrict__ pair_a, float4 *__restrict__ pair_b,
+               float4 *__restrict__ pair_as, int32_t *__restrict__ seg_org) {
+    constexpr int N = kFlSortMax, T = 256, PER = N / T;
+    __shared__ int s_key[N];
+    __shared__ int s_uniq[kFlDCap];
+    __shared__ int s_off[kFlSegs + 1], s_poff[kFlSegs + 1];
+    __shared__ int s_warp[T / 32 + 1];
+    const int4 un = units[blockIdx.x];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        int o = 0, po = 0;
+        for (int i = 0; i < un.y; ++i) {
+            const int4 sg = segs[un.x + i];
+            s_off[i] = o;
+            s_poff[i] = po;
+            o += sg.z - sg.y;
+            po += (sg.z - sg.y + 1) & ~1;
+        }
+        s_off[un.y] = o;
+        s_poff[un.y] = po;
+    }
+    __syncthreads();
+    // Keys: the entries' pixels, then each segment's origin pixel (the
+    // pixel of its row's first entry valid for the spread).
+    const int E = s_off[un.y];
+    for (int i = 0; i < un.y; ++i) {
+        const int4 sg = segs[un.x + i];
+        for (int j = tid; j < sg.z - sg.y; j += T) s_key[s_off[i] + j] = col[sg.y + j];
+    }
+    if (tid < un.y) {
+        const int fv = first_valid[segs[un.x + tid].x];
+        s_key[E + tid] = fv >= 0 ? col[fv] : INT_MAX;
+    }
+    for (int j = E + un.y + tid; j < N; j += T) s_key[j] = INT_MAX;
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1) {
+        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+            for (int i = tid; i < N; i += T) {
+                const int ixj = i ^ jj;
+                if (ixj > i) {
+                    const int a = s_key[i], b = s_key[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        s_key[i] = b;
+                        s_key[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // Distinct keys: flags over PER consecutive keys per thread, block scan.
+    int cnt = 0;
+    for (int t = 0; t < PER; ++t) {
+        const int i = tid * PER + t;
+        const int key = s_key[i];
+        cnt += key != INT_MAX && (i == 0 || key != s_key[i - 1]);
+    }
+    const int lane = tid & 31, w = tid >> 5;
+    int inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[w] = inc;
+    __syncthreads();
+    if (tid == 0) {
+        int run = 0;
+        for (int i = 0; i < T / 32; ++i) {
+            const int x = s_warp[i];
+            s_warp[i] = run;
+            run += x;
+        }
+        s_warp[T / 32] = run;
+    }
+    __syncthreads();
+    const int D = s_warp[T / 32];
+    if (tid == 0) out_d[blockIdx.x] = D;
+    if (!fill || D > kFlDCap) return;
+    int pos = s_warp[w] + inc - cnt;
+    for (int t = 0; t < PER; ++t) {
+        const int i = tid * PER + t;
+        const int key = s_key[i];
+        if (key != INT_MAX && (i == 0 || key != s_key[i - 1])) {
+            s_uniq[pos] = key;
+            unit_px[int64_t(blockIdx.x) * kFlDCap + pos] = key;
+            ++pos;
+        }
+    }
+    __syncthreads();
+    if (tid < un.y) {
+        const int fv = first_valid[segs[un.x + tid].x];
+        int a = kFlDCap;
+        if (fv >= 0) {
+            const int cc = col[fv];
+            int b = D;
+            a = 0;
+            while (a < b) {
+                const int m = (a + b) >> 1;
+                if (s_uniq[m] < cc) a = m + 1;
+                else b = m;
+            }
+        }
+        seg_org[un.x + tid] = a;
+    }
+    float *pa = reinterpret_cast<float *>(pair_a + un.z);
+    float *pb = reinterpret_cast<float *>(pair_b + un.z);
+    float *ps = pair_as ? reinterpret_cast<float *>(pair_as + un.z) : nullptr;
+    for (int i = 0; i < un.y; ++i) {
+        const int4 sg = segs[un.x + i];
+        const int len = sg.z - sg.y, padded = (len + 1) & ~1;
+        for (int j = tid; j < padded; j += T) {
+            const int p = s_poff[i] + j, rec = (p >> 1) * 4, h = p & 1;
+            int idx = kFlDCap;
+            float c = 0.f, cs = 0.f, n = 1.f, cr = 0.f;
+            if (j < len) {
+                const int k = sg.y + j, cc = col[k];
+                int a = 0, b = D;
+                while (a < b) {
+                    const int m = (a + b) >> 1;
+                    if (s_uniq[m] < cc) a = m + 1;
+                    else b = m;
+                }
+                idx = a;
+                c = __int_as_float(entry[k].y);
+                const float4 es = entry_std[k];
+                cs = es.y;
+                n = es.z;
+                cr = es.w;
+            }
+            pa[rec + h] = __int_as_float(idx);
+            pa[rec + 2 + h] = c;
+            pb[rec + h] = n;
+            pb[rec + 2 + h] = cr;
+            if (ps) {
+                ps[rec + h] = __int_as_float(idx);
+                ps[rec + 2 + h] = cs;
             }
         }
     }
@@ -391,13 +906,13 @@ __global__ void k_finalize(const double *__restrict__ partial, const int32_t *__
     constexpr int NA = NAcc<MODE, P>::value;
     int64_t id = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
     if (id >= int64_t(n_rows) * n_frames) return;
-    int f = int(id / n_rows), r = int(id % n_rows);
+    int f = int(id % n_frames), r = int(id / n_frames);
     double v[NA];
     for (int a = 0; a < NA; ++a) v[a] = 0.0;
     const int k0 = row_seg[r], k1 = row_seg[r + 1];
     for (int k = k0; k < k1; ++k) {
-        const double *p = partial + (int64_t(f) * n_segments + seg_ids[k]) * NA;
-        for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[a]);
+        const double *p = partial + int64_t(seg_ids[k]) * NA * n_frames + f;
+        for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
     }
     int64_t o = int64_t(f) * n_rows + r;
     if (MODE != kSpread) {
@@ -489,11 +1004,32 @@ __global__ void k_strip_bounds(const int64_t *__restrict__ row_ptr, int n_rows,
     }
 }
 
+template <int MODE, typename P, int U2, bool DB>
+void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, double *partial,
+               cudaStream_t s) {
+    if (t.fl_n_units <= 0)
+        fail(DG_UNSUPPORTED, "the frame-lane gather is not available for this table");
+    constexpr size_t smem = fl_smem_bytes<MODE, P, DB>();
+    auto kern = k_gather_fl<MODE, P, U2, DB>;
+    DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const float4 *pa = MODE == kSpread ? t.fl_pair_as : t.fl_pair_a.ptr;
+    kern<<<t.fl_n_units, kThreads, smem, s>>>(t.fl_unit.ptr, t.seg.ptr, t.fl_px.ptr, pa,
+                                              t.fl_pair_b.ptr, t.entry_std.ptr, t.first_valid.ptr,
+                                              t.fl_seg_org.ptr, fp, n_pixels, nf, t.n_segments,
+                                              partial);
+}
+
 // Launches lane-mapping variant `variant` of the gather (kVariantCount) with
 // its partial sums in `partial`.
 template <int MODE, typename P>
 void launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pixels, int nf,
                    double *partial, cudaStream_t s) {
+    if (variant == 5 || variant == 6) {
+        if (variant == 5) launch_fl<MODE, P, 4, false>(t, fp, n_pixels, nf, partial, s);
+        else launch_fl<MODE, P, 4, true>(t, fp, n_pixels, nf, partial, s);
+        DG_CUDA(cudaGetLastError());
+        return;
+    }
     const size_t smem = size_t(t.unit_cap) * (MODE == kSpread ? 16 : 8);
 #define DG_GATHER_ARGS                                                                        \
     t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp, n_pixels, nf, \
@@ -561,6 +1097,93 @@ void gather_kernel_time(GatherTable &t, bool reset, double *ms, int64_t *gather_
     }
 }
 
+// Frame-lane units (k_gather_fl): runs of at most kFlSegs segments and
+// kFlECap entries of one strip, split in halves by entries until each holds
+// at most kFlDCap distinct pixels; then their pixel lists and entry pairs.
+template <class Group>
+void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<int4> &segs,
+                    Group &&group, cudaStream_t s) {
+    out.fl_n_units = 0;
+    out.fl_pair_as = nullptr;
+    if (segs.empty() || table.nnz > INT32_MAX) return;
+    std::vector<int4> fl;
+    group(kFlECap, kFlSegs, fl);
+    DeviceArray<int4> d_units;
+    DeviceArray<int32_t> d_count;
+    std::vector<int32_t> count;
+    auto seg_len = [&](int i) { return segs[size_t(i)].z - segs[size_t(i)].y; };
+    for (int pass = 0;; ++pass) {
+        d_units.alloc(fl.size());
+        d_count.alloc(fl.size());
+        DG_CUDA(cudaMemcpyAsync(d_units.ptr, fl.data(), fl.size() * sizeof(int4),
+                                cudaMemcpyHostToDevice, s));
+        k_fl_units<<<unsigned(fl.size()), 256, 0, s>>>(
+            d_units.ptr, out.seg.ptr, table.col.ptr, out.first_valid.ptr, 0, d_count.ptr, nullptr,
+            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        DG_CUDA(cudaGetLastError());
+        count.resize(fl.size());
+        DG_CUDA(cudaMemcpyAsync(count.data(), d_count.ptr, count.size() * 4,
+                                cudaMemcpyDeviceToHost, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        std::vector<int4> next;
+        bool split = false;
+        for (size_t u = 0; u < fl.size(); ++u) {
+            const int4 un = fl[u];
+            if (count[u] <= kFlDCap || un.y < 2) {
+                next.push_back(make_int4(un.x, un.y, 0, count[u]));
+                continue;
+            }
+            // Split where the first part's entries reach half the unit's.
+            int total = 0;
+            for (int i = 0; i < un.y; ++i) total += seg_len(un.x + i);
+            int acc = 0, cut = 1;
+            for (int i = 0; i < un.y - 1; ++i) {
+                acc += seg_len(un.x + i);
+                cut = i + 1;
+                if (2 * acc >= total) break;
+            }
+            next.push_back(make_int4(un.x, cut, 0, 0));
+            next.push_back(make_int4(un.x + cut, un.y - cut, 0, 0));
+            split = true;
+        }
+        fl.swap(next);
+        if (!split) break;
+        if (pass > 8) fail(DG_DEVICE, "frame-lane units did not converge");
+    }
+    int64_t pairs = 0;
+    for (auto &un : fl) {
+        if (un.w > kFlDCap) fail(DG_DEVICE, "frame-lane unit exceeds its pixel cap");
+        un.z = int(pairs);
+        for (int i = 0; i < un.y; ++i) pairs += (seg_len(un.x + i) + 1) / 2;
+    }
+    // The spread needs its own weights only if it excludes some entry.
+    std::vector<int32_t> valid(size_t(out.n_rows));
+    if (!valid.empty())
+        DG_CUDA(cudaMemcpyAsync(valid.data(), out.valid_std.ptr, valid.size() * 4,
+                                cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
+    int64_t n_valid = 0;
+    for (int32_t v : valid) n_valid += v;
+    const bool own_spread = n_valid != table.nnz;
+    out.fl_unit.alloc(fl.size());
+    out.fl_px.alloc(fl.size() * size_t(kFlDCap));
+    out.fl_pair_a.alloc(size_t(std::max<int64_t>(pairs, 1)));
+    out.fl_pair_b.alloc(size_t(std::max<int64_t>(pairs, 1)));
+    if (own_spread) out.fl_pair_s.alloc(size_t(std::max<int64_t>(pairs, 1)));
+    else out.fl_pair_s.release();
+    DG_CUDA(cudaMemcpyAsync(out.fl_unit.ptr, fl.data(), fl.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, s));
+    out.fl_seg_org.alloc(segs.size());
+    k_fl_units<<<unsigned(fl.size()), 256, 0, s>>>(
+        out.fl_unit.ptr, out.seg.ptr, table.col.ptr, out.first_valid.ptr, 1, d_count.ptr,
+        out.fl_px.ptr, out.entry.ptr, out.entry_std.ptr, out.fl_pair_a.ptr, out.fl_pair_b.ptr,
+        own_spread ? out.fl_pair_s.ptr : nullptr, out.fl_seg_org.ptr);
+    DG_CUDA(cudaGetLastError());
+    DG_CUDA(cudaStreamSynchronize(s));
+    out.fl_pair_as = own_spread ? out.fl_pair_s.ptr : out.fl_pair_a.ptr;
+    out.fl_n_units = int32_t(fl.size());
+}
+
 void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1, int32_t dim2,
                        int32_t strip_rows, cudaStream_t s, GatherTable &out) {
     out.n_rows = int32_t(table.n_rows);
@@ -602,28 +1225,37 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     std::vector<int4> segs;
     std::vector<int2> units;
     std::vector<int32_t> seg_count(size_t(nb), 0);
+    std::vector<int32_t> strip_first(size_t(n_strips) + 1, 0);
     for (int st = 0; st < n_strips; ++st) {
-        int unit_first = int(segs.size()), unit_entries = 0;
-        auto close_unit = [&]() {
-            if (int(segs.size()) > unit_first)
-                units.push_back(make_int2(unit_first, int(segs.size()) - unit_first));
-            unit_first = int(segs.size());
-            unit_entries = 0;
-        };
+        strip_first[size_t(st)] = int32_t(segs.size());
         for (int64_t r = 0; r < nb; ++r) {
             const int32_t *b = hb.data() + r * (n_strips + 1);
             for (int32_t lo = b[st]; lo < b[st + 1]; lo += kSegMax) {
                 int32_t hi = std::min<int32_t>(lo + kSegMax, b[st + 1]);
-                int len = hi - lo;
-                if (int(segs.size()) - unit_first == kWarps || unit_entries + len > kUnitCap)
-                    close_unit();
                 segs.push_back(make_int4(int(r), lo, hi, int(rp[size_t(r) + 1])));
-                unit_entries += len;
                 seg_count[size_t(r)]++;
             }
         }
-        close_unit();
     }
+    strip_first[size_t(n_strips)] = int32_t(segs.size());
+    // Units: runs of consecutive segments of one strip, at most max_segs
+    // segments and `cap` entries each.
+    auto group = [&](int cap, int max_segs, auto &&emit) {
+        for (int st = 0; st < n_strips; ++st) {
+            int first = strip_first[size_t(st)], entries = 0;
+            for (int i = first; i < strip_first[size_t(st) + 1]; ++i) {
+                const int len = segs[size_t(i)].z - segs[size_t(i)].y;
+                if (i - first == max_segs || entries + len > cap) {
+                    emit(first, i - first);
+                    first = i;
+                    entries = 0;
+                }
+                entries += len;
+            }
+            if (strip_first[size_t(st) + 1] > first) emit(first, strip_first[size_t(st) + 1] - first);
+        }
+    };
+    group(kUnitCap, kWarps, [&](int first, int n) { units.push_back(make_int2(first, n)); });
     // Row -> its segments, in strip order (the finalize's fixed fold order).
     std::vector<int32_t> row_seg(size_t(nb) + 1, 0), seg_ids(segs.size());
     for (int64_t r = 0; r < nb; ++r) row_seg[size_t(r) + 1] = row_seg[size_t(r)] + seg_count[size_t(r)];
@@ -646,6 +1278,9 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     DG_CUDA(cudaMemcpyAsync(out.row_seg.ptr, row_seg.data(), row_seg.size() * 4,
                             cudaMemcpyHostToDevice, s));
     DG_CUDA(cudaStreamSynchronize(s));
+    build_fl_units(out, table, segs, [&](int cap, int max_segs, std::vector<int4> &fl) {
+        group(cap, max_segs, [&](int first, int n) { fl.push_back(make_int4(first, n, 0, 0)); });
+    }, s);
 }
 
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
@@ -718,6 +1353,12 @@ void launch_mode(GatherTable &t, int variant, int mode, const void *frames, int6
 
 int gather_variant_count() { return kVariantCount; }
 
+bool gather_variant_available(const GatherTable &t, int variant) {
+    if (variant < 0 || variant >= kVariantCount) return false;
+    if (variant == 5 || variant == 6) return t.fl_n_units > 0;
+    return true;
+}
+
 int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                     int64_t n_frames, uint32_t flags, cudaStream_t s,
                     std::vector<double> *each) {
@@ -737,6 +1378,10 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     float best_t = 3.4e38f;
     try {
         for (int v = 0; v < kVariantCount; ++v) {
+            if (!gather_variant_available(t, v)) {
+                if (each) (*each)[size_t(v)] = -1.0;
+                continue;
+            }
             float vt = 3.4e38f;
             for (int rep = 0; rep < 4; ++rep) {
                 DG_CUDA(cudaEventRecord(a, s));
@@ -865,6 +1510,12 @@ extern "C" dg_status dg_integrate_device_noalloc(dg_plan *plan, const void *d_fr
             fail(DG_INVALID_INPUT, "azimuthal_std requested without an output");
         if ((flags & DG_AZIMUTHAL_STD) && plan->n_azimuthal != 0)
             fail(DG_UNSUPPORTED, "azimuthal_std is defined for 1D tables only");
+        const uintptr_t pes = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
+        if (reinterpret_cast<uintptr_t>(d_frames) % pes)
+            fail(DG_INVALID_INPUT, "device frames must be aligned to the pixel size");
+        for (const void *o : {(const void *)d_i, (const void *)d_s, (const void *)d_d})
+            if (reinterpret_cast<uintptr_t>(o) % 8)
+                fail(DG_INVALID_INPUT, "device outputs must be 8-byte aligned");
         std::lock_guard<std::mutex> lock(plan->mu);
         int previous = -1;
         DG_CUDA(cudaGetDevice(&previous));

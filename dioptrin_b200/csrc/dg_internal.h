@@ -171,6 +171,17 @@ struct GatherTable {
     DeviceArray<double> den_f32;      // the same sum over the FP32-rounded c and n
     DeviceArray<int32_t> valid_std;   // entries valid for the spread, per row
     DeviceArray<double> partial;      // scratch: per (frame, segment) FP64 sums
+    // Frame-lane layout (k_gather_fl): units of segments with a bounded
+    // number of distinct pixels, their pixel lists (a fixed stride apart) and
+    // the entries in unit order as pairs, columns as indices into the lists.
+    int32_t fl_n_units = 0;
+    DeviceArray<int4> fl_unit;        // {first segment, segment count, first pair, pixels}
+    DeviceArray<int32_t> fl_px;
+    DeviceArray<float4> fl_pair_a;    // {index 0 bits, index 1 bits, c0, c1}
+    DeviceArray<float4> fl_pair_b;    // {n0, n1, c0/n0, c1/n1} (spread)
+    DeviceArray<float4> fl_pair_s;    // pair_a with the spread's weights, when they differ
+    const float4 *fl_pair_as = nullptr;  // the spread's pair_a (fl_pair_s or fl_pair_a)
+    DeviceArray<int32_t> fl_seg_org;  // per segment: its origin pixel's index in the unit list
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
     bool profile = false;
@@ -195,6 +206,7 @@ int gather_launches_per_call();
 // variant's gather launch on the given frames and keeps the fastest in
 // t.variant (returned; `each` receives every variant's time in ms).
 int gather_variant_count();
+bool gather_variant_available(const GatherTable &t, int variant);
 int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                     int64_t n_frames, uint32_t flags, cudaStream_t stream,
                     std::vector<double> *each);

@@ -193,9 +193,10 @@ DG_EXPORT dg_status dg_plan_kernel_time(dg_plan *plan, int32_t reset, double *ga
  * mapping in mapping order, n_ms entries at most.
  * Synchronous. The mappings round differently within the stated tolerance;
  * one plan's results are reproducible between calls made with the same
- * mapping. dg_plan_variant reads the plan's mapping into *current and the
- * number of mappings into *count (either may be NULL) and, when set >= 0,
- * selects mapping `set` first. */
+ * mapping; mappings a table cannot use are skipped (their time is -1).
+ * dg_plan_variant reads the plan's mapping into *current and the number of
+ * mappings into *count (either may be NULL) and, when set >= 0, selects
+ * mapping `set` first (DG_UNSUPPORTED if the table cannot use it). */
 DG_EXPORT dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype,
                                      int64_t n_frames, uint32_t flags, void *stream,
                                      int32_t *variant, double *ms, int32_t n_ms);

@@ -34,7 +34,10 @@ thread_local std::string g_last_error;
 // Detector rows per gather strip (see dg_gather.cu): small enough that a
 // unit's bins cover a few kilobytes of each frame, large enough that a bin's
 // ring is cut into few segments.
-constexpr int32_t kStripRows = 32;
+#ifndef DG_STRIP_ROWS
+#define DG_STRIP_ROWS 16
+#endif
+constexpr int32_t kStripRows = DG_STRIP_ROWS;
 
 }  // namespace
 

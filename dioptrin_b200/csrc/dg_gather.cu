@@ -536,7 +536,9 @@ __global__ void __launch_bounds__(kThreads, DB ? 1 : 2)
         if (SPREAD) s_pb[j] = pair_b[poff + j];
     }
     for (int j = tid; j < D; j += kThreads) s_px[j] = unit_px[int64_t(blockIdx.x) * kFlDCap + j];
-    for (int j = tid; j < (DB ? 64 : 32) * kFlStride; j += kThreads) s_buf[j] = S(0);
+    // Column kFlDCap of every frame row is read by padding entries and must
+    // hold 0; staging writes columns below D <= kFlDCap only.
+    for (int j = tid; j < (DB ? 64 : 32); j += kThreads) s_buf[j * kFlStride + kFlDCap] = S(0);
     // This warp's piece [lo, hi) (entries; pair aligned) and the segments
     // sa..sb it meets.
     const int lo = 2 * int(int64_t(warp) * np / kWarps);

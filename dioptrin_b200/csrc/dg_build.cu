@@ -525,6 +525,158 @@ __global__ void k_ps1d_fill(Ps1d a, const int64_t *__restrict__ off,
     }
 }
 
+// ----------------------------------------------- pyFAI full split 1D
+
+struct Pf1d {
+    int dim1, dim2, n;
+    double r0, r1;
+    const double *rc, *ac;
+};
+constexpr int kPfCap = 64;  // radial bins one pixel may span
+
+// split1d (pyfai_1d.rs:259-354) on n radial bins over [r0, r1), azimuthal
+// edges (-pi, pi), no sector, corner sign +1 (a geometry without a detector
+// object, pyfai_1d.rs:131-137). poly in pyFAI order A, D, C, B. Returns the
+// number of weights kept; with FILL writes them. Sets *overflow when the
+// pixel spans more than kPfCap bins.
+template <bool FILL>
+__device__ int pf_split1d(Pt poly[4], int n, double r0, double r1, int *bins, double *ws,
+                          int *overflow) {
+    for (int i = 0; i < 4; ++i) poly[i].y = wrap_tau(poly[i].y - 0.0 + kPi) - kPi;
+    const Pt a = poly[0], b = poly[1], c = poly[2], d = poly[3];
+    const double area = 1.0 * (0.5 * (c.x - a.x) * (d.y - b.y) - (c.y - a.y) * (d.x - b.x));
+    if (area > 0.0) {
+        for (int i = 0; i < 4; ++i)
+            if (poly[i].y < 0.0) poly[i].y += kTau;
+        double sum = -0.0;
+        for (int i = 0; i < 4; ++i) sum += poly[i].y;
+        if (sum * 0.25 > kPi)
+            for (int i = 0; i < 4; ++i) poly[i].y -= kTau;
+    }
+    for (int i = 0; i < 4; ++i) poly[i].y += 0.0;
+    const double dr = (r1 - r0) / double(n);
+    for (int i = 0; i < 4; ++i) poly[i].x = (poly[i].x - r0) / dr;
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        lo = fmin(lo, poly[i].x);
+        hi = fmax(hi, poly[i].x);
+    }
+    if (hi < 0.0 || lo >= double(n)) return 0;
+    const double flo = floor(lo), fhi = floor(hi);
+    const long long first = (long long)as_usize(fmax(flo, 0.0));
+    long long end = as_isize(fhi) + 1;
+    if (end < 0) end = 0;
+    if (end > n) end = n;
+    if (flo == fhi) {
+        if (FILL) {
+            bins[0] = int(first);
+            ws[0] = 1.0;
+        }
+        return 1;
+    }
+    const int span = int(end - first);
+    if (span > kPfCap) {
+        atomicExch(overflow + 1, 1);
+        return 0;
+    }
+    float buffer[kPfCap];
+    for (int j = 0; j < span; ++j) buffer[j] = 0.0f;
+    for (int i = 0; i < 4; ++i) {
+        const double x0 = poly[i].x, y0 = poly[i].y;
+        const double x1 = poly[(i + 1) & 3].x, y1 = poly[(i + 1) & 3].y;
+        if (x0 == x1) continue;
+        const double slope = (y1 - y0) / (x1 - x0);
+        const double intercept = y0 - slope * x0;
+        const double sg = x1 > x0 ? 1.0 : -1.0;
+        for (int j = 0; j < span; ++j) {
+            const double left = fmax(fmin(x0, x1), double(first + j));
+            const double right = fmin(fmax(x0, x1), double(first + j + 1));
+            if (right > left)
+                buffer[j] = __fadd_rn(buffer[j], __double2float_rn(
+                    sg * (right - left) * (0.5 * slope * (right + left) + intercept)));
+        }
+    }
+    double sum = -0.0;
+    for (int j = 0; j < span; ++j) sum += double(buffer[j]);
+    if (!isfinite(sum) || sum == 0.0) return 0;
+    int m = 0;
+    double total = -0.0;
+    for (int j = 0; j < span; ++j) {
+        const double w = double(buffer[j]) / sum;
+        if (isfinite(w) && w > 0.0) {
+            total += w;
+            if (FILL) {
+                bins[m] = int(first + j);
+                ws[m] = w;
+            }
+            ++m;
+        }
+    }
+    if (FILL)
+        for (int k = 0; k < m; ++k) ws[k] /= total;
+    return m;
+}
+
+// One pixel of build_lut1d_pyfai_csr (pyfai_1d.rs:77-93); -1 for a singular
+// pixel (detector-plane sampling, done by k_sample).
+template <bool FILL>
+__device__ int pf1d_pixel(const Pf1d &a, int64_t idx, int *bins, double *ws, int *overflow) {
+    const int64_t w = a.dim2 + 1;
+    const int64_t b0 = idx / a.dim2 * w + idx % a.dim2;
+    const int64_t ia = b0, ib = b0 + 1, ic = b0 + w + 1, id = b0 + w;
+    // corner_indices A, B, C, D taken as [a, d, c, b] (pyfai_1d.rs:73-76)
+    Pt poly[4] = {{a.rc[ia], a.ac[ia]}, {a.rc[id], a.ac[id]}, {a.rc[ic], a.ac[ic]},
+                  {a.rc[ib], a.ac[ib]}};
+    if (singular(poly)) return -1;
+    return pf_split1d<FILL>(poly, a.n, a.r0, a.r1, bins, ws, overflow);
+}
+
+__global__ void k_pf1d_count(Pf1d a, int32_t *__restrict__ count, int32_t *__restrict__ sing,
+                             int32_t sing_cap, int32_t *__restrict__ n_sing, int *overflow) {
+    const int64_t n = int64_t(a.dim1) * a.dim2;
+    for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < n;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        int c = pf1d_pixel<false>(a, p, nullptr, nullptr, overflow);
+        if (c < 0) {
+            const int slot = atomicAdd(n_sing, 1);
+            if (slot < sing_cap) sing[slot] = int32_t(p);
+            c = 0;
+        }
+        count[p] = c;
+    }
+}
+
+__global__ void k_pf1d_fill(Pf1d a, const int64_t *__restrict__ off,
+                            const int32_t *__restrict__ sing_slot,
+                            const int32_t *__restrict__ hits, int32_t *__restrict__ cbin,
+                            double *__restrict__ cw, int32_t *__restrict__ cpix, int *overflow) {
+    const int64_t n = int64_t(a.dim1) * a.dim2;
+    int bins[kPfCap];
+    double ws[kPfCap];
+    for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < n;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        int64_t o = off[p];
+        const int32_t s = sing_slot ? sing_slot[p] : -1;
+        if (s >= 0) {
+            const int32_t *h = hits + int64_t(s) * a.n;
+            for (int b = 0; b < a.n; ++b)
+                if (h[b]) {
+                    cbin[o] = b;
+                    cw[o] = double(h[b]) / 65536.0;
+                    cpix[o] = int32_t(p);
+                    ++o;
+                }
+            continue;
+        }
+        const int m = pf1d_pixel<true>(a, p, bins, ws, overflow);
+        for (int k = 0; k < m; ++k) {
+            cbin[o + k] = bins[k];
+            cw[o + k] = ws[k];
+            cpix[o + k] = int32_t(p);
+        }
+    }
+}
+
 // Corners whose scaled position lies within a guard band of a bin edge: the
 // only corners where a last-bit difference between CUDA's and glibc's atan2
 // could move an index.
@@ -995,14 +1147,82 @@ void build_table(const dg_geometry &geom, const dg_method &m, int32_t dim1, int3
         k_ss1d<<<grid_for(npix, 128), 128, 0, s>>>(a, off.ptr, count.ptr, cbin.ptr, cw.ptr,
                                                    cpix.ptr);
         DG_CUDA(cudaGetLastError());
+    } else if (m.kind == DG_METHOD_PYFAI_FULL) {
+        DeviceArray<double> rc, ac;
+        rc.alloc(ncorner);
+        ac.alloc(ncorner);
+        k_corners<<<grid_for(ncorner), 256, 0, s>>>(g, dim1, dim2, rc.ptr, ac.ptr);
+        DG_CUDA(cudaGetLastError());
+        Pf1d a{};
+        a.dim1 = dim1;
+        a.dim2 = dim2;
+        a.n = nb;
+        if (m.has_radial_range) {
+            // build_lut1d_pyfai_csr takes an explicit range as the edges.
+            a.r0 = m.radial_min;
+            a.r1 = m.radial_max;
+        } else {
+            // pyfai_radial_range (pyfai_1d.rs:36-46).
+            k_minmax<<<grid_for(ncorner), 256, 0, s>>>(rc.ptr, ncorner, mm.ptr);
+            DG_CUDA(cudaGetLastError());
+            auto k = to_host(mm.ptr, 2, s);
+            a.r0 = std::fmax(key_to_double(k[0]), 0.0);
+            a.r1 = key_to_double(k[1]) * (1.0 + double(FLT_EPSILON));
+        }
+        if (!grid_ok(a.r0, a.r1, nb))
+            fail(DG_INVALID_INPUT, "radial range must have finite, increasing, resolvable, "
+                                   "nonnegative bin edges for pyfai_full");
+        out.hist_min = a.r0;
+        out.hist_step = (a.r1 - a.r0) / double(nb);
+        a.rc = rc.ptr;
+        a.ac = ac.ptr;
+        const int32_t sing_cap = 1 << 16;
+        DeviceArray<int32_t> sing, n_sing;
+        sing.alloc(sing_cap);
+        n_sing.alloc(1);
+        DG_CUDA(cudaMemsetAsync(n_sing.ptr, 0, sizeof(int32_t), s));
+        k_pf1d_count<<<grid_for(npix, 128), 128, 0, s>>>(a, count.ptr, sing.ptr, sing_cap,
+                                                         n_sing.ptr, flags.ptr);
+        DG_CUDA(cudaGetLastError());
+        const int32_t ns = to_host(n_sing.ptr, 1, s)[0];
+        if (ns > sing_cap) fail(DG_UNSUPPORTED, "too many singular pixels for sampling");
+        out.singular_pixels = ns;
+        DeviceArray<int32_t> hits, slot;
+        if (ns > 0) {
+            std::vector<int32_t> hs = to_host(sing.ptr, size_t(ns), s);
+            std::sort(hs.begin(), hs.end());
+            DG_CUDA(cudaMemcpyAsync(sing.ptr, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, s));
+            hits.alloc(size_t(ns) * nb);
+            DG_CUDA(cudaMemsetAsync(hits.ptr, 0, hits.bytes(), s));
+            k_sample<<<ns, 256, 0, s>>>(g, dim2, sing.ptr, nb, a.r0, a.r1,
+                                        m.has_radial_range ? 0 : 1, hits.ptr);
+            DG_CUDA(cudaGetLastError());
+            k_sample_count<<<ns, 256, 0, s>>>(sing.ptr, nb, hits.ptr, count.ptr);
+            DG_CUDA(cudaGetLastError());
+            std::vector<int32_t> hslot(size_t(npix), -1);
+            for (int32_t i = 0; i < ns; ++i) hslot[size_t(hs[size_t(i)])] = i;
+            slot.alloc(size_t(npix));
+            DG_CUDA(cudaMemcpyAsync(slot.ptr, hslot.data(), size_t(npix) * 4,
+                                    cudaMemcpyHostToDevice, s));
+            DG_CUDA(cudaStreamSynchronize(s));
+        }
+        ncoo = scan_counts();
+        if (ncoo > 64ll * 1024 * 1024)
+            fail(DG_UNSUPPORTED, "pyFAI-compatible splitting exceeds the 64-million-entry memory "
+                                 "bound; reduce binning.");
+        k_pf1d_fill<<<grid_for(npix, 128), 128, 0, s>>>(a, off.ptr, ns ? slot.ptr : nullptr,
+                                                        hits.ptr, cbin.ptr, cw.ptr, cpix.ptr,
+                                                        flags.ptr);
+        DG_CUDA(cudaGetLastError());
     } else {
-        fail(DG_UNSUPPORTED, "pyfai_full tables are not built by this version of the library");
+        fail(DG_UNSUPPORTED, "unknown integration method");
     }
 
     int hflags[2] = {0, 0};
     DG_CUDA(cudaMemcpyAsync(hflags, flags.ptr, sizeof hflags, cudaMemcpyDeviceToHost, s));
     DG_CUDA(cudaStreamSynchronize(s));
     if (hflags[0]) fail(DG_UNSUPPORTED, "polygon clipping exceeded its vertex capacity");
+    if (hflags[1]) fail(DG_UNSUPPORTED, "a pixel spans more than 64 radial bins");
 
     transpose(cbin.ptr, cw.ptr, cpix.ptr, off.ptr, npix, ncoo, nb, s, out.full);
 

@@ -562,6 +562,191 @@ int or_build_ps1d(const or_poni *p, int64_t dim1, int64_t dim2, int unit, int64_
     return or_ps1d_fractions(p, dim1, dim2, unit, n, min, step, 1, out);
 }
 
+/* split1d (pyfai_1d.rs:259-354): pyFAI's fullSplit1D rule for one pixel
+ * quadrilateral given in pyFAI corner order (A, D, C, B) as (radial, chi)
+ * pairs, on n radial bins over [r0, r1) and azimuthal edges [a0, a1). The
+ * azimuths are recentred at the canonical seam and unwrapped when pyFAI's
+ * area4p test (with its operator precedence, times the corner sign) is
+ * positive; each edge's signed area under the line is integrated per radial
+ * bin into an f32 buffer; buffer / sum, kept if finite and > 0, renormalised.
+ * Writes at most cap pairs; returns their count, or -1 when the pixel spans
+ * more than cap bins. */
+int or_split1d(const double *poly_in, int64_t n, double r0, double r1, double a0, double a1,
+               int sector, double sign, int64_t *bins, double *weights, int64_t cap) {
+    pt_t poly[4];
+    for (int i = 0; i < 4; ++i) {
+        poly[i].x = poly_in[2 * i];
+        poly[i].y = poly_in[2 * i + 1];
+    }
+    double offset;
+    if (a0 >= -OR_PI && a1 <= OR_PI) offset = 0.0;
+    else if (a0 >= 0.0 && a1 <= OR_TAU) offset = OR_PI;
+    else offset = a0 + OR_PI;
+    for (int i = 0; i < 4; ++i) poly[i].y = wrap_tau(poly[i].y - offset + OR_PI) - OR_PI;
+    pt_t a = poly[0], b = poly[1], c = poly[2], d = poly[3];
+    double area = sign * (0.5 * (c.x - a.x) * (d.y - b.y) - (c.y - a.y) * (d.x - b.x));
+    if (area > 0.0) {
+        for (int i = 0; i < 4; ++i)
+            if (poly[i].y < 0.0) poly[i].y += OR_TAU;
+        double sum = -0.0;
+        for (int i = 0; i < 4; ++i) sum += poly[i].y;
+        if (sum * 0.25 > OR_PI)
+            for (int i = 0; i < 4; ++i) poly[i].y -= OR_TAU;
+    }
+    for (int i = 0; i < 4; ++i) poly[i].y += offset;
+    if (sector) {
+        int below = 1, above = 1;
+        for (int i = 0; i < 4; ++i) {
+            below &= poly[i].y < a0;
+            above &= poly[i].y > a1;
+        }
+        if (below || above) return 0;
+    }
+    double dr = (r1 - r0) / (double)n;
+    for (int i = 0; i < 4; ++i) poly[i].x = (poly[i].x - r0) / dr;
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        lo = fmin(lo, poly[i].x);
+        hi = fmax(hi, poly[i].x);
+    }
+    if (hi < 0.0 || lo >= (double)n) return 0;
+    double flo = floor(lo), fhi = floor(hi);
+    int64_t first = (int64_t)as_usize(fmax(flo, 0.0));
+    int64_t end_i = as_isize(fhi) + 1;
+    if (end_i < 0) end_i = 0;
+    if (end_i > n) end_i = n;
+    if (flo == fhi) {
+        if (cap < 1) return -1;
+        bins[0] = first;
+        weights[0] = 1.0;
+        return 1;
+    }
+    int64_t span = end_i - first;
+    if (span > cap) return -1;
+    float buffer[256];
+    if (span > 256) return -1;
+    for (int64_t j = 0; j < span; ++j) buffer[j] = 0.0f;
+    for (int i = 0; i < 4; ++i) {
+        double x0 = poly[i].x, y0 = poly[i].y, x1 = poly[(i + 1) % 4].x, y1 = poly[(i + 1) % 4].y;
+        if (x0 == x1) continue;
+        double slope = (y1 - y0) / (x1 - x0);
+        double intercept = y0 - slope * x0;
+        double sg = x1 > x0 ? 1.0 : -1.0;
+        for (int64_t j = 0; j < span; ++j) {
+            double left = fmax(fmin(x0, x1), (double)(first + j));
+            double right = fmin(fmax(x0, x1), (double)(first + j + 1));
+            if (right > left)
+                buffer[j] += (float)(sg * (right - left) * (0.5 * slope * (right + left) + intercept));
+        }
+    }
+    double sum = -0.0;
+    for (int64_t j = 0; j < span; ++j) sum += (double)buffer[j];
+    if (!isfinite(sum) || sum == 0.0) return 0;
+    int64_t m = 0;
+    for (int64_t j = 0; j < span; ++j) {
+        double w = (double)buffer[j] / sum;
+        if (isfinite(w) && w > 0.0) {
+            bins[m] = first + j;
+            weights[m] = w;
+            ++m;
+        }
+    }
+    double total = -0.0;
+    for (int64_t k = 0; k < m; ++k) total += weights[k];
+    for (int64_t k = 0; k < m; ++k) weights[k] /= total;
+    return (int)m;
+}
+
+/* pyfai_radial_range (pyfai_1d.rs:36-46): corner radial min (at least 0) and
+ * max * (1 + f32::EPSILON). */
+void or_pyfai_radial_range(const or_poni *p, int64_t dim1, int64_t dim2, int unit, double *lo,
+                           double *hi) {
+    int64_t ncorner = (dim1 + 1) * (dim2 + 1);
+    double *rc = (double *)malloc((size_t)ncorner * sizeof(double));
+    double *ac = (double *)malloc((size_t)ncorner * sizeof(double));
+    if (!rc || !ac) {
+        free(rc);
+        free(ac);
+        *lo = *hi = NAN;
+        return;
+    }
+    or_corners(p, dim1, dim2, unit, rc, ac);
+    double mn = INFINITY, mx = -INFINITY;
+    for (int64_t i = 0; i < ncorner; ++i) {
+        mn = fmin(mn, rc[i]);
+        mx = fmax(mx, rc[i]);
+    }
+    *lo = fmax(mn, 0.0);
+    *hi = mx * (1.0 + (double)FLT_EPSILON);
+    free(rc);
+    free(ac);
+}
+
+/* build_lut1d_pyfai_csr (pyfai_1d.rs:55-109) without an azimuthal sector and
+ * with the corner sign of a geometry without a detector object (+1,
+ * pyfai_1d.rs:131-137): singular pixels by detector-plane sampling, the rest by
+ * split1d. Returns -2 past the 64 Mi entry bound, -3 for a grid
+ * IntegrationGrid2d::new rejects. */
+int or_build_pf1d(const or_poni *p, int64_t dim1, int64_t dim2, int unit, int64_t n,
+                  int has_range, double rmin, double rmax, or_lut *out) {
+    double r0 = rmin, r1 = rmax;
+    if (!has_range) or_pyfai_radial_range(p, dim1, dim2, unit, &r0, &r1);
+    if (!grid_ok(r0, r1, n)) return -3;
+    int64_t ncorner = (dim1 + 1) * (dim2 + 1);
+    double *rc = (double *)malloc((size_t)ncorner * sizeof(double));
+    double *ac = (double *)malloc((size_t)ncorner * sizeof(double));
+    bucket_t *buckets = (bucket_t *)calloc((size_t)n, sizeof(bucket_t));
+    int rc_ = -1;
+    if (rc && ac && buckets) {
+        or_corners(p, dim1, dim2, unit, rc, ac);
+        const int64_t w = dim2 + 1;
+        int64_t entries = 0;
+        int64_t bins[256];
+        double ws[256];
+        rc_ = 0;
+        for (int64_t idx = 0; idx < dim1 * dim2 && rc_ == 0; ++idx) {
+            int64_t b0 = idx / dim2 * w + idx % dim2;
+            int64_t ia = b0, ib = b0 + 1, ic = b0 + w + 1, id = b0 + w;
+            /* corner_indices order A, B, C, D taken as [a, d, c, b] */
+            pt_t poly[4] = {{rc[ia], ac[ia]}, {rc[id], ac[id]}, {rc[ic], ac[ic]}, {rc[ib], ac[ib]}};
+            if (singular(poly)) {
+                int64_t before = 0;
+                for (int64_t k = 0; k < n; ++k) before += buckets[k].n;
+                if (sample_pixel(p, dim2, idx, unit, r0, r1, n, !has_range, buckets)) rc_ = -1;
+                int64_t after = 0;
+                for (int64_t k = 0; k < n; ++k) after += buckets[k].n;
+                entries += after - before;
+            } else {
+                double flat[8] = {poly[0].x, poly[0].y, poly[1].x, poly[1].y,
+                                  poly[2].x, poly[2].y, poly[3].x, poly[3].y};
+                int m = or_split1d(flat, n, r0, r1, -OR_PI, OR_PI, 0, 1.0, bins, ws, 256);
+                if (m < 0) {
+                    rc_ = -1;
+                    break;
+                }
+                entries += m;
+                for (int k = 0; k < m; ++k)
+                    if (bucket_push(&buckets[bins[k]], idx, ws[k])) rc_ = -1;
+            }
+            if (entries > 64LL * 1024 * 1024) rc_ = -2;
+        }
+        if (rc_ == 0) {
+            rc_ = buckets_to_lut(buckets, n, 1, r0, (r1 - r0) / (double)n, out);
+            buckets = NULL;
+        }
+    }
+    if (buckets) {
+        for (int64_t i = 0; i < n; ++i) {
+            free(buckets[i].col);
+            free(buckets[i].w);
+        }
+        free(buckets);
+    }
+    free(rc);
+    free(ac);
+    return rc_;
+}
+
 /* build_lut1d_csr (counting_csr.rs:54-89) and _with_range (:95-134). */
 int or_build_counting1d(const double *radial, int64_t npix, int64_t n, int has_range,
                         double rmin, double rmax, or_lut *out) {

@@ -71,6 +71,13 @@ int or_ps1d_fractions(const or_poni *p, int64_t dim1, int64_t dim2, int unit,
                       int64_t n_points, double min, double step, int clamp_low,
                       or_lut *out);
 /* Counting 1D (counting_csr.rs:54-134). */
+/* pyFAI full splitting, 1D (pyfai_1d.rs:36-354). */
+int or_split1d(const double *poly, int64_t n, double r0, double r1, double a0, double a1,
+               int sector, double sign, int64_t *bins, double *weights, int64_t cap);
+void or_pyfai_radial_range(const or_poni *p, int64_t dim1, int64_t dim2, int unit, double *lo,
+                           double *hi);
+int or_build_pf1d(const or_poni *p, int64_t dim1, int64_t dim2, int unit, int64_t n_points,
+                  int has_range, double rmin, double rmax, or_lut *out);
 int or_build_counting1d(const double *radial, int64_t npix, int64_t n_points, int has_range,
                         double rmin, double rmax, or_lut *out);
 /* Supersampled 1D (supersampled.rs:517-593), exact per-sample path. */

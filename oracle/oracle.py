@@ -8,6 +8,7 @@ package ``dioptrin_b200`` never does.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from dataclasses import dataclass
@@ -99,6 +100,9 @@ def _lib():
         lib.or_build_ps1d.argtypes = [P(Poni), i64, i64, i, i64, i, d, d, P(_Lut)]
         lib.or_ps1d_fractions.argtypes = [P(Poni), i64, i64, i, i64, d, d, i, P(_Lut)]
         lib.or_build_counting1d.argtypes = [pd, i64, i64, i, d, d, P(_Lut)]
+        lib.or_split1d.argtypes = [pd, i64, d, d, d, d, i, d, P(C.c_int64), pd, i64]
+        lib.or_pyfai_radial_range.argtypes = [P(Poni), i64, i64, i, pd, pd]
+        lib.or_build_pf1d.argtypes = [P(Poni), i64, i64, i, i64, i, d, d, P(_Lut)]
         lib.or_build_ss1d.argtypes = [P(Poni), i64, i64, i, i64, i64, i, d, d, P(_Lut)]
         lib.or_compact.argtypes = [P(_Lut), pu8, P(_Lut)]
         lib.or_denominators.argtypes = [P(_Lut), pd, pd]
@@ -196,6 +200,42 @@ def build_ps1d(p: Poni, dim1: int, dim2: int, n_points: int, unit: str = "2th_ra
                               1 if radial_range else 0, rr[0], rr[1], C.byref(lut))
     if rc:
         raise MemoryError("oracle ps1d build failed")
+    return _take(lut)
+
+
+def split1d(poly, n_points: int, radial_range, azimuthal_range=(-math.pi, math.pi),
+            sector: bool = False, sign: float = 1.0):
+    """pyFAI full splitting of one quadrilateral (pyFAI corner order, (radial,
+    chi) pairs): list of (bin, weight)."""
+    flat = np.ascontiguousarray(np.asarray(poly, np.float64).ravel())
+    bins = np.zeros(256, np.int64)
+    w = np.zeros(256)
+    m = _lib().or_split1d(_dp(flat), n_points, radial_range[0], radial_range[1],
+                          azimuthal_range[0], azimuthal_range[1], 1 if sector else 0, sign,
+                          bins.ctypes.data_as(C.POINTER(C.c_int64)), _dp(w), 256)
+    if m < 0:
+        raise ValueError("pixel spans more bins than the oracle buffer")
+    return [(int(bins[k]), float(w[k])) for k in range(m)]
+
+
+def pyfai_radial_range(p: Poni, dim1: int, dim2: int, unit: str = "2th_rad"):
+    lo, hi = C.c_double(), C.c_double()
+    _lib().or_pyfai_radial_range(C.byref(p), dim1, dim2, UNITS[unit], C.byref(lo), C.byref(hi))
+    return lo.value, hi.value
+
+
+def build_pf1d(p: Poni, dim1: int, dim2: int, n_points: int, unit: str = "2th_rad",
+               radial_range=None) -> Lut:
+    lut = _Lut()
+    rr = radial_range or (0.0, 0.0)
+    rc = _lib().or_build_pf1d(C.byref(p), dim1, dim2, UNITS[unit], n_points,
+                              1 if radial_range else 0, rr[0], rr[1], C.byref(lut))
+    if rc == -2:
+        raise ValueError("pyFAI-compatible splitting exceeds the 64-million-entry bound")
+    if rc == -3:
+        raise ValueError("invalid pyFAI full-splitting grid")
+    if rc:
+        raise MemoryError("oracle pyfai_full build failed")
     return _take(lut)
 
 

@@ -40,6 +40,8 @@ def oracle_table(o, poni, shape, method, n, unit="2th_rad", rng=None, n_ss=2):
         return o.build_counting1d(c["radial"], n, rng)
     if method == "supersampled":
         return o.build_ss1d(p, *shape, n, n_ss, unit=unit, radial_range=rng)
+    if method == "pyfai_full":
+        return o.build_pf1d(p, *shape, n, unit=unit, radial_range=rng)
     raise ValueError(method)
 
 
@@ -72,7 +74,7 @@ def check_tables(o, plan, ref, mask, norm):
     return refc, ref_den
 
 
-@pytest.mark.parametrize("method", ["pixel_split", "counting", "supersampled"])
+@pytest.mark.parametrize("method", ["pixel_split", "counting", "supersampled", "pyfai_full"])
 @pytest.mark.parametrize("unit", ["2th_rad", "2th_deg", "q_nm^-1"])
 @pytest.mark.parametrize("ranged", [False, True])
 def test_table_bit_exact_small(dg, oracle, method, unit, ranged):
@@ -140,6 +142,33 @@ def test_integration_matches_oracle(dg, oracle, dtype):
         scale = _scale(oracle, table, den, sig)
         assert np.all(np.abs(I2[k] - yi) <= TOL_I * scale)
         np.testing.assert_allclose(S2[k], ys, rtol=TOL_I, atol=0)
+
+
+@pytest.mark.parametrize("method", ["pyfai_full", "supersampled", "counting"])
+def test_other_methods_integrate_like_the_oracle(dg, oracle, method):
+    poni = small_poni()
+    shape = (64, 80)
+    n = 90
+    mask = np.zeros(shape, np.uint8)
+    mask[30, :] = 1
+    it = make_integrator(dg, poni, method, mask=mask)
+    plan = it.prepare_cuda1d(shape, n)
+    ref = oracle_table(oracle, poni, shape, method, n)
+    norm = oracle.centres(oracle.poni(**poni), *shape, polarization_factor=0.99)["norm"]
+    table = oracle.compact(ref, mask.ravel())
+    den = oracle.denominators(table, norm)
+    frames = np.random.default_rng(17).poisson(120.0, (4,) + shape).astype(np.uint32)
+    I, S, D = plan.integrate_stack(frames, errors=True, azimuthal_std=True)
+    for k in range(len(frames)):
+        sig = frames[k].astype(np.float64).ravel()
+        yi, ys = oracle.integrate_strict(table, den, sig, True)
+        scale = _scale(oracle, table, den, sig)
+        assert np.all(np.abs(I[k] - yi) <= TOL_I * scale), f"{method} frame {k}"
+        np.testing.assert_allclose(S[k], ys, rtol=TOL_I, atol=1e-12)
+        si, se, sd = oracle.azimuthal_std(ref, mask.ravel(), norm, sig, sig)
+        fin = np.isfinite(sd)
+        assert np.array_equal(fin, np.isfinite(D[k]))
+        np.testing.assert_allclose(D[k][fin], sd[fin], rtol=TOL_STD, atol=1e-6 * np.nanmax(si))
 
 
 def test_batch_is_bit_identical_to_single_frames(dg):

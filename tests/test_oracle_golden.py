@@ -294,3 +294,55 @@ def test_ss1d_counts_every_subpixel(oracle):
     totals = np.bincount(lut.col, weights=lut.w, minlength=100)
     assert np.max(np.abs(totals - 1.0)) < 1e-12
     assert set(np.round(lut.w * 4).astype(int)) <= {1, 2, 3, 4}
+
+
+def test_pf_radial_line_weights_match_pyfai_golden(oracle):
+    # pyfai_1d.rs:392-413: pyFAI fullSplit1D_engine weights of one pixel on
+    # four bins over [0, 2].
+    w = oracle.split1d([(0.1, 0.2), (1.2, 0.3), (1.8, 1.5), (0.4, 1.7)], 4, (0.0, 2.0))
+    expected = [0.21462747684427036, 0.4066985688044358, 0.32228298342690204,
+                0.05639097092439181]
+    assert [b for b, _ in w] == [0, 1, 2, 3]
+    assert all(abs(a - e) < 1e-7 for (_, a), e in zip(w, expected))
+
+
+def test_pf_partial_radial_pixel_renormalizes_and_disjoint_sector_excludes(oracle):
+    # pyfai_1d.rs:415-424.
+    poly = [(-0.5, 0.1), (-0.5, 0.8), (0.75, 0.8), (0.75, 0.1)]
+    w = oracle.split1d(poly, 4, (0.0, 2.0), (0.2, 0.4), sector=True)
+    assert abs(sum(x for _, x in w) - 1.0) < 1e-12
+    assert all(math.isfinite(x) and x > 0 for _, x in w)
+    assert oracle.split1d(poly, 4, (0.0, 2.0), (1.0, 2.0), sector=True) == []
+
+
+def test_pf_seam_test_uses_pyfai_operator_precedence(oracle):
+    # pyfai_1d.rs:429-434: 0.5 * X - Y is negative for this folded quad.
+    poly = [(1.0, -0.5), (1.2, -0.4), (2.0, 0.25), (2.2, 0.6)]
+    assert oracle.split1d(poly, 10, (0.0, 3.0), (1.0, 2.0), sector=True) == []
+
+
+def _beam_geometry(oracle, poni1, poni2):
+    # pyfai_1d.rs:532-541: 9 x 11 detector, 100 um pixels, beam in pixel (4, 5).
+    return oracle.poni(pixel1=1e-4, pixel2=1e-4, distance=0.05, poni1=poni1, poni2=poni2,
+                       wavelength=1e-10)
+
+
+def test_pf_automatic_range_conserves_the_beam_pixel(oracle):
+    # pyfai_1d.rs:554-567.
+    for poni1, poni2 in [(4.5e-4, 5.5e-4), (4.3e-4, 5.6e-4)]:
+        lut = oracle.build_pf1d(_beam_geometry(oracle, poni1, poni2), 9, 11, 200, unit="2th_deg")
+        totals = np.bincount(lut.col, weights=lut.w, minlength=99)
+        assert abs(totals[4 * 11 + 5] - 1.0) < 1e-12
+        assert np.max(np.abs(totals - 1.0)) < 1e-9
+
+
+def test_pf_explicit_range_clips_the_beam_pixel(oracle):
+    # pyfai_1d.rs:569-588 (radial part; the sector form is not on this path).
+    p = _beam_geometry(oracle, 4.5e-4, 5.5e-4)
+    auto = oracle.pyfai_radial_range(p, 9, 11, unit="2th_deg")
+    lo = math.degrees(math.atan(0.5e-4 / 0.05))
+    lut = oracle.build_pf1d(p, 9, 11, 200, unit="2th_deg", radial_range=(lo, auto[1]))
+    total = np.bincount(lut.col, weights=lut.w, minlength=99)[4 * 11 + 5]
+    assert abs(total - (1.0 - math.pi / 4.0)) < 2e-3
+    lut = oracle.build_pf1d(p, 9, 11, 200, unit="2th_deg", radial_range=auto)
+    assert np.bincount(lut.col, weights=lut.w, minlength=99)[4 * 11 + 5] == 0.0

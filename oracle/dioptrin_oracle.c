@@ -869,6 +869,519 @@ int or_build_ss1d(const or_poni *p, int64_t dim1, int64_t dim2, int unit, int64_
 
 /* ---------------------------------------------------------------- gather */
 
+/* ================================================================ 2D tables */
+
+/* IntegrationGrid2d::new (grid.rs:49-105): bin counts, finite, increasing and
+ * resolvable edges, nonnegative radial start, azimuthal span of at most one
+ * turn, a start outside +-2pi moved into [-pi, pi). Returns 0 or -1. */
+int or_grid2d_new(int64_t nr, int64_t na, double r0, double r1, double a0, double a1,
+                  or_grid2d *g) {
+    memset(g, 0, sizeof(*g));
+    if (nr <= 0 || na <= 0) return -1;
+    double lo[2] = {r0, a0}, hi[2] = {r1, a1};
+    int64_t cnt[2] = {nr, na};
+    for (int k = 0; k < 2; ++k) {
+        double step = (hi[k] - lo[k]) / (double)cnt[k];
+        if (!isfinite(lo[k]) || !isfinite(hi[k]) || !isfinite(step) || step <= 0.0 ||
+            lo[k] + step == lo[k] || hi[k] - step == hi[k])
+            return -1;
+    }
+    if (r0 < 0.0) return -1;
+    if (a1 - a0 > OR_TAU + 1e-12) return -1;
+    if (!(a0 >= -OR_TAU && a0 <= OR_TAU)) {
+        double start = rem_euclid_tau(a0);
+        if (start >= OR_PI) start -= OR_TAU;
+        double span = a1 - a0;
+        a0 = start;
+        a1 = start + span;
+    }
+    g->n_radial = nr;
+    g->n_azimuthal = na;
+    g->r0 = r0;
+    g->r1 = r1;
+    g->a0 = a0;
+    g->a1 = a1;
+    return 0;
+}
+
+static inline double grid_dr(const or_grid2d *g) { return (g->r1 - g->r0) / (double)g->n_radial; }
+static inline double grid_da(const or_grid2d *g) { return (g->a1 - g->a0) / (double)g->n_azimuthal; }
+
+/* f64::clamp. */
+static inline double clampd(double x, double lo, double hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+
+/* IntegrationGrid2d::bin (grid.rs:176-222); -1 for no bin. */
+int64_t or_grid2d_bin(const or_grid2d *g, double radial, double azimuthal) {
+    double r0 = g->r0, r1 = g->r1, a0 = g->a0, a1 = g->a1;
+    if (!isfinite(radial) || !isfinite(azimuthal)) return -1;
+    if (!g->clamp_radial_outside &&
+        (radial < r0 || radial > r1 || (radial == r1 && !g->clamp_radial_end)))
+        return -1;
+    double offset;
+    if (g->clamp_azimuthal_outside) {
+        offset = clampd(azimuthal - a0, 0.0, a1 - a0);
+    } else if (g->clamp_index_rounding) {
+        double wrapped = (azimuthal >= a0 && azimuthal < a1)
+                             ? azimuthal
+                             : a0 + rem_euclid_tau(azimuthal - a0);
+        if (wrapped >= a1 && a1 - a0 < OR_TAU) return -1;
+        offset = wrapped - a0;
+    } else {
+        double az = a0 + rem_euclid_tau(azimuthal - a0);
+        if (az >= a1) return -1;
+        offset = az - a0;
+    }
+    uint64_t r = as_usize((radial - r0) / grid_dr(g));
+    uint64_t a = as_usize(offset / grid_da(g));
+    if (g->clamp_radial_end || g->clamp_index_rounding || g->clamp_radial_outside)
+        if (r > (uint64_t)(g->n_radial - 1)) r = (uint64_t)(g->n_radial - 1);
+    if (g->clamp_index_rounding || g->clamp_azimuthal_outside)
+        if (a > (uint64_t)(g->n_azimuthal - 1)) a = (uint64_t)(g->n_azimuthal - 1);
+    if (r < (uint64_t)g->n_radial && a < (uint64_t)g->n_azimuthal)
+        return (int64_t)(a * (uint64_t)g->n_radial + r);
+    return -1;
+}
+
+/* Radial and azimuthal extremes of the hull grid (lut/common.rs:33-65). */
+static int hull_extremes(const or_poni *p, int64_t dim1, int64_t dim2, int64_t n_ss, int unit,
+                         double *rlo, double *rhi, double *alo, double *ahi) {
+    int64_t hn = 2 * (dim1 + dim2) * n_ss;
+    double *hd1 = (double *)malloc((size_t)hn * sizeof(double));
+    double *hd2 = (double *)malloc((size_t)hn * sizeof(double));
+    double *ht = (double *)malloc((size_t)hn * sizeof(double));
+    double *hc = (double *)malloc((size_t)hn * sizeof(double));
+    if (!hd1 || !hd2 || !ht || !hc) {
+        free(hd1);
+        free(hd2);
+        free(ht);
+        free(hc);
+        return -1;
+    }
+    int64_t m = hull_grid(dim1, dim2, n_ss, hd1, hd2);
+    or_tth_chi_at(p, hd1, hd2, m, ht, hc);
+    for (int64_t i = 0; i < m; ++i) ht[i] = or_convert_unit(unit, p->wavelength, ht[i]);
+    *rlo = seq_min(ht, m);
+    *rhi = seq_max(ht, m);
+    *alo = seq_min(hc, m);
+    *ahi = seq_max(hc, m);
+    free(hd1);
+    free(hd2);
+    free(ht);
+    free(hc);
+    return 0;
+}
+
+/* The grid prepare_cuda2d uses (cuda.rs:1111-1157 via device.rs:2502 and
+ * the shared-grid key of methods.rs:365-388): explicit or default radial
+ * edges (default_radial_edges_2d, grid.rs:975-1028), explicit or default
+ * azimuthal edges (default_azimuthal_edges_2d, grid.rs:700-755; (-pi, pi)
+ * for pyfai_full), index-rounding clamps, then per method: pyFAI histogram
+ * mode, the counting radial end, the supersampled outside clamps
+ * (azimuthal_range_grid, grid.rs:579-624). Returns 0 or -1. */
+int or_grid2d_for(const or_poni *p, int64_t dim1, int64_t dim2, int method, int64_t n_ss,
+                  int unit, int64_t nr, int64_t na, int has_rr, double rmin, double rmax,
+                  int has_ar, double amin, double amax, or_grid2d *g) {
+    int64_t npix = dim1 * dim2, ncorner = (dim1 + 1) * (dim2 + 1);
+    double *cr = (double *)malloc((size_t)npix * sizeof(double));
+    double *cc = (double *)malloc((size_t)npix * sizeof(double));
+    double *rc = (double *)malloc((size_t)ncorner * sizeof(double));
+    double *ac = (double *)malloc((size_t)ncorner * sizeof(double));
+    int rc_ = -1;
+    if (!cr || !cc || !rc || !ac) goto done;
+    or_centres(p, dim1, dim2, unit, 0, 0.0, NULL, cr, cc, NULL, NULL, NULL);
+    or_corners(p, dim1, dim2, unit, rc, ac);
+    double r0, r1, a0, a1;
+    if (has_rr) {
+        r0 = rmin;
+        r1 = rmax;
+    } else if (method == 0) {
+        r0 = seq_min(cr, npix);
+        r1 = seq_max(cr, npix) + 10.0 * OR_EPS;
+    } else if (method == 1) {
+        r0 = seq_min(rc, ncorner);
+        r1 = seq_max(rc, ncorner) + 10.0 * OR_EPS;
+    } else if (method == 2) {
+        or_pyfai_radial_range(p, dim1, dim2, unit, &r0, &r1);
+    } else {
+        double hlo, hhi, alo, ahi;
+        if (hull_extremes(p, dim1, dim2, n_ss, unit, &hlo, &hhi, &alo, &ahi)) goto done;
+        double a = seq_min(cr, npix), b = seq_max(cr, npix);
+        r0 = hlo < a ? hlo : a;
+        r1 = (hhi > b ? hhi : b) + 3.0 * OR_EPS;
+    }
+    if (has_ar) {
+        a0 = amin;
+        a1 = amax;
+    } else if (method == 2) {
+        a0 = -OR_PI;
+        a1 = OR_PI;
+    } else {
+        if (method == 0) {
+            a0 = seq_min(cc, npix);
+            a1 = seq_max(cc, npix) + 10.0 * OR_EPS;
+        } else if (method == 3) {
+            double hlo, hhi, alo, ahi;
+            if (hull_extremes(p, dim1, dim2, n_ss, unit, &hlo, &hhi, &alo, &ahi)) goto done;
+            double a = seq_min(cc, npix), b = seq_max(cc, npix);
+            a0 = alo < a ? alo : a;
+            a1 = (ahi > b ? ahi : b) + 3.0 * OR_EPS;
+        } else {
+            a0 = seq_min(ac, ncorner);
+            a1 = seq_max(ac, ncorner) + 10.0 * OR_EPS;
+        }
+        if (!(a1 - a0 > 1e-12)) {
+            a0 = -OR_PI;
+            a1 = OR_PI;
+        }
+    }
+    if (or_grid2d_new(nr, na, r0, r1, a0, a1, g)) goto done;
+    g->clamp_index_rounding = 1;
+    if (method == 2) g->pyfai = 1;
+    else if (!has_rr && method == 0) g->clamp_radial_end = 1;
+    else if (!has_rr && method == 3) g->clamp_radial_outside = 1;
+    if (method == 3 && !has_ar) g->clamp_azimuthal_outside = 1;
+    rc_ = 0;
+done:
+    free(cr);
+    free(cc);
+    free(rc);
+    free(ac);
+    return rc_;
+}
+
+/* (bin, weight) list of one pixel; repeated bins add up (shared_grid.rs). */
+typedef struct {
+    int64_t *bin;
+    double *w;
+    int64_t n, cap;
+} entries_t;
+
+static int entries_add(entries_t *e, int64_t bin, double w) {
+    for (int64_t k = 0; k < e->n; ++k)
+        if (e->bin[k] == bin) {
+            e->w[k] += w;
+            return 0;
+        }
+    if (e->n == e->cap) {
+        int64_t cap = e->cap ? 2 * e->cap : 16;
+        int64_t *b = (int64_t *)realloc(e->bin, (size_t)cap * sizeof(int64_t));
+        if (!b) return -1;
+        e->bin = b;
+        double *w2 = (double *)realloc(e->w, (size_t)cap * sizeof(double));
+        if (!w2) return -1;
+        e->w = w2;
+        e->cap = cap;
+    }
+    e->bin[e->n] = bin;
+    e->w[e->n] = w;
+    e->n++;
+    return 0;
+}
+
+/* sample_pixel (shared_grid.rs:202-232), n_ss = 128 with four offsets:
+ * detector-plane samples binned on the grid, weight 1/65536 each. */
+static int sample_pixel_2d(const or_poni *p, int64_t dim2, int64_t pixel, int unit,
+                           const or_grid2d *g, entries_t *e) {
+    const int64_t n_ss = 128;
+    static const double off[4][2] = {{0.25, 0.5}, {0.5, 0.25}, {0.75, 0.5}, {0.5, 0.75}};
+    const double weight = 1.0 / ((double)(n_ss * n_ss) * 4.0);
+    trig_t t = trig_of(p);
+    int64_t row = pixel / dim2, col = pixel % dim2;
+    for (int64_t i = 0; i < n_ss; ++i)
+        for (int64_t j = 0; j < n_ss; ++j)
+            for (int o = 0; o < 4; ++o) {
+                double d1 = (double)row + ((double)i + off[o][0]) / (double)n_ss;
+                double d2 = ((double)(col * n_ss + j) + off[o][1]) / (double)n_ss;
+                double a = d1 * p->pixel1 - p->poni1;
+                double b = d2 * p->pixel2 - p->poni2;
+                double x = f_x1(a, b, p->distance, &t);
+                double y = f_x2(a, b, p->distance, &t);
+                double z = f_x3(a, b, p->distance, &t);
+                double r = or_convert_unit(unit, p->wavelength, f_tth(x, y, z));
+                int64_t bin = or_grid2d_bin(g, r, f_azimuth(x, y));
+                if (bin >= 0 && entries_add(e, bin, weight)) return -1;
+            }
+    return 0;
+}
+
+/* split_polygon (shared_grid.rs:152-200): clip against every bin rectangle of
+ * the three periodic copies (-2pi, 0, +2pi) of the polygon. */
+static int split_polygon_2d(const pt_t poly[4], double area, const or_grid2d *g, entries_t *e) {
+    double r0 = g->r0, a0 = g->a0, dr = grid_dr(g), da = grid_da(g);
+    double rmn = INFINITY, rmx = -INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        rmn = fmin(rmn, poly[i].x);
+        rmx = fmax(rmx, poly[i].x);
+    }
+    int64_t rs = as_isize(floor((rmn - r0) / dr));
+    if (rs < 0) rs = 0;
+    int64_t re = as_isize(floor((rmx - r0) / dr));
+    if (re > g->n_radial - 1) re = g->n_radial - 1;
+    pt_t buf1[64], buf2[64];
+    const double shifts[3] = {-OR_TAU, 0.0, OR_TAU};
+    for (int sh = 0; sh < 3; ++sh) {
+        pt_t q[4];
+        double amn = INFINITY, amx = -INFINITY;
+        for (int i = 0; i < 4; ++i) {
+            q[i].x = poly[i].x;
+            q[i].y = poly[i].y + shifts[sh];
+            amn = fmin(amn, q[i].y);
+            amx = fmax(amx, q[i].y);
+        }
+        int64_t as_ = as_isize(floor((amn - a0) / da));
+        if (as_ < 0) as_ = 0;
+        int64_t ae = as_isize(floor((amx - a0) / da));
+        if (ae > g->n_azimuthal - 1) ae = g->n_azimuthal - 1;
+        for (int64_t ar = as_; ar <= ae; ++ar)
+            for (int64_t rr = rs; rr <= re; ++rr) {
+                double r = r0 + (double)rr * dr;
+                double a = a0 + (double)ar * da;
+                const pt_t *clipped;
+                int m = clip_rect(q, 4, r, r + dr, a, a + da, buf1, buf2, &clipped);
+                double w = fabs(polygon_area(clipped, m)) / area;
+                if (w > 0.0 && entries_add(e, ar * g->n_radial + rr, w)) return -1;
+            }
+    }
+    return 0;
+}
+
+/* line (pyfai_split.rs:146-168): one contour edge's signed area, rasterised
+ * into azimuthal rows in strips of one radial column. */
+static void pyfai_line(float *buffer, int64_t stride, pt_t start, pt_t stop) {
+    if (start.x == stop.x) return;
+    float slope = (float)((stop.y - start.y) / (stop.x - start.x));
+    float intercept = (float)(stop.y - (double)slope * stop.x);
+    double lo = fmin(start.x, stop.x), hi = fmax(start.x, stop.x);
+    double sign = stop.x > start.x ? 1.0 : -1.0;
+    uint64_t rb = as_usize(floor(lo)), re = as_usize(ceil(hi));
+    for (uint64_t r = rb; r < re; ++r) {
+        double left = fmax(lo, (double)r), right = fmin(hi, (double)(r + 1));
+        float area =
+            (float)(sign * (right - left) * (0.5 * (double)slope * (right + left) + (double)intercept));
+        float width = (float)(right - left);
+        float remaining = fabsf(area);
+        for (int64_t a = 0; a < stride; ++a) {
+            if (remaining <= 0.0f) break;
+            float increment = fminf(width, remaining);
+            buffer[(int64_t)r * stride + a] += copysignf(increment, area);
+            remaining -= increment;
+        }
+    }
+}
+
+/* pyfai_split::split (pyfai_split.rs:35-144); poly in pyFAI order (top-left,
+ * bottom-left, bottom-right, top-right) with raw angles. Returns the number
+ * of entries, -1 for None (the caller falls back to fractional clipping),
+ * -2 when the raster exceeds the oracle's buffer. */
+int or_pyfai_split2d(const double *poly_in, const or_grid2d *g, double sign, int64_t *bins,
+                     double *weights, int64_t cap) {
+    pt_t poly[4];
+    for (int i = 0; i < 4; ++i) {
+        poly[i].x = poly_in[2 * i];
+        poly[i].y = poly_in[2 * i + 1];
+    }
+    double a0 = g->a0, a1 = g->a1, r0 = g->r0, r1 = g->r1;
+    double canonical = (a0 >= -OR_PI && a1 <= OR_PI) ? -OR_PI : (a0 >= 0.0 && a1 <= OR_TAU) ? 0.0 : a0;
+    double offset = canonical + OR_PI;
+    for (int i = 0; i < 4; ++i) poly[i].y = wrap_tau(poly[i].y - offset + OR_PI) - OR_PI;
+    pt_t a = poly[0], b = poly[1], c = poly[2], d = poly[3];
+    double area = sign * (0.5 * (c.x - a.x) * (d.y - b.y) - (c.y - a.y) * (d.x - b.x));
+    if (area > 0.0) {
+        for (int i = 0; i < 4; ++i)
+            if (poly[i].y < 0.0) poly[i].y += OR_TAU;
+        double s = -0.0;
+        for (int i = 0; i < 4; ++i) s += poly[i].y;
+        if (s * 0.25 > OR_PI)
+            for (int i = 0; i < 4; ++i) poly[i].y -= OR_TAU;
+    }
+    for (int i = 0; i < 4; ++i) poly[i].y += offset;
+    int all_lo_r = 1, all_hi_r = 1, all_lo_a = 1, all_hi_a = 1;
+    for (int i = 0; i < 4; ++i) {
+        all_lo_r &= poly[i].x < r0;
+        all_hi_r &= poly[i].x > r1;
+        all_lo_a &= poly[i].y < a0;
+        all_hi_a &= poly[i].y > a1;
+    }
+    if (all_lo_r || all_hi_r || all_lo_a || all_hi_a) return 0;
+    double dr = grid_dr(g), da = grid_da(g);
+    for (int i = 0; i < 4; ++i) {
+        poly[i].x = (clampd(poly[i].x, r0, r1) - r0) / dr;
+        poly[i].y = (clampd(poly[i].y, a0, a1) - a0) / da;
+    }
+    double mr = INFINITY, ma = INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        mr = fmin(mr, poly[i].x);
+        ma = fmin(ma, poly[i].y);
+    }
+    uint64_t ir = as_usize(floor(mr)), ia = as_usize(floor(ma));
+    for (int i = 0; i < 4; ++i) {
+        poly[i].x -= (double)ir;
+        poly[i].y -= (double)ia;
+    }
+    double xr = 0.0, xa = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        xr = fmax(xr, poly[i].x);
+        xa = fmax(xa, poly[i].y);
+    }
+    uint64_t nr = as_usize(ceil(xr)), na = as_usize(ceil(xa));
+    if (nr == 0 || na == 0) return -1;
+    if ((nr + 1) * (na + 1) > 4096) return -2;
+    float buffer[4096];
+    for (uint64_t k = 0; k < (nr + 1) * (na + 1); ++k) buffer[k] = 0.0f;
+    for (int i = 0; i < 4; ++i) pyfai_line(buffer, (int64_t)(na + 1), poly[i], poly[(i + 1) % 4]);
+    int64_t m = 0;
+    double total = 0.0;
+    for (uint64_t r = 0; r < nr; ++r)
+        for (uint64_t q = 0; q < na; ++q) {
+            double value = sign * (double)buffer[r * (na + 1) + q];
+            if (!isfinite(value)) return -1;
+            if (value > 0.0 && ir + r < (uint64_t)g->n_radial && ia + q < (uint64_t)g->n_azimuthal) {
+                if (m >= cap) return -2;
+                bins[m] = (int64_t)((ia + q) * (uint64_t)g->n_radial + ir + r);
+                weights[m] = value;
+                total += value;
+                ++m;
+            }
+        }
+    if (total <= 0.0) return -1;
+    for (int64_t k = 0; k < m; ++k) weights[k] /= total;
+    return (int)m;
+}
+
+/* shared_grid::build (shared_grid.rs:13-150) and, for supersampling,
+ * build_shared_grid_ss_csr through the exact counted path
+ * (supersampled.rs:1437-1477, :21-104 with normalize_bins false): per pixel
+ * entries, then rows filled in pixel order. method 0 counting, 1 pixel
+ * split (fractional), 2 pyfai_full (pyFAI histogram mode), 3 supersampled. */
+int or_build_2d(const or_poni *p, int64_t dim1, int64_t dim2, int method, int64_t n_ss,
+                int unit, const or_grid2d *g, or_lut *out) {
+    int64_t npix = dim1 * dim2, ncorner = (dim1 + 1) * (dim2 + 1);
+    int64_t nb = g->n_radial * g->n_azimuthal;
+    double *cr = (double *)malloc((size_t)npix * sizeof(double));
+    double *cc = (double *)malloc((size_t)npix * sizeof(double));
+    double *rc = (double *)malloc((size_t)ncorner * sizeof(double));
+    double *ac = (double *)malloc((size_t)ncorner * sizeof(double));
+    bucket_t *buckets = (bucket_t *)calloc((size_t)nb, sizeof(bucket_t));
+    entries_t e = {0};
+    int64_t pb[4096];
+    double pw[4096];
+    int rc_ = -1;
+    if (!cr || !cc || !rc || !ac || !buckets) goto done;
+    or_centres(p, dim1, dim2, unit, 0, 0.0, NULL, cr, cc, NULL, NULL, NULL);
+    or_corners(p, dim1, dim2, unit, rc, ac);
+    trig_t t = trig_of(p);
+    const int64_t w = dim2 + 1;
+    rc_ = 0;
+    for (int64_t pixel = 0; pixel < npix && rc_ == 0; ++pixel) {
+        e.n = 0;
+        if (method == 0) {
+            int64_t bin = or_grid2d_bin(g, cr[pixel], cc[pixel]);
+            if (bin >= 0 && entries_add(&e, bin, 1.0)) rc_ = -1;
+        } else if (method == 3) {
+            int64_t row = pixel / dim2, col = pixel % dim2;
+            int64_t cb[256], cn[256];
+            int nc = 0;
+            for (int64_t i = 0; i < n_ss; ++i) {
+                double d1 = (double)row + ((double)i + 0.5) / (double)n_ss;
+                for (int64_t j = 0; j < n_ss; ++j) {
+                    double d2 = ((double)(col * n_ss + j) + 0.5) / (double)n_ss;
+                    double a = d1 * p->pixel1 - p->poni1;
+                    double bb = d2 * p->pixel2 - p->poni2;
+                    double x = f_x1(a, bb, p->distance, &t);
+                    double y = f_x2(a, bb, p->distance, &t);
+                    double z = f_x3(a, bb, p->distance, &t);
+                    double r = or_convert_unit(unit, p->wavelength, f_tth(x, y, z));
+                    int64_t bin = or_grid2d_bin(g, r, f_azimuth(x, y));
+                    if (bin < 0) continue;
+                    int f = -1;
+                    for (int q = 0; q < nc; ++q)
+                        if (cb[q] == bin) {
+                            f = q;
+                            break;
+                        }
+                    if (f < 0) {
+                        cb[nc] = bin;
+                        cn[nc++] = 1;
+                    } else {
+                        cn[f]++;
+                    }
+                }
+            }
+            for (int q = 0; q < nc && rc_ == 0; ++q)
+                if (entries_add(&e, cb[q], (double)cn[q] / (double)(n_ss * n_ss))) rc_ = -1;
+        } else {
+            int64_t b0 = pixel / dim2 * w + pixel % dim2;
+            int64_t idx[4] = {b0, b0 + 1, b0 + w + 1, b0 + w};
+            int axis_on_edge = 0, has_zero = 0;
+            double winding = 0.0;
+            for (int i = 0; i < 4; ++i) {
+                double delta = ac[idx[(i + 1) % 4]] - ac[idx[i]];
+                delta = rem_euclid_tau(delta + OR_PI) - OR_PI;
+                if (fabs(delta) >= OR_PI - 64.0 * OR_EPS) axis_on_edge = 1;
+                winding += delta;
+                if (rc[idx[i]] == 0.0) has_zero = 1;
+            }
+            if (fabs(winding) > OR_PI || axis_on_edge || has_zero) {
+                if (sample_pixel_2d(p, dim2, pixel, unit, g, &e)) rc_ = -1;
+            } else {
+                int done_pixel = 0;
+                if (g->pyfai) {
+                    double poly[8] = {rc[idx[0]], ac[idx[0]], rc[idx[3]], ac[idx[3]],
+                                      rc[idx[2]], ac[idx[2]], rc[idx[1]], ac[idx[1]]};
+                    int m = or_pyfai_split2d(poly, g, 1.0, pb, pw, 4096);
+                    if (m == -2) {
+                        rc_ = -1;
+                    } else if (m >= 0) {
+                        for (int k = 0; k < m && rc_ == 0; ++k)
+                            if (entries_add(&e, pb[k], pw[k])) rc_ = -1;
+                        done_pixel = 1;
+                    }
+                }
+                if (!done_pixel && rc_ == 0) {
+                    double center = g->a0 + rem_euclid_tau(cc[pixel] - g->a0);
+                    pt_t poly[4];
+                    for (int i = 0; i < 4; ++i) {
+                        poly[i].x = rc[idx[i]];
+                        poly[i].y = center + rem_euclid_tau(ac[idx[i]] - center + OR_PI) - OR_PI;
+                    }
+                    double area = fabs(polygon_area(poly, 4));
+                    if (area > 0.0) {
+                        if (split_polygon_2d(poly, area, g, &e)) rc_ = -1;
+                    } else {
+                        int64_t bin = or_grid2d_bin(g, cr[pixel], cc[pixel]);
+                        if (bin >= 0 && entries_add(&e, bin, 1.0)) rc_ = -1;
+                    }
+                }
+            }
+        }
+        for (int64_t k = 0; k < e.n && rc_ == 0; ++k)
+            if (bucket_push(&buckets[e.bin[k]], pixel, e.w[k])) rc_ = -1;
+    }
+    if (rc_ == 0) {
+        rc_ = buckets_to_lut(buckets, nb, 1, g->r0, grid_dr(g), out);
+        buckets = NULL;
+    }
+done:
+    if (buckets) {
+        for (int64_t i = 0; i < nb; ++i) {
+            free(buckets[i].col);
+            free(buckets[i].w);
+        }
+        free(buckets);
+    }
+    free(e.bin);
+    free(e.w);
+    free(cr);
+    free(cc);
+    free(rc);
+    free(ac);
+    return rc_;
+}
+
 /* fixed_table (prepared.rs:163-192). An all-zero mask keeps the table. */
 int or_compact(const or_lut *in, const uint8_t *mask, or_lut *out) {
     memset(out, 0, sizeof(*out));

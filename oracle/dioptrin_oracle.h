@@ -78,6 +78,25 @@ void or_pyfai_radial_range(const or_poni *p, int64_t dim1, int64_t dim2, int uni
                            double *hi);
 int or_build_pf1d(const or_poni *p, int64_t dim1, int64_t dim2, int unit, int64_t n_points,
                   int has_range, double rmin, double rmax, or_lut *out);
+/* 2D tables on an explicit grid (integration/grid.rs:26-222, shared_grid.rs,
+ * pyfai_split.rs, supersampled.rs:1437-1477). */
+typedef struct or_grid2d {
+    int64_t n_radial, n_azimuthal;
+    double r0, r1, a0, a1;
+    int clamp_radial_end, clamp_index_rounding, clamp_radial_outside, clamp_azimuthal_outside;
+    int pyfai; /* pyFAI histogram splitting (pyfai_full) */
+} or_grid2d;
+int or_grid2d_new(int64_t n_radial, int64_t n_azimuthal, double r0, double r1, double a0,
+                  double a1, or_grid2d *g);
+int64_t or_grid2d_bin(const or_grid2d *g, double radial, double azimuthal);
+int or_grid2d_for(const or_poni *p, int64_t dim1, int64_t dim2, int method, int64_t n_ss,
+                  int unit, int64_t n_radial, int64_t n_azimuthal, int has_radial_range,
+                  double rmin, double rmax, int has_azimuthal_range, double amin, double amax,
+                  or_grid2d *g);
+int or_pyfai_split2d(const double *poly, const or_grid2d *g, double sign, int64_t *bins,
+                     double *weights, int64_t cap);
+int or_build_2d(const or_poni *p, int64_t dim1, int64_t dim2, int method, int64_t n_ss,
+                int unit, const or_grid2d *g, or_lut *out);
 int or_build_counting1d(const double *radial, int64_t npix, int64_t n_points, int has_range,
                         double rmin, double rmax, or_lut *out);
 /* Supersampled 1D (supersampled.rs:517-593), exact per-sample path. */

@@ -101,6 +101,13 @@ def _lib():
         lib.or_ps1d_fractions.argtypes = [P(Poni), i64, i64, i, i64, d, d, i, P(_Lut)]
         lib.or_build_counting1d.argtypes = [pd, i64, i64, i, d, d, P(_Lut)]
         lib.or_split1d.argtypes = [pd, i64, d, d, d, d, i, d, P(C.c_int64), pd, i64]
+        lib.or_grid2d_new.argtypes = [i64, i64, d, d, d, d, P(Grid2d)]
+        lib.or_grid2d_bin.argtypes = [P(Grid2d), d, d]
+        lib.or_grid2d_bin.restype = i64
+        lib.or_grid2d_for.argtypes = [P(Poni), i64, i64, i, i64, i, i64, i64, i, d, d, i, d, d,
+                                      P(Grid2d)]
+        lib.or_pyfai_split2d.argtypes = [pd, P(Grid2d), d, P(C.c_int64), pd, i64]
+        lib.or_build_2d.argtypes = [P(Poni), i64, i64, i, i64, i, P(Grid2d), P(_Lut)]
         lib.or_pyfai_radial_range.argtypes = [P(Poni), i64, i64, i, pd, pd]
         lib.or_build_pf1d.argtypes = [P(Poni), i64, i64, i, i64, i, d, d, P(_Lut)]
         lib.or_build_ss1d.argtypes = [P(Poni), i64, i64, i, i64, i64, i, d, d, P(_Lut)]
@@ -200,6 +207,74 @@ def build_ps1d(p: Poni, dim1: int, dim2: int, n_points: int, unit: str = "2th_ra
                               1 if radial_range else 0, rr[0], rr[1], C.byref(lut))
     if rc:
         raise MemoryError("oracle ps1d build failed")
+    return _take(lut)
+
+
+class Grid2d(C.Structure):
+    """IntegrationGrid2d (integration/grid.rs:26-47)."""
+    _fields_ = [("n_radial", C.c_int64), ("n_azimuthal", C.c_int64), ("r0", C.c_double),
+                ("r1", C.c_double), ("a0", C.c_double), ("a1", C.c_double),
+                ("clamp_radial_end", C.c_int), ("clamp_index_rounding", C.c_int),
+                ("clamp_radial_outside", C.c_int), ("clamp_azimuthal_outside", C.c_int),
+                ("pyfai", C.c_int)]
+
+    def bin(self, radial: float, azimuthal: float):
+        b = _lib().or_grid2d_bin(C.byref(self), radial, azimuthal)
+        return None if b < 0 else int(b)
+
+    def radial_centres(self):
+        step = (self.r1 - self.r0) / self.n_radial
+        return np.array([self.r0 + (i + 0.5) * step for i in range(self.n_radial)])
+
+    def azimuthal_centres(self):
+        step = (self.a1 - self.a0) / self.n_azimuthal
+        return np.array([self.a0 + (i + 0.5) * step for i in range(self.n_azimuthal)])
+
+
+METHOD_CODES = {"counting": 0, "pixel_split": 1, "pyfai_full": 2, "supersampled": 3}
+
+
+def grid2d(n_radial: int, n_azimuthal: int, radial_range, azimuthal_range) -> Grid2d:
+    g = Grid2d()
+    if _lib().or_grid2d_new(n_radial, n_azimuthal, radial_range[0], radial_range[1],
+                            azimuthal_range[0], azimuthal_range[1], C.byref(g)):
+        raise ValueError("invalid 2D grid")
+    return g
+
+
+def grid2d_for(p: Poni, dim1: int, dim2: int, method: str, n_radial: int, n_azimuthal: int,
+               unit: str = "2th_rad", n_ss: int = 1, radial_range=None,
+               azimuthal_range=None) -> Grid2d:
+    g = Grid2d()
+    rr = radial_range or (0.0, 0.0)
+    ar = azimuthal_range or (0.0, 0.0)
+    if _lib().or_grid2d_for(C.byref(p), dim1, dim2, METHOD_CODES[method], n_ss, UNITS[unit],
+                            n_radial, n_azimuthal, 1 if radial_range else 0, rr[0], rr[1],
+                            1 if azimuthal_range else 0, ar[0], ar[1], C.byref(g)):
+        raise ValueError("invalid 2D grid")
+    return g
+
+
+def pyfai_split2d(poly, g: Grid2d, sign: float = 1.0):
+    """pyfai_split::split: list of (bin, weight), or None for the fallback."""
+    flat = np.ascontiguousarray(np.asarray(poly, np.float64).ravel())
+    bins = np.zeros(4096, np.int64)
+    w = np.zeros(4096)
+    m = _lib().or_pyfai_split2d(_dp(flat), C.byref(g), sign,
+                                bins.ctypes.data_as(C.POINTER(C.c_int64)), _dp(w), 4096)
+    if m == -1:
+        return None
+    if m < 0:
+        raise ValueError("raster exceeds the oracle buffer")
+    return [(int(bins[k]), float(w[k])) for k in range(m)]
+
+
+def build_2d(p: Poni, dim1: int, dim2: int, method: str, g: Grid2d, unit: str = "2th_rad",
+             n_ss: int = 1) -> Lut:
+    lut = _Lut()
+    if _lib().or_build_2d(C.byref(p), dim1, dim2, METHOD_CODES[method], n_ss, UNITS[unit],
+                          C.byref(g), C.byref(lut)):
+        raise MemoryError("oracle 2D build failed")
     return _take(lut)
 
 

@@ -3,14 +3,15 @@
 The CSR table is built on the GPU and integrated there by hand-written
 sm_100a kernels in libdioptrin_b200.so, reached through the C ABI in
 include/dioptrin_gpu.h. This package mirrors the reference's Python API:
-``Integrator`` with ``integrate1d``, ``batch1d`` and ``batch1d_iter``, and
-``Cuda1dPlan`` from ``Integrator.prepare_cuda1d``.
+``Integrator`` with ``integrate1d``, ``integrate2d``, ``batch1d`` and
+``batch1d_iter``, and ``Cuda1dPlan`` / ``Cuda2dPlan`` from
+``Integrator.prepare_cuda1d`` / ``prepare_cuda2d``.
 """
 from ._native import CudaUnavailableError, RequestTimeout
-from .integrator import (BatchIterator, BatchResult, Cuda1dPlan, IntegrationResult,
-                         Integrator, Poni, cuda_available, cuda_info)
+from .integrator import (BatchIterator, BatchResult, Cuda1dPlan, Cuda2dPlan,
+                         IntegrationResult, Integrator, Poni, cuda_available, cuda_info)
 from .server import RequestLoop
 
-__all__ = ["BatchIterator", "BatchResult", "Cuda1dPlan", "CudaUnavailableError",
+__all__ = ["BatchIterator", "BatchResult", "Cuda1dPlan", "Cuda2dPlan", "CudaUnavailableError",
            "IntegrationResult", "Integrator", "Poni", "RequestLoop", "RequestTimeout",
            "cuda_available", "cuda_info"]

@@ -171,13 +171,14 @@ __global__ void k_minmax(const double *__restrict__ v, int64_t n, unsigned long 
     }
 }
 
-// hull_grid (lut/common.rs:33-65) point k, radial value only.
+// hull_grid (lut/common.rs:33-65) point k: radial extremes into out and,
+// when out_az is given, azimuthal extremes into out_az.
 __global__ void k_hull_minmax(GeomParams g, int dim1, int dim2, int n_ss,
-                              unsigned long long *out) {
+                              unsigned long long *out, unsigned long long *out_az) {
     int64_t a = int64_t(dim1) * n_ss, b = int64_t(dim2) * n_ss - 1;
     int64_t n = 2 * a + 2 * b;
     double off = 0.5 / double(n_ss), st = 1.0 / double(n_ss);
-    unsigned long long lo = ~0ull, hi = 0ull;
+    unsigned long long lo = ~0ull, hi = 0ull, alo = ~0ull, ahi = 0ull;
     for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < n;
          k += int64_t(gridDim.x) * blockDim.x) {
         double d1, d2;
@@ -190,16 +191,27 @@ __global__ void k_hull_minmax(GeomParams g, int dim1, int dim2, int n_ss,
         unsigned long long key = dkey(r);
         lo = key < lo ? key : lo;
         hi = key > hi ? key : hi;
+        key = dkey(chi);
+        alo = key < alo ? key : alo;
+        ahi = key > ahi ? key : ahi;
     }
     for (int o = 16; o > 0; o >>= 1) {
         unsigned long long x = __shfl_down_sync(0xffffffffu, lo, o);
         unsigned long long y = __shfl_down_sync(0xffffffffu, hi, o);
         lo = x < lo ? x : lo;
         hi = y > hi ? y : hi;
+        x = __shfl_down_sync(0xffffffffu, alo, o);
+        y = __shfl_down_sync(0xffffffffu, ahi, o);
+        alo = x < alo ? x : alo;
+        ahi = y > ahi ? y : ahi;
     }
     if ((threadIdx.x & 31) == 0) {
         atomicMin(&out[0], lo);
         atomicMax(&out[1], hi);
+        if (out_az) {
+            atomicMin(&out_az[0], alo);
+            atomicMax(&out_az[1], ahi);
+        }
     }
 }
 
@@ -787,6 +799,411 @@ __global__ void k_ss1d(Ss1d a, const int64_t *__restrict__ off, int32_t *__restr
     }
 }
 
+// ------------------------------------------------------------ 2D tables
+
+// IntegrationGrid2d (grid.rs:26-222) with its steps precomputed on the host
+// as (hi - lo) / n, the reference's radial_step/azimuthal_step.
+struct Grid2 {
+    int nr, na;
+    double r0, r1, a0, a1, dr, da;
+    int clamp_radial_end, clamp_index_rounding, clamp_radial_outside, clamp_azimuthal_outside;
+    int pyfai;
+};
+
+// IntegrationGrid2d::bin (grid.rs:176-222); -1 for no bin.
+__device__ long long bin2d(const Grid2 &g, double radial, double azimuthal) {
+    if (!isfinite(radial) || !isfinite(azimuthal)) return -1;
+    if (!g.clamp_radial_outside &&
+        (radial < g.r0 || radial > g.r1 || (radial == g.r1 && !g.clamp_radial_end)))
+        return -1;
+    double offset;
+    if (g.clamp_azimuthal_outside) {
+        offset = azimuthal - g.a0;
+        const double span = g.a1 - g.a0;
+        if (offset < 0.0) offset = 0.0;
+        if (offset > span) offset = span;
+    } else if (g.clamp_index_rounding) {
+        const double wrapped = (azimuthal >= g.a0 && azimuthal < g.a1)
+                                   ? azimuthal
+                                   : g.a0 + rem_euclid_tau(azimuthal - g.a0);
+        if (wrapped >= g.a1 && g.a1 - g.a0 < kTau) return -1;
+        offset = wrapped - g.a0;
+    } else {
+        const double az = g.a0 + rem_euclid_tau(azimuthal - g.a0);
+        if (az >= g.a1) return -1;
+        offset = az - g.a0;
+    }
+    unsigned long long r = as_usize((radial - g.r0) / g.dr);
+    unsigned long long a = as_usize(offset / g.da);
+    if (g.clamp_radial_end || g.clamp_index_rounding || g.clamp_radial_outside)
+        if (r > (unsigned long long)(g.nr - 1)) r = (unsigned long long)(g.nr - 1);
+    if (g.clamp_index_rounding || g.clamp_azimuthal_outside)
+        if (a > (unsigned long long)(g.na - 1)) a = (unsigned long long)(g.na - 1);
+    if (r < (unsigned long long)g.nr && a < (unsigned long long)g.na)
+        return (long long)(a * (unsigned long long)g.nr + r);
+    return -1;
+}
+
+// Counting 2D (shared_grid.rs:57-61): the pixel centre's bin, weight 1.
+__global__ void k_count2d(Grid2 g, const double *__restrict__ cr, const double *__restrict__ cc,
+                          int64_t n, int32_t *__restrict__ count, int32_t *__restrict__ bin_of) {
+    for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < n;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        const long long b = bin2d(g, cr[p], cc[p]);
+        bin_of[p] = int32_t(b);
+        count[p] = b >= 0;
+    }
+}
+
+constexpr int kEnt2Cap = 128;   // entries of one pixel (fractional / pyFAI split)
+constexpr int kRaster2Cap = 512; // cells of one pixel's pyFAI raster
+
+struct Split2 {
+    Grid2 g;
+    int dim1, dim2;
+    const double *rc, *ac, *cr, *cc;
+};
+
+// Adds w to bin in the pixel's list (repeated bins add up, shared_grid.rs).
+__device__ __forceinline__ void ent_add(int *bins, double *ws, int &m, int bin, double w,
+                                        int *overflow) {
+    for (int k = 0; k < m; ++k)
+        if (bins[k] == bin) {
+            ws[k] += w;
+            return;
+        }
+    if (m == kEnt2Cap) {
+        atomicExch(overflow + 1, 1);
+        return;
+    }
+    bins[m] = bin;
+    ws[m] = w;
+    ++m;
+}
+
+// line (pyfai_split.rs:146-168).
+__device__ void pyfai_line(float *buffer, int stride, Pt start, Pt stop) {
+    if (start.x == stop.x) return;
+    const float slope = __double2float_rn((stop.y - start.y) / (stop.x - start.x));
+    const float intercept = __double2float_rn(stop.y - double(slope) * stop.x);
+    const double lo = fmin(start.x, stop.x), hi = fmax(start.x, stop.x);
+    const double sign = stop.x > start.x ? 1.0 : -1.0;
+    const unsigned long long rb = as_usize(floor(lo)), re = as_usize(ceil(hi));
+    for (unsigned long long r = rb; r < re; ++r) {
+        const double left = fmax(lo, double(r)), right = fmin(hi, double(r + 1));
+        const float area = __double2float_rn(
+            sign * (right - left) * (0.5 * double(slope) * (right + left) + double(intercept)));
+        const float width = __double2float_rn(right - left);
+        float remaining = fabsf(area);
+        for (int a = 0; a < stride; ++a) {
+            if (remaining <= 0.0f) break;
+            const float increment = fminf(width, remaining);
+            float *cell = buffer + int64_t(r) * stride + a;
+            *cell = __fadd_rn(*cell, copysignf(increment, area));
+            remaining = __fsub_rn(remaining, increment);
+        }
+    }
+}
+
+// pyfai_split::split (pyfai_split.rs:35-144) with corner sign +1. Returns the
+// number of entries, -1 for None (fractional fallback).
+__device__ int pyfai_split2(const Grid2 &g, Pt poly[4], int *bins, double *ws, float *buffer,
+                            int *overflow) {
+    const double canonical = (g.a0 >= -kPi && g.a1 <= kPi) ? -kPi
+                             : (g.a0 >= 0.0 && g.a1 <= kTau) ? 0.0
+                                                            : g.a0;
+    const double offset = canonical + kPi;
+    for (int i = 0; i < 4; ++i) poly[i].y = wrap_tau(poly[i].y - offset + kPi) - kPi;
+    const Pt a = poly[0], b = poly[1], c = poly[2], d = poly[3];
+    const double area = 1.0 * (0.5 * (c.x - a.x) * (d.y - b.y) - (c.y - a.y) * (d.x - b.x));
+    if (area > 0.0) {
+        for (int i = 0; i < 4; ++i)
+            if (poly[i].y < 0.0) poly[i].y += kTau;
+        double s = -0.0;
+        for (int i = 0; i < 4; ++i) s += poly[i].y;
+        if (s * 0.25 > kPi)
+            for (int i = 0; i < 4; ++i) poly[i].y -= kTau;
+    }
+    for (int i = 0; i < 4; ++i) poly[i].y += offset;
+    bool lr = true, hr = true, la = true, ha = true;
+    for (int i = 0; i < 4; ++i) {
+        lr &= poly[i].x < g.r0;
+        hr &= poly[i].x > g.r1;
+        la &= poly[i].y < g.a0;
+        ha &= poly[i].y > g.a1;
+    }
+    if (lr || hr || la || ha) return 0;
+    for (int i = 0; i < 4; ++i) {
+        double x = poly[i].x, y = poly[i].y;
+        x = x < g.r0 ? g.r0 : x;
+        x = x > g.r1 ? g.r1 : x;
+        y = y < g.a0 ? g.a0 : y;
+        y = y > g.a1 ? g.a1 : y;
+        poly[i].x = (x - g.r0) / g.dr;
+        poly[i].y = (y - g.a0) / g.da;
+    }
+    double mr = INFINITY, ma = INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        mr = fmin(mr, poly[i].x);
+        ma = fmin(ma, poly[i].y);
+    }
+    const unsigned long long ir = as_usize(floor(mr)), ia = as_usize(floor(ma));
+    for (int i = 0; i < 4; ++i) {
+        poly[i].x -= double(ir);
+        poly[i].y -= double(ia);
+    }
+    double xr = 0.0, xa = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        xr = fmax(xr, poly[i].x);
+        xa = fmax(xa, poly[i].y);
+    }
+    const unsigned long long nr = as_usize(ceil(xr)), na = as_usize(ceil(xa));
+    if (nr == 0 || na == 0) return -1;
+    if ((nr + 1) * (na + 1) > (unsigned long long)kRaster2Cap) {
+        atomicExch(overflow + 1, 1);
+        return 0;
+    }
+    const int stride = int(na + 1);
+    for (int k = 0; k < int((nr + 1) * (na + 1)); ++k) buffer[k] = 0.0f;
+    for (int i = 0; i < 4; ++i) pyfai_line(buffer, stride, poly[i], poly[(i + 1) & 3]);
+    int m = 0;
+    double total = 0.0;
+    for (unsigned long long r = 0; r < nr; ++r)
+        for (unsigned long long q = 0; q < na; ++q) {
+            const double value = 1.0 * double(buffer[r * stride + q]);
+            if (!isfinite(value)) return -1;
+            if (value > 0.0 && ir + r < (unsigned long long)g.nr &&
+                ia + q < (unsigned long long)g.na) {
+                if (m == kEnt2Cap) {
+                    atomicExch(overflow + 1, 1);
+                    return 0;
+                }
+                bins[m] = int((ia + q) * (unsigned long long)g.nr + ir + r);
+                ws[m] = value;
+                total += value;
+                ++m;
+            }
+        }
+    if (total <= 0.0) return -1;
+    for (int k = 0; k < m; ++k) ws[k] /= total;
+    return m;
+}
+
+// split_polygon (shared_grid.rs:152-200).
+__device__ int split_polygon2(const Grid2 &g, const Pt poly[4], double area, int *bins,
+                              double *ws, int *overflow) {
+    double rmn = INFINITY, rmx = -INFINITY;
+    for (int i = 0; i < 4; ++i) {
+        rmn = fmin(rmn, poly[i].x);
+        rmx = fmax(rmx, poly[i].x);
+    }
+    long long rs = as_isize(floor((rmn - g.r0) / g.dr));
+    if (rs < 0) rs = 0;
+    long long re = as_isize(floor((rmx - g.r0) / g.dr));
+    if (re > g.nr - 1) re = g.nr - 1;
+    int m = 0;
+    const double shifts[3] = {-kTau, 0.0, kTau};
+    for (int sh = 0; sh < 3; ++sh) {
+        Pt q[4];
+        double amn = INFINITY, amx = -INFINITY;
+        for (int i = 0; i < 4; ++i) {
+            q[i].x = poly[i].x;
+            q[i].y = poly[i].y + shifts[sh];
+            amn = fmin(amn, q[i].y);
+            amx = fmax(amx, q[i].y);
+        }
+        long long as_ = as_isize(floor((amn - g.a0) / g.da));
+        if (as_ < 0) as_ = 0;
+        long long ae = as_isize(floor((amx - g.a0) / g.da));
+        if (ae > g.na - 1) ae = g.na - 1;
+        for (long long ar = as_; ar <= ae; ++ar)
+            for (long long rr = rs; rr <= re; ++rr) {
+                const double r = g.r0 + double(rr) * g.dr;
+                const double a = g.a0 + double(ar) * g.da;
+                const double w = clipped_area(q, r, r + g.dr, a, a + g.da, overflow) / area;
+                if (w > 0.0) ent_add(bins, ws, m, int(ar * g.nr + rr), w, overflow);
+            }
+    }
+    return m;
+}
+
+// One pixel of shared_grid::build for pixel splitting (shared_grid.rs:62-117):
+// -1 for a pixel sampled on the detector plane.
+__device__ int split2_pixel(const Split2 &s, int64_t pixel, int *bins, double *ws, float *raster,
+                            int *overflow) {
+    const Grid2 &g = s.g;
+    const int64_t w = s.dim2 + 1;
+    const int64_t b0 = pixel / s.dim2 * w + pixel % s.dim2;
+    const int64_t idx[4] = {b0, b0 + 1, b0 + w + 1, b0 + w};
+    bool axis_on_edge = false, has_zero = false;
+    double winding = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        double delta = s.ac[idx[(i + 1) & 3]] - s.ac[idx[i]];
+        delta = rem_euclid_tau(delta + kPi) - kPi;
+        axis_on_edge |= fabs(delta) >= kPi - 64.0 * kEps;
+        winding += delta;
+        has_zero |= s.rc[idx[i]] == 0.0;
+    }
+    if (fabs(winding) > kPi || axis_on_edge || has_zero) return -1;
+    if (g.pyfai) {
+        Pt poly[4] = {{s.rc[idx[0]], s.ac[idx[0]]}, {s.rc[idx[3]], s.ac[idx[3]]},
+                      {s.rc[idx[2]], s.ac[idx[2]]}, {s.rc[idx[1]], s.ac[idx[1]]}};
+        const int m = pyfai_split2(g, poly, bins, ws, raster, overflow);
+        if (m >= 0) return m;
+    }
+    const double center = g.a0 + rem_euclid_tau(s.cc[pixel] - g.a0);
+    Pt poly[4];
+    for (int i = 0; i < 4; ++i) {
+        poly[i].x = s.rc[idx[i]];
+        poly[i].y = center + rem_euclid_tau(s.ac[idx[i]] - center + kPi) - kPi;
+    }
+    const double area = fabs(polygon_area(poly, 4));
+    if (area > 0.0) return split_polygon2(g, poly, area, bins, ws, overflow);
+    const long long b = bin2d(g, s.cr[pixel], s.cc[pixel]);
+    if (b < 0) return 0;
+    bins[0] = int(b);
+    ws[0] = 1.0;
+    return 1;
+}
+
+// FILL = false: counts and lists the sampled pixels; true: writes entries.
+template <bool FILL>
+__global__ void __launch_bounds__(128)
+    k_split2(Split2 s, const int64_t *__restrict__ off, int32_t *__restrict__ count,
+             int32_t *__restrict__ sing, int32_t sing_cap, int32_t *__restrict__ n_sing,
+             int32_t *__restrict__ cbin, double *__restrict__ cw, int32_t *__restrict__ cpix,
+             int *overflow) {
+    const int64_t n = int64_t(s.dim1) * s.dim2;
+    int bins[kEnt2Cap];
+    double ws[kEnt2Cap];
+    float raster[kRaster2Cap];
+    for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < n;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        const int m = split2_pixel(s, p, bins, ws, raster, overflow);
+        if (FILL && m < 0) continue;  // sampled pixel, filled by k_sample2d_fill
+        if (!FILL) {
+            if (m < 0) {
+                const int slot = atomicAdd(n_sing, 1);
+                if (slot < sing_cap) sing[slot] = int32_t(p);
+            }
+            count[p] = m;  // -1 marks a sampled pixel until its count is known
+            continue;
+        }
+        const int64_t o = off[p];
+        for (int k = 0; k < m; ++k) {
+            cbin[o + k] = bins[k];
+            cw[o + k] = ws[k];
+            cpix[o + k] = int32_t(p);
+        }
+    }
+}
+
+// sample_pixel (shared_grid.rs:202-232) for sampled pixel blockIdx.x of a
+// batch: 128 x 128 x 4 detector-plane samples counted per grid bin.
+__global__ void k_sample2d(GeomParams gp, Grid2 g, int dim2, const int32_t *__restrict__ sing,
+                           int32_t *__restrict__ hits) {
+    const int N = 128;
+    const double off[4][2] = {{0.25, 0.5}, {0.5, 0.25}, {0.75, 0.5}, {0.5, 0.75}};
+    const int32_t pixel = sing[blockIdx.x];
+    int32_t *h = hits + int64_t(blockIdx.x) * g.nr * g.na;
+    const int64_t row = pixel / dim2, col = pixel % dim2;
+    for (int sm = threadIdx.x; sm < N * N * 4; sm += blockDim.x) {
+        const int i = sm / (N * 4), j = (sm / 4) % N, o = sm & 3;
+        const double d1 = double(row) + (double(i) + off[o][0]) / double(N);
+        const double d2 = (double(col * N + j) + off[o][1]) / double(N);
+        double r, az;
+        radial_chi(gp, d1, d2, r, az);
+        const long long b = bin2d(g, r, az);
+        if (b >= 0) atomicAdd(&h[b], 1);
+    }
+}
+
+// Entry count of each sampled pixel of a batch (bins with hits).
+__global__ void k_sample2d_count(const int32_t *__restrict__ sing, int64_t nb,
+                                 const int32_t *__restrict__ hits, int32_t *__restrict__ count) {
+    const int32_t *h = hits + int64_t(blockIdx.x) * nb;
+    int c = 0;
+    for (int64_t b = threadIdx.x; b < nb; b += blockDim.x) c += h[b] != 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    __shared__ int wsum[32];
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int i = 0; i < int(blockDim.x + 31) / 32; ++i) t += wsum[i];
+        count[sing[blockIdx.x]] = t;
+    }
+}
+
+// Entries of each sampled pixel of a batch, bins ascending, weight hits/65536
+// (the sum of hits samples of weight 2^-16, exact).
+__global__ void k_sample2d_fill(const int32_t *__restrict__ sing, int64_t nb,
+                                const int32_t *__restrict__ hits, const int64_t *__restrict__ off,
+                                int32_t *__restrict__ cbin, double *__restrict__ cw,
+                                int32_t *__restrict__ cpix) {
+    if (threadIdx.x != 0) return;
+    const int32_t pixel = sing[blockIdx.x];
+    const int32_t *h = hits + int64_t(blockIdx.x) * nb;
+    int64_t o = off[pixel];
+    for (int64_t b = 0; b < nb; ++b)
+        if (h[b]) {
+            cbin[o] = int32_t(b);
+            cw[o] = double(h[b]) / 65536.0;
+            cpix[o] = pixel;
+            ++o;
+        }
+}
+
+// build_shared_grid_ss_csr through the exact counted path (supersampled.rs
+// :1437-1477, :21-104, normalize_bins false): samples d1 = row + (i+.5)/n,
+// d2 = ((col*n + j) + .5)/n, distinct grid bins in first-seen order, weight
+// count / n^2.
+__global__ void k_ss2d(GeomParams gp, Grid2 g, int dim1, int dim2, int n_ss,
+                       const int64_t *__restrict__ off, int32_t *__restrict__ count,
+                       int32_t *__restrict__ cbin, double *__restrict__ cw,
+                       int32_t *__restrict__ cpix) {
+    const int64_t n = int64_t(dim1) * dim2;
+    int bins[kMaxSs * kMaxSs], cnt[kMaxSs * kMaxSs];
+    for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < n;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t row = p / dim2, col = p % dim2;
+        int nc = 0;
+        for (int i = 0; i < n_ss; ++i) {
+            const double d1 = double(row) + (double(i) + 0.5) / double(n_ss);
+            for (int j = 0; j < n_ss; ++j) {
+                const double d2 = (double(col * n_ss + j) + 0.5) / double(n_ss);
+                double r, az;
+                radial_chi(gp, d1, d2, r, az);
+                const long long b = bin2d(g, r, az);
+                if (b < 0) continue;
+                int f = -1;
+                for (int q = 0; q < nc; ++q)
+                    if (bins[q] == int(b)) {
+                        f = q;
+                        break;
+                    }
+                if (f < 0) {
+                    bins[nc] = int(b);
+                    cnt[nc++] = 1;
+                } else {
+                    cnt[f]++;
+                }
+            }
+        }
+        if (!off) {
+            count[p] = nc;
+            continue;
+        }
+        const int64_t o = off[p];
+        const double denom = double(n_ss * n_ss);
+        for (int q = 0; q < nc; ++q) {
+            cbin[o + q] = bins[q];
+            cw[o + q] = double(cnt[q]) / denom;
+            cpix[o + q] = int32_t(p);
+        }
+    }
+}
+
 // ------------------------------------------------ ordered transpose
 
 __global__ void k_chunk_count(const int32_t *__restrict__ cbin, const int32_t *__restrict__ cpix,
@@ -952,12 +1369,260 @@ void transpose(const int32_t *cbin, const double *cw, const int32_t *cpix,
 
 }  // namespace
 
+namespace {
+
+// IntegrationGrid2d::new (grid.rs:49-105) on host values; the azimuthal start
+// is corrected into [-pi, pi) when it lies outside +-2pi.
+void grid2_new(int nr, int na, double r0, double r1, double a0, double a1, Grid2 &g) {
+    const double lo[2] = {r0, a0}, hi[2] = {r1, a1};
+    const int cnt[2] = {nr, na};
+    const char *name[2] = {"radial", "azimuthal"};
+    for (int k = 0; k < 2; ++k) {
+        const double step = (hi[k] - lo[k]) / double(cnt[k]);
+        if (!std::isfinite(lo[k]) || !std::isfinite(hi[k]) || !std::isfinite(step) ||
+            step <= 0.0 || lo[k] + step == lo[k] || hi[k] - step == hi[k])
+            fail(DG_INVALID_INPUT, std::string(name[k]) +
+                                       " range must have finite, increasing, resolvable bin edges");
+    }
+    if (r0 < 0.0) fail(DG_INVALID_INPUT, "radial range must be nonnegative");
+    if (a1 - a0 > kTau + 1e-12)
+        fail(DG_INVALID_INPUT, "azimuthal span must be at most 2pi (one full turn)");
+    if (!(a0 >= -kTau && a0 <= kTau)) {
+        double start = std::fmod(a0, kTau);
+        if (start < 0.0) start += kTau;
+        if (start >= kPi) start -= kTau;
+        const double span = a1 - a0;
+        a0 = start;
+        a1 = start + span;
+    }
+    g = Grid2{};
+    g.nr = nr;
+    g.na = na;
+    g.r0 = r0;
+    g.r1 = r1;
+    g.a0 = a0;
+    g.a1 = a1;
+    g.dr = (r1 - r0) / double(nr);
+    g.da = (a1 - a0) / double(na);
+}
+
+// 2D tables: the grid of prepare_cuda2d (cuda.rs:1111-1157; edges and clamps
+// of methods.rs:365-388 and grid.rs:579-624, :700-755, :975-1028), then
+// shared_grid::build (shared_grid.rs:13-150) or the supersampled counted
+// table, transposed into rows a * n_radial + r.
+void build_table_2d(const dg_geometry &geom, const dg_method &m, int32_t dim1, int32_t dim2,
+                    int32_t nr, int32_t na, const double *azimuthal_range, cudaStream_t s,
+                    BuildResult &out) {
+    GeomParams gp = make_geom_params(geom, m);
+    const int64_t npix = int64_t(dim1) * dim2;
+    const int64_t ncorner = int64_t(dim1 + 1) * (dim2 + 1);
+    const int64_t nb = int64_t(nr) * na;
+    if (nb > INT32_MAX) fail(DG_INVALID_INPUT, "2D bin count must be in 1..=2147483647");
+    const double eps = DBL_EPSILON;
+    if (azimuthal_range) {
+        Grid2 probe;
+        grid2_new(nr, na, 0.0, 1.0, azimuthal_range[0], azimuthal_range[1], probe);
+    }
+    if (m.kind == DG_METHOD_SUPERSAMPLED && (m.n_ss < 1 || m.n_ss > kMaxSs))
+        fail(DG_UNSUPPORTED, "supersampling factor must be between 1 and 8");
+
+    DeviceArray<double> cr, cc, rc, ac;
+    cr.alloc(npix);
+    cc.alloc(npix);
+    rc.alloc(ncorner);
+    ac.alloc(ncorner);
+    out.norm.alloc(npix);
+    k_centres<<<grid_for(npix), 256, 0, s>>>(gp, dim1, dim2, cr.ptr, cc.ptr, out.norm.ptr);
+    k_corners<<<grid_for(ncorner), 256, 0, s>>>(gp, dim1, dim2, rc.ptr, ac.ptr);
+    DG_CUDA(cudaGetLastError());
+    DeviceArray<unsigned long long> mm;
+    mm.alloc(12);
+    unsigned long long init[12];
+    for (int i = 0; i < 12; i += 2) {
+        init[i] = ~0ull;
+        init[i + 1] = 0ull;
+    }
+    DG_CUDA(cudaMemcpyAsync(mm.ptr, init, sizeof init, cudaMemcpyHostToDevice, s));
+    k_minmax<<<grid_for(npix), 256, 0, s>>>(cr.ptr, npix, mm.ptr);
+    k_minmax<<<grid_for(npix), 256, 0, s>>>(cc.ptr, npix, mm.ptr + 2);
+    k_minmax<<<grid_for(ncorner), 256, 0, s>>>(rc.ptr, ncorner, mm.ptr + 4);
+    k_minmax<<<grid_for(ncorner), 256, 0, s>>>(ac.ptr, ncorner, mm.ptr + 6);
+    if (m.kind == DG_METHOD_SUPERSAMPLED)
+        k_hull_minmax<<<grid_for(2 * (int64_t(dim1) + dim2) * m.n_ss), 256, 0, s>>>(
+            gp, dim1, dim2, m.n_ss, mm.ptr + 8, mm.ptr + 10);
+    DG_CUDA(cudaGetLastError());
+    auto k = to_host(mm.ptr, 12, s);
+    double ext[12];
+    for (int i = 0; i < 12; ++i) ext[i] = key_to_double(k[size_t(i)]);
+    // ext: centre radial lo/hi, centre chi lo/hi, corner radial lo/hi, corner
+    // chi lo/hi, hull radial lo/hi, hull chi lo/hi.
+    double r0, r1, a0, a1;
+    if (m.has_radial_range) {
+        r0 = m.radial_min;
+        r1 = m.radial_max;
+    } else if (m.kind == DG_METHOD_COUNTING) {
+        r0 = ext[0];
+        r1 = ext[1] + 10.0 * eps;
+    } else if (m.kind == DG_METHOD_PIXEL_SPLIT) {
+        r0 = ext[4];
+        r1 = ext[5] + 10.0 * eps;
+    } else if (m.kind == DG_METHOD_PYFAI_FULL) {
+        r0 = std::fmax(ext[4], 0.0);
+        r1 = ext[5] * (1.0 + double(FLT_EPSILON));
+    } else {
+        r0 = std::fmin(ext[0], ext[8]);
+        r1 = std::fmax(ext[1], ext[9]) + 3.0 * eps;
+    }
+    if (azimuthal_range) {
+        a0 = azimuthal_range[0];
+        a1 = azimuthal_range[1];
+    } else if (m.kind == DG_METHOD_PYFAI_FULL) {
+        a0 = -kPi;
+        a1 = kPi;
+    } else {
+        if (m.kind == DG_METHOD_COUNTING) {
+            a0 = ext[2];
+            a1 = ext[3] + 10.0 * eps;
+        } else if (m.kind == DG_METHOD_SUPERSAMPLED) {
+            a0 = std::fmin(ext[2], ext[10]);
+            a1 = std::fmax(ext[3], ext[11]) + 3.0 * eps;
+        } else {
+            a0 = ext[6];
+            a1 = ext[7] + 10.0 * eps;
+        }
+        if (!(a1 - a0 > 1e-12)) {
+            a0 = -kPi;
+            a1 = kPi;
+        }
+    }
+    Grid2 g;
+    grid2_new(nr, na, r0, r1, a0, a1, g);
+    g.clamp_index_rounding = 1;
+    if (m.kind == DG_METHOD_PYFAI_FULL) g.pyfai = 1;
+    else if (!m.has_radial_range && m.kind == DG_METHOD_COUNTING) g.clamp_radial_end = 1;
+    else if (!m.has_radial_range && m.kind == DG_METHOD_SUPERSAMPLED) g.clamp_radial_outside = 1;
+    if (m.kind == DG_METHOD_SUPERSAMPLED && !azimuthal_range) g.clamp_azimuthal_outside = 1;
+    out.hist_min = g.r0;
+    out.hist_step = g.dr;
+    out.radial_centres.resize(size_t(nr));
+    for (int i = 0; i < nr; ++i) out.radial_centres[size_t(i)] = g.r0 + (double(i) + 0.5) * g.dr;
+    out.azimuthal_centres.resize(size_t(na));
+    for (int i = 0; i < na; ++i)
+        out.azimuthal_centres[size_t(i)] = g.a0 + (double(i) + 0.5) * g.da;
+
+    DeviceArray<int32_t> count;
+    count.alloc(npix + 1);
+    DG_CUDA(cudaMemsetAsync(count.ptr, 0, count.bytes(), s));
+    DeviceArray<int64_t> off;
+    off.alloc(npix + 1);
+    DeviceArray<unsigned char> scan_tmp;
+    scan_tmp.alloc(scan_temp_bytes(npix + 1));
+    DeviceArray<int32_t> cbin, cpix;
+    DeviceArray<double> cw;
+    DeviceArray<int> flags;
+    flags.alloc(2);
+    DG_CUDA(cudaMemsetAsync(flags.ptr, 0, flags.bytes(), s));
+    auto scan_counts = [&]() -> int64_t {
+        exclusive_scan_i32_to_i64(count.ptr, off.ptr, npix + 1, scan_tmp.ptr, s);
+        int64_t total = 0;
+        DG_CUDA(cudaMemcpyAsync(&total, off.ptr + npix, sizeof total, cudaMemcpyDeviceToHost, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        if (total > int64_t(INT32_MAX) - 128)
+            fail(DG_UNSUPPORTED, "lookup table of " + std::to_string(total) +
+                                     " entries exceeds 32-bit indexing");
+        cbin.alloc(size_t(total));
+        cpix.alloc(size_t(total));
+        cw.alloc(size_t(total));
+        return total;
+    };
+    int64_t ncoo = 0;
+    if (m.kind == DG_METHOD_COUNTING) {
+        DeviceArray<int32_t> bin_of;
+        bin_of.alloc(npix);
+        k_count2d<<<grid_for(npix), 256, 0, s>>>(g, cr.ptr, cc.ptr, npix, count.ptr, bin_of.ptr);
+        DG_CUDA(cudaGetLastError());
+        ncoo = scan_counts();
+        k_count1d_fill<<<grid_for(npix), 256, 0, s>>>(bin_of.ptr, npix, off.ptr, cbin.ptr,
+                                                      cw.ptr, cpix.ptr);
+        DG_CUDA(cudaGetLastError());
+    } else if (m.kind == DG_METHOD_SUPERSAMPLED) {
+        k_ss2d<<<grid_for(npix, 128), 128, 0, s>>>(gp, g, dim1, dim2, m.n_ss, nullptr, count.ptr,
+                                                   nullptr, nullptr, nullptr);
+        DG_CUDA(cudaGetLastError());
+        ncoo = scan_counts();
+        k_ss2d<<<grid_for(npix, 128), 128, 0, s>>>(gp, g, dim1, dim2, m.n_ss, off.ptr, count.ptr,
+                                                   cbin.ptr, cw.ptr, cpix.ptr);
+        DG_CUDA(cudaGetLastError());
+    } else {
+        Split2 sp{};
+        sp.g = g;
+        sp.dim1 = dim1;
+        sp.dim2 = dim2;
+        sp.rc = rc.ptr;
+        sp.ac = ac.ptr;
+        sp.cr = cr.ptr;
+        sp.cc = cc.ptr;
+        const int32_t sing_cap = 1 << 16;
+        DeviceArray<int32_t> sing, n_sing;
+        sing.alloc(sing_cap);
+        n_sing.alloc(1);
+        DG_CUDA(cudaMemsetAsync(n_sing.ptr, 0, sizeof(int32_t), s));
+        k_split2<false><<<grid_for(npix, 128), 128, 0, s>>>(sp, nullptr, count.ptr, sing.ptr,
+                                                             sing_cap, n_sing.ptr, nullptr,
+                                                             nullptr, nullptr, flags.ptr);
+        DG_CUDA(cudaGetLastError());
+        const int32_t ns = to_host(n_sing.ptr, 1, s)[0];
+        if (ns > sing_cap) fail(DG_UNSUPPORTED, "too many singular pixels for sampling");
+        out.singular_pixels = ns;
+        // Sampled pixels in batches, each with a hit count per grid bin; the
+        // fill below samples them again (integer counts, order-independent).
+        const int64_t batch = std::max<int64_t>(1, std::min<int64_t>(64, (int64_t(1) << 28) / nb));
+        DeviceArray<int32_t> hits;
+        if (ns > 0) {
+            std::vector<int32_t> hs = to_host(sing.ptr, size_t(ns), s);
+            std::sort(hs.begin(), hs.end());
+            DG_CUDA(cudaMemcpyAsync(sing.ptr, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, s));
+            hits.alloc(size_t(std::min<int64_t>(batch, ns) * nb));
+            for (int64_t b0 = 0; b0 < ns; b0 += batch) {
+                const int nbat = int(std::min<int64_t>(batch, ns - b0));
+                DG_CUDA(cudaMemsetAsync(hits.ptr, 0, size_t(nbat) * nb * 4, s));
+                k_sample2d<<<nbat, 256, 0, s>>>(gp, g, dim2, sing.ptr + b0, hits.ptr);
+                k_sample2d_count<<<nbat, 256, 0, s>>>(sing.ptr + b0, nb, hits.ptr, count.ptr);
+                DG_CUDA(cudaGetLastError());
+            }
+        }
+        ncoo = scan_counts();
+        k_split2<true><<<grid_for(npix, 128), 128, 0, s>>>(sp, off.ptr, count.ptr, nullptr, 0,
+                                                            nullptr, cbin.ptr, cw.ptr, cpix.ptr,
+                                                            flags.ptr);
+        DG_CUDA(cudaGetLastError());
+        for (int64_t b0 = 0; b0 < ns; b0 += batch) {
+            const int nbat = int(std::min<int64_t>(batch, ns - b0));
+            DG_CUDA(cudaMemsetAsync(hits.ptr, 0, size_t(nbat) * nb * 4, s));
+            k_sample2d<<<nbat, 256, 0, s>>>(gp, g, dim2, sing.ptr + b0, hits.ptr);
+            k_sample2d_fill<<<nbat, 32, 0, s>>>(sing.ptr + b0, nb, hits.ptr, off.ptr, cbin.ptr,
+                                                cw.ptr, cpix.ptr);
+            DG_CUDA(cudaGetLastError());
+        }
+    }
+    int hflags[2] = {0, 0};
+    DG_CUDA(cudaMemcpyAsync(hflags, flags.ptr, sizeof hflags, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
+    if (hflags[0]) fail(DG_UNSUPPORTED, "polygon clipping exceeded its vertex capacity");
+    if (hflags[1])
+        fail(DG_UNSUPPORTED, "a pixel covers more 2D bins than the builder's per-pixel capacity");
+    transpose(cbin.ptr, cw.ptr, cpix.ptr, off.ptr, npix, ncoo, int(nb), s, out.full);
+}
+
+}  // namespace
+
 void build_table(const dg_geometry &geom, const dg_method &m, int32_t dim1, int32_t dim2,
                  int32_t n_radial, int32_t n_azimuthal, const double *azimuthal_range,
                  cudaStream_t s, BuildResult &out) {
-    if (n_azimuthal != 0)
-        fail(DG_UNSUPPORTED, "2D tables are not built by this version of the library");
-    (void)azimuthal_range;
+    if (n_azimuthal != 0) {
+        build_table_2d(geom, m, dim1, dim2, n_radial, n_azimuthal, azimuthal_range, s, out);
+        return;
+    }
     GeomParams g = make_geom_params(geom, m);
     const int64_t npix = int64_t(dim1) * dim2;
     const int64_t ncorner = int64_t(dim1 + 1) * (dim2 + 1);
@@ -1129,7 +1794,7 @@ void build_table(const dg_geometry &geom, const dg_method &m, int32_t dim1, int3
             // ss_tth_min_max_step (histogram.rs:151-166): centres and hull.
             k_minmax<<<grid_for(npix), 256, 0, s>>>(cr.ptr, npix, mm.ptr);
             k_hull_minmax<<<grid_for(2 * (int64_t(dim1) + dim2) * m.n_ss), 256, 0, s>>>(
-                g, dim1, dim2, m.n_ss, mm.ptr + 2);
+                g, dim1, dim2, m.n_ss, mm.ptr + 2, nullptr);
             DG_CUDA(cudaGetLastError());
             auto k = to_host(mm.ptr, 4, s);
             double c_lo = key_to_double(k[0]), c_hi = key_to_double(k[1]);

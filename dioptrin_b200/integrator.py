@@ -281,6 +281,60 @@ class Cuda1dPlan:
                                   None if d is None else d[k]) for k in range(len(i))]
 
 
+class Cuda2dPlan(Cuda1dPlan):
+    """A fixed-mask 2D table resident in HBM (src/integration/cuda.rs:620-870,
+    dioptrin.pyi:1463-1520): bins are the rows a * n_radial + r of an
+    n_azimuthal x n_radial cake."""
+
+    def __init__(self, handle, shape, n_radial, n_azimuthal, precision, device,
+                 axes_given: bool):
+        super().__init__(handle, shape, n_radial, precision, device, n_azimuthal)
+        az = np.empty(n_azimuthal)
+        N.check(N.lib().dg_plan_azimuthal(self._h, _dp(az), n_azimuthal))
+        self._azimuthal = az
+        self._axes_given = axes_given
+
+    @property
+    def n_radial(self) -> int:
+        return self.n_points
+
+    @property
+    def azimuthal(self) -> list:
+        return self._azimuthal.tolist()
+
+    @property
+    def azimuthal_array(self) -> np.ndarray:
+        return self._azimuthal
+
+    def _result(self, i, s) -> IntegrationResult:
+        return IntegrationResult(self._radial if self._axes_given else None, i, s,
+                                 azimuthal=self._azimuthal if self._axes_given else None,
+                                 n_radial=self.n_points, n_azimuthal=self.n_azimuthal)
+
+    def integrate2d(self, image: np.ndarray, *, errors: bool = False) -> IntegrationResult:
+        a = _frame_array(image)
+        i, s, _ = self.integrate_stack(a, errors)
+        return self._result(i[0], None if s is None else s[0])
+
+    def batch2d(self, images, *, errors: bool = False) -> list:
+        if isinstance(images, np.ndarray) and images.ndim == 3:
+            stack = images
+        else:
+            arrays = [_frame_array(a) for a in images]
+            if not arrays:
+                return []
+            if len({a.dtype for a in arrays}) > 1:
+                raise TypeError("all images of one call must have the same dtype")
+            stack = np.stack(arrays)
+        i, s, _ = self.integrate_stack(stack, errors)
+        return [self._result(i[k], None if s is None else s[k]) for k in range(len(i))]
+
+    def integrate1d(self, *a, **k):
+        raise TypeError("a 2D plan integrates with integrate2d")
+
+    batch1d = integrate1d
+
+
 class BatchIterator(Iterator[BatchResult]):
     """Streaming results in input order (src/batch/bounded.rs:172-420,
     dioptrin.pyi:277-335): frames are gathered into device batches of up to
@@ -483,6 +537,70 @@ class Integrator:
         N.check(N.lib().dg_plan_create(C.byref(self.poni._c()), C.byref(m), mask, dim1, dim2,
                                        int(n_points), 0, None, C.byref(h)))
         return Cuda1dPlan(h, (dim1, dim2), int(n_points), precision, device)
+
+    def prepare_cuda2d(self, shape, n_radial: int, n_azimuthal: Optional[int] = None, *,
+                       azimuthal_range=None, azimuthal_bracket: Optional[float] = None,
+                       precision: str = "f32_compensated", device: int = 0,
+                       max_batch_bytes: Optional[int] = None,
+                       keep_tables: bool = False) -> Cuda2dPlan:
+        """Integrator::prepare_cuda2d (src/integration/cuda.rs:1111-1157): the
+        2D table on the shared grid of the method (default or explicit radial
+        and azimuthal edges) is built on the device and kept there."""
+        if azimuthal_bracket is not None:
+            raise NotImplementedError("azimuthal_bracket rows are not supported by this build; "
+                                      "give n_azimuthal and azimuthal_range")
+        if n_azimuthal is None:
+            raise ValueError("give n_azimuthal")
+        if n_radial <= 0 or n_azimuthal <= 0:
+            raise ValueError("n_radial and n_azimuthal must be positive")
+        if n_radial * n_azimuthal > 2147483647:
+            raise ValueError(f"2D bin count ({n_radial} x {n_azimuthal}) must be in "
+                             "1..=2147483647")
+        if precision not in N.PRECISIONS:
+            raise ValueError(f"unknown CUDA precision {precision!r}")
+        if device < 0:
+            raise OverflowError("device must be non-negative")
+        if max_batch_bytes is not None and max_batch_bytes <= 0:
+            raise ValueError("max_batch_bytes must be positive")
+        dim1, dim2 = (int(v) for v in shape)
+        if self._mask is not None and self._mask.shape != (dim1, dim2):
+            raise ValueError(f"image shape ({dim1}, {dim2}) does not match mask shape "
+                             f"{self._mask.shape}")
+        m = self._method_struct(precision, device, max_batch_bytes or 0, keep_tables)
+        h = C.c_void_p()
+        mask = (None if self._mask is None
+                else self._mask.ctypes.data_as(C.POINTER(C.c_uint8)))
+        rng = None
+        if azimuthal_range is not None:
+            rng = (C.c_double * 2)(float(azimuthal_range[0]), float(azimuthal_range[1]))
+        N.check(N.lib().dg_plan_create(C.byref(self.poni._c()), C.byref(m), mask, dim1, dim2,
+                                       int(n_radial), int(n_azimuthal), rng, C.byref(h)))
+        axes = azimuthal_range is not None or self._radial_range is not None
+        return Cuda2dPlan(h, (dim1, dim2), int(n_radial), int(n_azimuthal), precision, device,
+                          axes)
+
+    def integrate2d(self, image, n_radial: int, n_azimuthal: Optional[int] = None,
+                    errors: bool = False, azimuthal_range=None, *,
+                    azimuthal_bracket: Optional[float] = None) -> IntegrationResult:
+        """Integrator.integrate2d (dioptrin.pyi:660-730): a flat cake of
+        n_azimuthal x n_radial bins (row a * n_radial + r)."""
+        a = _frame_array(image)
+        key = ("2d", a.shape, int(n_radial), n_azimuthal,
+               None if azimuthal_range is None else tuple(float(v) for v in azimuthal_range))
+        with self._lock:
+            p = self._plans.get(key)
+            if p is None:
+                p = self.prepare_cuda2d(a.shape, n_radial, n_azimuthal,
+                                        azimuthal_range=azimuthal_range,
+                                        azimuthal_bracket=azimuthal_bracket,
+                                        precision=self.precision, device=self.device)
+                self._plans[key] = p
+        return p.integrate2d(a, errors=errors)
+
+    def integrate2d_on_azimuthal_range(self, image, n_radial: int, n_azimuthal: int,
+                                       azimuthal_range, errors: bool = False) -> IntegrationResult:
+        """Integrator::integrate2d_on_azimuthal_range (src/integration/grid.rs:439)."""
+        return self.integrate2d(image, n_radial, n_azimuthal, errors, azimuthal_range)
 
     def _plan(self, shape, n_points: int) -> Cuda1dPlan:
         key = (tuple(shape), int(n_points))

@@ -121,16 +121,35 @@ class ClockSampler:
                 "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
-def cpu_reference(w, frames_np, threads: int, budget_s: float, n_steps: int):
-    """Times the oracle (restated reference CPU algorithm) frame-parallel on
-    host cores; returns (frames/s, frames per sample, seconds)."""
+def oracle_tables(w):
+    """The oracle's unmasked and masked tables, normalisation and denominators
+    for workload w (1D or 2D, any method)."""
     from oracle import oracle as o
     p = o.poni(**w.poni_dict())
-    full = o.build_ps1d(p, w.dim1, w.dim2, w.n_points)
+    if w.n_azimuthal:
+        g = o.grid2d_for(p, w.dim1, w.dim2, w.method, w.n_points, w.n_azimuthal,
+                         n_ss=w.n_ss or 1, azimuthal_range=w.azimuthal_range)
+        full = o.build_2d(p, w.dim1, w.dim2, w.method, g, n_ss=w.n_ss or 1)
+    elif w.method == "pixel_split":
+        full = o.build_ps1d(p, w.dim1, w.dim2, w.n_points)
+    elif w.method == "pyfai_full":
+        full = o.build_pf1d(p, w.dim1, w.dim2, w.n_points)
+    elif w.method == "supersampled":
+        full = o.build_ss1d(p, w.dim1, w.dim2, w.n_points, w.n_ss)
+    else:
+        full = o.build_counting1d(o.centres(p, w.dim1, w.dim2)["radial"], w.n_points)
     mask = w.mask().ravel()
     norm = o.centres(p, w.dim1, w.dim2, polarization_factor=w.polarization_factor)["norm"]
     table = o.compact(full, mask)
     den = o.denominators(table, norm)
+    return full, table, mask, norm, den
+
+
+def cpu_reference(w, frames_np, threads: int, budget_s: float, n_steps: int):
+    """Times the oracle (restated reference CPU algorithm) frame-parallel on
+    host cores; returns (frames/s, frames per sample, seconds)."""
+    from oracle import oracle as o
+    full, table, mask, norm, den = oracle_tables(w)
     # calibrate on a small sample, then size the per-step sample to the budget
     t = time.perf_counter()
     o.integrate_frames_mt(table, den, full, mask, norm, frames_np[:2], w.errors,
@@ -151,16 +170,18 @@ def run_reference(args, w):
     from dioptrin_b200 import workloads as W
     threads = os.cpu_count() or 1
     n_src = 16
-    frames = W.frames_numpy(w, n_src)
+    frames = W.frames_numpy(w, n_src, kind=w.kind)
     steps = args.steps + args.warmup
     rate, per_step, secs = cpu_reference(w, frames, threads, 120.0, steps)
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(rate, 3), "unit": "frames/s",
+        "impl": "reference", "metric": metric_of(w), "value": round(rate, 3),
+        "unit": "frames/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * per_step / rate, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "frames_per_step": per_step, "n_points": w.n_points,
-                   "method": w.method, "errors": w.errors, "azimuthal_std": w.azimuthal_std},
+                   "n_azimuthal": w.n_azimuthal, "method": w.method, "errors": w.errors,
+                   "azimuthal_std": w.azimuthal_std},
         "cpu_baseline": {"value": round(rate, 3), "unit": "frames/s", "cores": threads,
                          "kind": "port",
                          "sample": f"{per_step} frames per step x {steps} steps of {w.name}; "
@@ -170,6 +191,42 @@ def run_reference(args, w):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def metric_of(w) -> str:
+    return METRIC if w.name == "eiger4m_ps2000_b256" else f"{w.name}_frames_per_s"
+
+
+def precision_report(w, frames, oi, os_, od, n: int = 4):
+    """Max and RMS relative error of intensity, sigma and the spread against
+    the FP64 oracle on the first n frames (bins with a nonzero finite
+    reference value)."""
+    import numpy as np
+    from oracle import oracle as o
+    full, table, mask, norm, den = oracle_tables(w)
+    fr = frames[:n].cpu().numpy()
+    gi, gs, gd = oi[:n].cpu().numpy(), os_[:n].cpu().numpy(), od[:n].cpu().numpy()
+    errs = {"intensity": [], "sigma": [], "azimuthal_std": []}
+    for k in range(len(fr)):
+        sig = fr[k].astype(np.float64).ravel()
+        yi, ys = o.integrate_strict(table, den, sig, True)
+        errs["intensity"].append((gi[k], yi))
+        if w.errors:
+            errs["sigma"].append((gs[k], ys))
+        if w.azimuthal_std:
+            _, _, sd = o.azimuthal_std(full, mask, norm, sig, np.maximum(sig, 0))
+            errs["azimuthal_std"].append((gd[k], sd))
+    out = {"frames": int(len(fr)), "reference": "FP64 oracle (strict sums)"}
+    for name, pairs in errs.items():
+        if not pairs:
+            continue
+        got = np.concatenate([a for a, _ in pairs])
+        ref = np.concatenate([b for _, b in pairs])
+        ok = np.isfinite(ref) & (ref != 0)
+        rel = np.abs(got[ok] - ref[ok]) / np.abs(ref[ok])
+        out[name] = {"max_rel": float(rel.max()), "rms_rel": float(np.sqrt(np.mean(rel ** 2))),
+                     "bins": int(ok.sum())}
+    return out
 
 
 def main():
@@ -200,11 +257,15 @@ def main():
     it = dg.Integrator.from_poni_dict(w.poni_dict(), method=w.method, n_ss=w.n_ss,
                                       polarization_factor=w.polarization_factor)
     it.set_mask(w.mask())
-    plan = it.prepare_cuda1d(w.shape, w.n_points, device=local)
+    if w.n_azimuthal:
+        plan = it.prepare_cuda2d(w.shape, w.n_points, w.n_azimuthal,
+                                 azimuthal_range=w.azimuthal_range, device=local)
+    else:
+        plan = it.prepare_cuda1d(w.shape, w.n_points, device=local)
     info = plan.info()
     L = N.lib()
-    frames = W.frames_torch(w, n_frames, device=f"cuda:{local}")
-    nb = w.n_points
+    frames = W.frames_torch(w, n_frames, device=f"cuda:{local}", kind=w.kind)
+    nb = w.n_points * max(1, w.n_azimuthal)
     oi = torch.empty((n_frames, nb), dtype=torch.float64, device=frames.device)
     os_ = torch.empty_like(oi)
     od = torch.empty_like(oi)
@@ -274,12 +335,15 @@ def main():
     achieved = alg / per_launch_s / 1e9
     peak, peak_kind = peaks()
     line = {
-        "metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": world,
+        "metric": metric_of(w), "value": round(value, 2), "unit": "frames/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"uint16": "u16", "uint32": "u32", "int32": "i32", "float32": "f32",
+                  "float64": "f64"}[w.dtype],
         "data": "synthetic",
         "config": {"workload": w.name, "frames_per_step": n_frames, "detector": list(w.shape),
-                   "n_points": nb, "method": w.method, "errors": w.errors,
+                   "n_points": w.n_points, "n_azimuthal": w.n_azimuthal, "method": w.method,
+                   "errors": w.errors,
                    "azimuthal_std": w.azimuthal_std, "table_entries": E,
                    "l2": "inputs larger than L2: each step reads %.2f GB of frames"
                          % (n_frames * w.dim1 * w.dim2 * px / 1e9),
@@ -295,6 +359,9 @@ def main():
         "gpu_launches": int(launches.value),
         "build_ms": round(info.build_ms, 2),
     }
+    if w.kind == "precision" and rank == 0:
+        torch.cuda.synchronize()
+        line["precision"] = precision_report(w, frames, oi, os_, od)
     if not args.no_extras and rank == 0:
         # plain one-frame-per-launch GPU path on the same resident frames
         nplain = min(n_frames, 64)

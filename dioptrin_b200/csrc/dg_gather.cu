@@ -728,6 +728,7 @@ __global__ void __launch_bounds__(kThreads, DB ? 1 : 2)
             const int b = s_bseg[bi];
             double v = 0.0;
             for (int w = s_bwlo[bi]; w <= s_bwhi[bi]; ++w) {
+                if (s_sb[w] < 0) continue;  // an empty piece (units of < kWarps pairs)
                 const int slot = 2 * w + (b == s_sa[w] ? 0 : 1);
                 v = __dadd_rn(v, s_red[(slot * NA + a) * 32 + f]);
             }

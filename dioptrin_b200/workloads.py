@@ -38,6 +38,9 @@ class Workload:
     errors: bool = True
     azimuthal_std: bool = False
     n_frames: int = 1
+    n_azimuthal: int = 0  # > 0: a 2D cake of n_azimuthal x n_points bins
+    azimuthal_range: Optional[tuple] = None
+    kind: str = "counts"  # expected_image kind of the frames
     gaps: tuple = ()  # (module rows, module cols, module h, module w, gap h, gap w)
     dead_fraction: float = 0.0
     seed: int = 20261203
@@ -99,7 +102,7 @@ EIGER_4M_F32 = Workload(
     name="eiger4m_ps3000_f32", dim1=2167, dim2=2070, pixel=75e-6, distance=0.15,
     poni1=(2167 / 2 + 40) * 75e-6, poni2=(2070 / 2 - 25) * 75e-6, rot1=0.02, rot2=-0.01,
     wavelength=0.3e-10, n_points=3000, dtype="float32", errors=True, azimuthal_std=True,
-    n_frames=128, gaps=(4, 2, 514, 1030, 37, 10), dead_fraction=0.02)
+    n_frames=128, kind="precision", gaps=(4, 2, 514, 1030, 37, 10), dead_fraction=0.02)
 
 EIGER_9M = Workload(
     name="eiger9m_ss4", dim1=3269, dim2=3110, pixel=75e-6, distance=0.25,
@@ -107,7 +110,23 @@ EIGER_9M = Workload(
     method="supersampled", n_ss=4, n_points=1000, dtype="uint16", errors=False,
     n_frames=64, gaps=(6, 3, 514, 1030, 37, 10))
 
-WORKLOADS = {w.name: w for w in (PILATUS_1M, EIGER_4M, EIGER_4M_F32, EIGER_9M)}
+# Eiger-9M-shaped 2D cakes: 1000 radial x 360 azimuthal bins over (-pi, pi),
+# beam near one edge so the chi seam crosses the detector.
+EIGER_9M_2D_SS4 = Workload(
+    name="eiger9m_2d_ss4", dim1=3269, dim2=3110, pixel=75e-6, distance=0.25,
+    poni1=0.5 * 3269 * 75e-6, poni2=40 * 75e-6, rot1=0.05, wavelength=0.3e-10,
+    method="supersampled", n_ss=4, n_points=1000, n_azimuthal=360,
+    azimuthal_range=(-math.pi, math.pi), dtype="uint16", errors=True, n_frames=64,
+    gaps=(6, 3, 514, 1030, 37, 10))
+
+EIGER_9M_2D_PF = Workload(
+    name="eiger9m_2d_pyfai", dim1=3269, dim2=3110, pixel=75e-6, distance=0.25,
+    poni1=0.5 * 3269 * 75e-6, poni2=40 * 75e-6, rot1=0.05, wavelength=0.3e-10,
+    method="pyfai_full", n_points=1000, n_azimuthal=360, azimuthal_range=(-math.pi, math.pi),
+    dtype="uint16", errors=True, n_frames=64, gaps=(6, 3, 514, 1030, 37, 10))
+
+WORKLOADS = {w.name: w for w in (PILATUS_1M, EIGER_4M, EIGER_4M_F32, EIGER_9M, EIGER_9M_2D_SS4,
+                                 EIGER_9M_2D_PF)}
 
 
 def expected_image(w: Workload, kind: str = "counts") -> np.ndarray:

@@ -39,6 +39,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "eiger4m_1d_frames_per_s"
 
+# DRAM bytes (read + write) of one gather launch from an ncu capture, keyed by
+# (workload, gather mapping, frames per launch): a 32-frame launch captured in
+# full, its frame and partial-sum bytes scaled to 256 frames
+# (profiles/k_gather_fl_eiger4m_32frames_full.md).
+MEASURED_TRAFFIC = {("eiger4m_ps2000_b256", 6, 256): 5_533_000_000}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -351,7 +357,8 @@ def main():
                    "gather_variant": variant,
                    "autotune_ms": [round(x, 4) for x in variant_ms]},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": MEASURED_TRAFFIC.get((w.name, variant, n_frames)),
                      "peak_kind": peak_kind, "kernel": "k_gather",
                      "alg_bytes_per_launch": alg,
                      "kernel_ms_per_launch": round(per_launch_s * 1000, 4)},
@@ -363,7 +370,11 @@ def main():
         torch.cuda.synchronize()
         line["precision"] = precision_report(w, frames, oi, os_, od)
     if not args.no_extras and rank == 0:
-        # plain one-frame-per-launch GPU path on the same resident frames
+        # plain one-frame-per-launch GPU path on the same resident frames,
+        # with the lane mapping tuned for one-frame launches
+        with torch.cuda.stream(stream):
+            batch_variant = plan.gather_variant
+            plan.autotune(frames[:1], errors=w.errors, azimuthal_std=w.azimuthal_std)
         nplain = min(n_frames, 64)
         step(L.dg_integrate_device_plain, nplain)
         torch.cuda.synchronize()
@@ -375,7 +386,9 @@ def main():
         p1.record(stream)
         torch.cuda.synchronize()
         line["plain"] = {"value": round(nplain * reps / (p0.elapsed_time(p1) / 1000), 2),
-                         "unit": "frames/s", "frames": nplain * reps}
+                         "unit": "frames/s", "frames": nplain * reps,
+                         "gather_variant": plan.gather_variant}
+        plan.gather_variant = batch_variant
         # end to end through the public host API: pinned host frames in,
         # results back, every step
         host = torch.empty(frames.shape, dtype=frames.dtype, pin_memory=True)

@@ -325,10 +325,8 @@ def main():
     N.check(L.dg_plan_kernel_time(plan.handle, 1, C.byref(gms), C.byref(gl),
                                   C.byref(launches)))
     N.check(L.dg_plan_profile(plan.handle, 0))
-    t = torch.tensor([ms], dtype=torch.float64, device=frames.device)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    from dioptrin_b200.sharding import max_over_ranks
+    ms_max = max_over_ranks(ms, device=frames.device)
     value = world * n_frames * args.steps / (ms_max / 1000.0)
 
     # Roofline of the gather kernel: algorithmic bytes per launch (table once,

@@ -90,7 +90,7 @@ class Workload:
 PILATUS_1M = Workload(
     name="pilatus1m_ps1250", dim1=1043, dim2=981, pixel=172e-6, distance=0.200,
     poni1=0.0897, poni2=0.0844, wavelength=0.4e-10, n_points=1250, polarization_factor=0.99,
-    dtype="int32", errors=True, gaps=(5, 2, 195, 487, 17, 7))
+    dtype="int32", errors=True, n_frames=256, gaps=(5, 2, 195, 487, 17, 7))
 
 EIGER_4M = Workload(
     name="eiger4m_ps2000_b256", dim1=2167, dim2=2070, pixel=75e-6, distance=0.15,

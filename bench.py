@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, plain and CPU legs")
     ap.add_argument("--variant", type=int, default=None,
                     help="force a gather lane mapping instead of the autotuned one")
+    ap.add_argument("--serve", action="store_true",
+                    help="mixed-stream serving run (6 plans, Poisson arrivals) instead")
+    ap.add_argument("--rate", type=float, default=1000.0, help="serving arrivals per second")
+    ap.add_argument("--seconds", type=float, default=4.0, help="serving stream length")
     return ap.parse_args()
 
 
@@ -235,8 +239,103 @@ def precision_report(w, frames, oi, os_, od, n: int = 4):
     return out
 
 
+def run_serving(args):
+    """Mixed stream: seeded Poisson arrivals over six plans (Pilatus-1M,
+    Eiger-4M and Eiger-9M shapes, each as a 1D PixelSplit pattern and a 2D
+    supersampled n_ss=2 cake) through the request loop; halfway through, two
+    plans get a new PONI (distance +1 mm, rot1 +0.001), which forces a
+    rebuild. Reports completed frames/s and submit-to-result latency."""
+    import math
+    import threading
+    import numpy as np
+    import dioptrin_b200 as dg
+    from dioptrin_b200 import workloads as W
+    shapes = [W.PILATUS_1M, W.EIGER_4M, W.EIGER_9M]
+    specs = []  # (key, workload, method, n_radial, n_azimuthal, errors, std)
+    for i, w in enumerate(shapes):
+        specs.append((2 * i + 1, w, "pixel_split", (1250, 2000, 3000)[i], 0, True, i == 1))
+        specs.append((2 * i + 2, w, "supersampled", (500, 1000, 1000)[i], (180, 360, 360)[i],
+                      True, False))
+
+    def integrator(w, method, moved=False):
+        pd = w.poni_dict()
+        if moved:
+            pd = dict(pd, distance=pd["distance"] + 1e-3, rot1=pd["rot1"] + 1e-3)
+        it = dg.Integrator.from_poni_dict(pd, method=method, n_ss=2,
+                                          polarization_factor=w.polarization_factor)
+        it.set_mask(w.mask())
+        return it
+
+    loop = dg.RequestLoop(cache_bytes=60 << 30, max_inflight_frames=256, max_coalesce=32)
+    pools = {}
+    for key, w, method, nr, na, err, std in specs:
+        loop.register(key, integrator(w, method), w.shape, nr, n_azimuthal=na,
+                      azimuthal_range=(-math.pi, math.pi) if na else None)
+        pools[key] = W.frames_numpy(w, 3)
+        for f in pools[key][:1]:  # build and warm every plan before the stream
+            loop.poll(loop.submit(key, f, errors=err, azimuthal_std=std), key, errors=err,
+                      azimuthal_std=std)
+    rng = np.random.default_rng(20261203 + 5)
+    n = int(args.rate * args.seconds)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
+    picks = rng.integers(0, len(specs), n)
+    tickets = [None] * n
+    t0 = time.perf_counter()
+    half = args.seconds / 2
+    moved = {"done": False}
+
+    def producer(lane, lanes):
+        for k in range(lane, n, lanes):
+            wait = arrivals[k] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            if lane == 0 and not moved["done"] and arrivals[k] >= half:
+                moved["done"] = True
+                for key, w, method, nr, na, err, std in (specs[2], specs[5]):
+                    loop.register(key, integrator(w, method, moved=True), w.shape, nr,
+                                  n_azimuthal=na,
+                                  azimuthal_range=(-math.pi, math.pi) if na else None)
+            key, w, method, nr, na, err, std = specs[int(picks[k])]
+            frame = pools[key][k % len(pools[key])]
+            tickets[k] = (key, loop.submit(key, frame, errors=err, azimuthal_std=std,
+                                           wait_ms=60000), err, std, time.perf_counter() - t0)
+
+    lanes = 4
+    threads = [threading.Thread(target=producer, args=(i, lanes)) for i in range(lanes)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    lat = []
+    for key, t, err, std, _ in tickets:
+        lat.append(loop.poll(t, key, errors=err, azimuthal_std=std, wait_ms=60000)[3])
+    elapsed = time.perf_counter() - t0
+    st = loop.stats()
+    loop.close()
+    lat = np.array(lat) / 1000.0
+    submitted = max(tk[4] for tk in tickets)
+    line = {
+        "metric": "mixed_stream_frames_per_s", "value": round(n / elapsed, 2),
+        "unit": "frames/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+        "p50_ms": round(float(np.percentile(lat, 50)), 3),
+        "p99_ms": round(float(np.percentile(lat, 99)), 3),
+        "max_ms": round(float(lat.max()), 3),
+        "offered_rate": args.rate, "achieved_submit_rate": round(n / submitted, 1),
+        "requests": n, "seconds": round(elapsed, 3),
+        "server": {k: int(v) for k, v in st.items()},
+        "config": {"workload": "mixed stream: 6 plans (Pilatus-1M, Eiger-4M, Eiger-9M shapes "
+                               "x 1D pixel_split 1250-3000 bins / 2D supersampled n_ss=2 "
+                               "500x180-1000x360), host frames, 2 mid-stream PONI changes",
+                   "cache_bytes": 60 << 30, "max_coalesce": 32},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.serve:
+        run_serving(args)
+        return
     from dioptrin_b200 import workloads as W
     w = W.WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))

@@ -6,10 +6,14 @@
 // max_coalesce) into one launch, and publish results per request. Plans live
 // in an HBM cache bounded by bytes: a miss builds the plan on the device, and
 // least-recently-used plans that no worker is using are evicted until the
-// cache fits. Two workers run different plans concurrently on their own
-// streams, so a batch's copies and gather overlap another's. Each request's
-// result is identical alone and in any mix: the gather's arithmetic depends
-// only on the plan, never on which frames share a launch.
+// cache fits. Four workers run batches concurrently on their own streams,
+// so one batch's copies overlap another's gather. A submit copies its frame
+// into a pooled pinned buffer outside the server lock; the worker copies the
+// pinned buffers straight to the device. Re-registering a key (a changed
+// PONI) gives it a new generation: the next request rebuilds the plan, and
+// the stale plan is destroyed once no worker uses it. Each request's result
+// is identical alone and in any mix: the gather's arithmetic depends only on
+// the plan, never on which frames share a launch.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -32,14 +36,48 @@ struct PlanSpec {
     int32_t dim1 = 0, dim2 = 0, n_radial = 0, n_azimuthal = 0;
     bool has_az_range = false;
     double az_range[2] = {0, 0};
+    uint64_t generation = 0;
     int64_t n_bins() const { return n_azimuthal ? int64_t(n_radial) * n_azimuthal : n_radial; }
+};
+
+// Pinned host buffers by byte size, reused across requests.
+struct PinnedPool {
+    std::mutex mu;
+    std::unordered_map<size_t, std::vector<void *>> free;
+    void *get(size_t bytes) {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            auto &v = free[bytes];
+            if (!v.empty()) {
+                void *p = v.back();
+                v.pop_back();
+                return p;
+            }
+        }
+        void *p = nullptr;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    }
+    void put(size_t bytes, void *p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> lock(mu);
+        free[bytes].push_back(p);
+    }
+    ~PinnedPool() {
+        for (auto &kv : free)
+            for (void *p : kv.second) cudaFreeHost(p);
+    }
 };
 
 struct Request {
     uint64_t ticket = 0, key = 0;
     int32_t dtype = 0;
     uint32_t flags = 0;
-    std::vector<unsigned char> frame;
+    void *frame = nullptr;  // pinned, frame_bytes long
+    size_t frame_bytes = 0;
     Clock::time_point submitted;
     double latency_us = 0;
     std::vector<double> out_i, out_s, out_d;
@@ -53,6 +91,7 @@ struct CacheEntry {
     int64_t bytes = 0;
     int users = 0;
     uint64_t last_use = 0;
+    uint64_t generation = 0;
 };
 
 size_t px_size(int32_t dtype) {
@@ -81,6 +120,9 @@ struct dg_server {
     dg_server_stats stats{};
     bool stop = false;
     std::vector<std::thread> workers;
+    PinnedPool pinned;
+    std::vector<CacheEntry> retired;  // stale plans still in use
+    uint64_t next_generation = 1;
 
     // Returns a plan for `key` with a user reference, building it on a miss and
     // evicting idle LRU plans to stay within the byte budget. Called unlocked.
@@ -88,14 +130,15 @@ struct dg_server {
         PlanSpec spec;
         {
             std::unique_lock<std::mutex> lock(mu);
+            spec = specs.at(key);
             auto it = cache.find(key);
-            if (it != cache.end()) {
+            if (it != cache.end() && it->second.generation == spec.generation) {
                 it->second.users++;
                 it->second.last_use = ++use_clock;
                 stats.plan_hits++;
                 return it->second.plan;
             }
-            spec = specs.at(key);
+            if (it != cache.end()) retire_locked(it);
         }
         dg_plan *plan = nullptr;
         st = dg_plan_create(&spec.geometry, &spec.method, spec.mask.empty() ? nullptr : spec.mask.data(),
@@ -112,6 +155,10 @@ struct dg_server {
         {
             std::unique_lock<std::mutex> lock(mu);
             auto it = cache.find(key);
+            if (it != cache.end() && it->second.generation != spec.generation) {
+                retire_locked(it);
+                it = cache.end();
+            }
             if (it != cache.end()) {  // another worker built it meanwhile
                 evicted.push_back(plan);
                 it->second.users++;
@@ -138,6 +185,7 @@ struct dg_server {
                 e.bytes = info.device_bytes;
                 e.users = 1;
                 e.last_use = ++use_clock;
+                e.generation = spec.generation;
                 cache[key] = e;
                 cache_bytes += e.bytes;
                 result = plan;
@@ -147,17 +195,46 @@ struct dg_server {
         return result;
     }
 
-    void release(uint64_t key) {
-        std::unique_lock<std::mutex> lock(mu);
-        auto it = cache.find(key);
-        if (it != cache.end() && it->second.users > 0) it->second.users--;
+    // Moves a stale cache entry out of the cache (lock held): destroyed now
+    // if idle, else when its last user releases it.
+    void retire_locked(std::unordered_map<uint64_t, CacheEntry>::iterator it) {
+        cache_bytes -= it->second.bytes;
+        if (it->second.users == 0) {
+            dg_plan *p = it->second.plan;
+            cache.erase(it);
+            dg_plan_destroy(p);  // not in use by any worker
+            return;
+        }
+        retired.push_back(it->second);
+        cache.erase(it);
+    }
+
+    void release(uint64_t key, dg_plan *plan) {
+        dg_plan *dead = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            auto it = cache.find(key);
+            if (it != cache.end() && it->second.plan == plan) {
+                if (it->second.users > 0) it->second.users--;
+            } else {
+                for (size_t i = 0; i < retired.size(); ++i)
+                    if (retired[i].plan == plan) {
+                        if (--retired[i].users == 0) {
+                            dead = plan;
+                            retired.erase(retired.begin() + long(i));
+                        }
+                        break;
+                    }
+            }
+        }
+        if (dead) dg_plan_destroy(dead);
     }
 
     void worker_main() {
         cudaSetDevice(cfg.device);
         cudaStream_t stream = nullptr;
         cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-        unsigned char *d_in = nullptr, *h_in = nullptr;
+        unsigned char *d_in = nullptr;
         double *d_out = nullptr, *h_out = nullptr;
         size_t in_cap = 0, out_cap = 0;
         for (;;) {
@@ -187,20 +264,17 @@ struct dg_server {
             dg_status st = DG_OK;
             dg_plan *plan = acquire(head->key, err, st);
             if (plan) {
-                const size_t fb = head->frame.size();
+                const size_t fb = head->frame_bytes;
                 const int64_t nb = plan->n_bins;
                 const int nout = 1 + ((head->flags & DG_ERRORS) ? 1 : 0) +
                                  ((head->flags & DG_AZIMUTHAL_STD) ? 1 : 0);
                 const size_t nf = batch.size();
                 if (in_cap < nf * fb) {
                     if (d_in) cudaFree(d_in);
-                    if (h_in) cudaFreeHost(h_in);
                     in_cap = nf * fb;
-                    if (cudaMalloc(&d_in, in_cap) != cudaSuccess ||
-                        cudaMallocHost(&h_in, in_cap) != cudaSuccess) {
+                    if (cudaMalloc(&d_in, in_cap) != cudaSuccess) {
                         (void)cudaGetLastError();
                         d_in = nullptr;
-                        h_in = nullptr;
                         in_cap = 0;
                     }
                 }
@@ -221,8 +295,8 @@ struct dg_server {
                     err = "request loop staging allocation failed";
                 } else {
                     for (size_t i = 0; i < nf; ++i)
-                        std::memcpy(h_in + i * fb, batch[i]->frame.data(), fb);
-                    cudaMemcpyAsync(d_in, h_in, nf * fb, cudaMemcpyHostToDevice, stream);
+                        cudaMemcpyAsync(d_in + i * fb, batch[i]->frame, fb, cudaMemcpyHostToDevice,
+                                        stream);
                     double *di = d_out, *ds = nullptr, *dd = nullptr;
                     int k = 1;
                     if (head->flags & DG_ERRORS) ds = d_out + nf * nb * k++;
@@ -253,7 +327,7 @@ struct dg_server {
                         }
                     }
                 }
-                release(head->key);
+                release(head->key, plan);
             }
             {
                 std::unique_lock<std::mutex> lock(mu);
@@ -268,8 +342,8 @@ struct dg_server {
                         std::chrono::duration<double, std::micro>(now - r->submitted).count();
                     if (st == DG_OK) stats.completed++;
                     else stats.failed++;
-                    r->frame.clear();
-                    r->frame.shrink_to_fit();
+                    pinned.put(r->frame_bytes, r->frame);
+                    r->frame = nullptr;
                     inflight--;
                 }
             }
@@ -277,7 +351,6 @@ struct dg_server {
             cv_slot.notify_all();
         }
         if (d_in) cudaFree(d_in);
-        if (h_in) cudaFreeHost(h_in);
         if (d_out) cudaFree(d_out);
         if (h_out) cudaFreeHost(h_out);
         if (stream) cudaStreamDestroy(stream);
@@ -306,7 +379,7 @@ dg_status dg_server_create(const dg_server_config *config, dg_server **out) {
         return server_fail(DG_INVALID_INPUT, "server limits must be positive");
     auto s = std::make_unique<dg_server>();
     s->cfg = *config;
-    for (int i = 0; i < 2; ++i) s->workers.emplace_back([p = s.get()] { p->worker_main(); });
+    for (int i = 0; i < 4; ++i) s->workers.emplace_back([p = s.get()] { p->worker_main(); });
     *out = s.release();
     return DG_OK;
 }
@@ -320,6 +393,9 @@ dg_status dg_server_destroy(dg_server *server) {
     server->cv_work.notify_all();
     for (auto &t : server->workers) t.join();
     for (auto &kv : server->cache) dg_plan_destroy(kv.second.plan);
+    for (auto &e : server->retired) dg_plan_destroy(e.plan);
+    for (auto &kv : server->requests)
+        if (kv.second->frame) server->pinned.put(kv.second->frame_bytes, kv.second->frame);
     delete server;
     return DG_OK;
 }
@@ -344,19 +420,15 @@ dg_status dg_server_register(dg_server *server, uint64_t key, const dg_geometry 
         spec.az_range[0] = azimuthal_range[0];
         spec.az_range[1] = azimuthal_range[1];
     }
-    std::vector<dg_plan *> stale;
     {
         std::unique_lock<std::mutex> lock(server->mu);
+        // A re-registered key (a changed PONI) gets a new generation; its
+        // cached plan is retired (now, or when its users finish).
+        spec.generation = server->next_generation++;
         server->specs[key] = std::move(spec);
-        // A re-registered key (a changed PONI) drops its cached plan.
         auto it = server->cache.find(key);
-        if (it != server->cache.end() && it->second.users == 0) {
-            server->cache_bytes -= it->second.bytes;
-            stale.push_back(it->second.plan);
-            server->cache.erase(it);
-        }
+        if (it != server->cache.end()) server->retire_locked(it);
     }
-    for (dg_plan *p : stale) dg_plan_destroy(p);
     return DG_OK;
 }
 
@@ -368,23 +440,33 @@ dg_status dg_server_submit(dg_server *server, uint64_t key, const void *frame, i
     std::unique_lock<std::mutex> lock(server->mu);
     auto spec = server->specs.find(key);
     if (spec == server->specs.end()) return server_fail(DG_INVALID_INPUT, "unregistered plan key");
+    const size_t bytes = size_t(spec->second.dim1) * spec->second.dim2 * px_size(dtype);
     if (!server->cv_slot.wait_for(lock, std::chrono::milliseconds(std::max(wait_ms, 0)), [&] {
             return server->inflight < server->cfg.max_inflight_frames;
         }))
         return server_fail(DG_TIMEOUT, "no request slot freed in time");
+    server->inflight++;  // the slot is taken; the copy happens unlocked
+    lock.unlock();
     auto r = std::make_unique<Request>();
-    r->ticket = server->next_ticket++;
     r->key = key;
     r->dtype = dtype;
     r->flags = flags;
-    size_t bytes = size_t(spec->second.dim1) * spec->second.dim2 * px_size(dtype);
-    r->frame.assign(static_cast<const unsigned char *>(frame),
-                    static_cast<const unsigned char *>(frame) + bytes);
     r->submitted = Clock::now();
+    r->frame_bytes = bytes;
+    r->frame = server->pinned.get(bytes);
+    if (!r->frame) {
+        lock.lock();
+        server->inflight--;
+        lock.unlock();
+        server->cv_slot.notify_one();
+        return server_fail(DG_DEVICE, "pinned staging allocation failed");
+    }
+    std::memcpy(r->frame, frame, bytes);
+    lock.lock();
+    r->ticket = server->next_ticket++;
     *ticket = r->ticket;
     server->queue.push_back(r.get());
     server->requests[r->ticket] = std::move(r);
-    server->inflight++;
     server->stats.submitted++;
     lock.unlock();
     server->cv_work.notify_one();

@@ -16,21 +16,28 @@ class RequestLoop:
     def __init__(self, device: int = 0, cache_bytes: int = 60 << 30,
                  max_inflight_frames: int = 512, max_coalesce: int = 64, poll_us: int = 100):
         cfg = N.ServerConfig(device, max_inflight_frames, cache_bytes, max_coalesce, poll_us)
+        self._device = device
         self._h = C.c_void_p()
         N.check(N.lib().dg_server_create(C.byref(cfg), C.byref(self._h)))
         self._bins: dict = {}
         self._shapes: dict = {}
 
     def register(self, key: int, integrator: Integrator, shape, n_points: int,
-                 precision: str = "f32_compensated") -> None:
-        """Registers (or re-registers, after a PONI change) a plan under key."""
+                 precision: str = "f32_compensated", n_azimuthal: int = 0,
+                 azimuthal_range=None) -> None:
+        """Registers (or re-registers, after a PONI change) a plan under key:
+        1D with n_points bins, or a 2D cake of n_azimuthal x n_points."""
         dim1, dim2 = shape
-        m = integrator._method_struct(precision, 0, 0, False)
+        m = integrator._method_struct(precision, self._device, 0, False)
         mask = (None if integrator._mask is None
                 else integrator._mask.ctypes.data_as(C.POINTER(C.c_uint8)))
+        rng = None
+        if azimuthal_range is not None:
+            rng = (C.c_double * 2)(float(azimuthal_range[0]), float(azimuthal_range[1]))
         N.check(N.lib().dg_server_register(self._h, key, C.byref(integrator.poni._c()),
-                                           C.byref(m), mask, dim1, dim2, n_points, 0, None))
-        self._bins[key] = n_points
+                                           C.byref(m), mask, dim1, dim2, n_points, n_azimuthal,
+                                           rng))
+        self._bins[key] = n_points * max(1, n_azimuthal)
         self._shapes[key] = (dim1, dim2)
 
     def submit(self, key: int, frame: np.ndarray, errors: bool = False,

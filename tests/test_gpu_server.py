@@ -1,0 +1,101 @@
+"""The request loop (continuous batching across plans) on the device.
+
+Requests for several plans (1D and 2D, different shapes and bin counts)
+arrive from two threads at once; the loop coalesces same-plan requests into
+one launch and runs plans concurrently. Every result must equal the same
+frame integrated alone through the loop, bit for bit (a frame's sums do not
+depend on the frames launched with it), and match the oracle-checked
+Integrator path of the same configuration."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dg():
+    import dioptrin_b200 as d
+    if not d.cuda_available():
+        pytest.fail("CUDA device required for -m gpu tests: " + str(d.cuda_info()))
+    return d
+
+
+def _configs(dg):
+    poni = dict(pixel1=1e-4, pixel2=1e-4, distance=0.05, poni1=0.003, poni2=0.004,
+                rot1=0.01, wavelength=1e-10)
+    a = dg.Integrator.from_poni_dict(poni, method="pixel_split", polarization_factor=0.99)
+    b = dg.Integrator.from_poni_dict(poni, method="supersampled", n_ss=2)
+    c = dg.Integrator.from_poni_dict(dict(poni, distance=0.07), method="counting")
+    return [(1, a, (60, 80), 90, 0, np.uint32, True, True),
+            (2, b, (60, 80), 24, 18, np.uint16, True, False),
+            (3, c, (48, 64), 50, 0, np.float32, False, False)]
+
+
+def test_mixed_stream_results_equal_the_frames_alone(dg):
+    loop = dg.RequestLoop(max_inflight_frames=64, max_coalesce=16)
+    cfgs = _configs(dg)
+    for key, it, shape, nb, na, _, _, _ in cfgs:
+        loop.register(key, it, shape, nb, n_azimuthal=na)
+    rng = np.random.default_rng(12)
+    work = []
+    for i in range(60):
+        key, it, shape, nb, na, dt, err, std = cfgs[i % 3]
+        work.append((key, rng.poisson(100.0, shape).astype(dt), err, std))
+    results = {}
+
+    def producer(items):
+        for idx, (key, frame, err, std) in items:
+            t = loop.submit(key, frame, errors=err, azimuthal_std=std)
+            results[idx] = (key, t, err, std)
+
+    threads = [threading.Thread(target=producer, args=(list(enumerate(work))[k::2],))
+               for k in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    mixed = {}
+    for idx, (key, t, err, std) in results.items():
+        mixed[idx] = loop.poll(t, key, errors=err, azimuthal_std=std)
+    stats = loop.stats()
+    assert stats["completed"] == 60 and stats["failed"] == 0
+    # alone: one request in flight at a time
+    for idx, (key, frame, err, std) in enumerate(work):
+        t = loop.submit(key, frame, errors=err, azimuthal_std=std)
+        alone = loop.poll(t, key, errors=err, azimuthal_std=std)
+        for a, b in zip(mixed[idx][:3], alone[:3]):
+            if a is None:
+                assert b is None
+            else:
+                assert np.array_equal(a, b, equal_nan=True), (idx, key)
+    # the Integrator path of the same configurations
+    for idx in (0, 1, 2):
+        key, it, shape, nb, na, dt, err, std = cfgs[idx]
+        frame = work[idx][1]
+        if na:
+            r = it.integrate2d(frame, nb, na, err)
+            np.testing.assert_allclose(mixed[idx][0], r.intensity_array, rtol=1e-12)
+        else:
+            r = it.integrate1d(frame, nb, err, azimuthal_std=std)
+            np.testing.assert_allclose(mixed[idx][0], r.intensity_array, rtol=1e-12)
+    loop.close()
+
+
+def test_reregistered_plan_is_rebuilt(dg):
+    loop = dg.RequestLoop()
+    poni = dict(pixel1=1e-4, pixel2=1e-4, distance=0.05, poni1=0.003, poni2=0.004,
+                wavelength=1e-10)
+    it = dg.Integrator.from_poni_dict(poni, method="pixel_split")
+    loop.register(7, it, (40, 50), 30)
+    frame = np.full((40, 50), 10.0, np.float32)
+    a = loop.poll(loop.submit(7, frame), 7)[0]
+    moved = dg.Integrator.from_poni_dict(dict(poni, distance=0.051), method="pixel_split")
+    loop.register(7, moved, (40, 50), 30)
+    b = loop.poll(loop.submit(7, frame), 7)[0]
+    assert loop.stats()["plan_builds"] == 2
+    ref = moved.integrate1d(frame, 30).intensity_array
+    np.testing.assert_allclose(b, ref, rtol=1e-12)
+    assert not np.array_equal(a, b)
+    loop.close()

@@ -399,9 +399,12 @@ __global__ void __launch_bounds__(kThreads)
 // cut by piece boundaries are added in warp order. Results depend on the
 // table alone, not on the frames around them in a batch.
 
+#ifndef DG_FL_DCAP
+#define DG_FL_DCAP 384
+#endif
 constexpr int kFlSegs = 32;               // segments per frame-lane unit, at most
-constexpr int kFlECap = 1152;             // entries per frame-lane unit before padding
-constexpr int kFlDCap = 576;              // distinct pixels per frame-lane unit
+constexpr int kFlDCap = DG_FL_DCAP;       // distinct pixels per frame-lane unit (even)
+constexpr int kFlECap = 2 * kFlDCap;      // entries per frame-lane unit before padding
 constexpr int kFlPairCap = (kFlECap + kFlSegs) / 2;
 constexpr int kFlStride = kFlDCap + 1;    // odd; column kFlDCap stays 0
 constexpr int kFlSlots = 2 * kWarps;      // first and last segment of each piece
@@ -481,8 +484,15 @@ constexpr size_t fl_smem_bytes() {
            size_t(DB ? 64 : 32) * kFlStride * 4 + size_t(kFlSlots) * NAcc<MODE, P>::value * 32 * 8;
 }
 
+// CTAs per SM the frame-lane gather's shared memory allows (227 KB per CTA,
+// 228 KB per SM with 1 KB reserved per CTA), for its launch bounds.
+template <int MODE, typename P, bool DB>
+constexpr int fl_ctas_per_sm() {
+    return fl_smem_bytes<MODE, P, DB>() + 6 * 1024 <= 113 * 1024 ? 2 : 1;
+}
+
 template <int MODE, typename P, int U2, bool DB>
-__global__ void __launch_bounds__(kThreads, DB ? 1 : 2)
+__global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
     k_gather_fl(const int4 *__restrict__ units, const int4 *__restrict__ segs,
                 const int32_t *__restrict__ unit_px, const float4 *__restrict__ pair_a,
                 const float4 *__restrict__ pair_b, const float4 *__restrict__ entry_std,

@@ -1619,3 +1619,110 @@ int or_integrate_frames_mt(const or_lut *table, const double *den, const or_lut 
     free(jobs);
     return status;
 }
+
+/* ================================================== Bitshuffle + LZ4 chunks */
+
+static uint64_t be64(const uint8_t *p) {
+    uint64_t v = 0;
+    for (int i = 0; i < 8; ++i) v = (v << 8) | p[i];
+    return v;
+}
+static uint32_t be32(const uint8_t *p) {
+    return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3];
+}
+
+/* One LZ4 block (the published LZ4 block format: sequences of a token,
+ * literal length with 255-extensions, literals, a 2-byte little-endian
+ * offset, a match length of (token & 15) + 4 with 255-extensions; the last
+ * sequence has literals only). Returns the decoded length or -1. */
+static int64_t lz4_block_decode(const uint8_t *in, int64_t n, uint8_t *out, int64_t cap) {
+    int64_t ip = 0, op = 0;
+    while (ip < n) {
+        unsigned token = in[ip++];
+        int64_t lit = token >> 4;
+        if (lit == 15) {
+            unsigned s;
+            do {
+                if (ip >= n) return -1;
+                s = in[ip++];
+                lit += s;
+            } while (s == 255);
+        }
+        if (lit > n - ip || lit > cap - op) return -1;
+        memcpy(out + op, in + ip, (size_t)lit);
+        ip += lit;
+        op += lit;
+        if (ip >= n) break; /* last sequence: literals only */
+        if (ip + 2 > n) return -1;
+        int64_t offset = (int64_t)in[ip] | ((int64_t)in[ip + 1] << 8);
+        ip += 2;
+        if (offset == 0 || offset > op) return -1;
+        int64_t mlen = (token & 15) + 4;
+        if ((token & 15) == 15) {
+            unsigned s;
+            do {
+                if (ip >= n) return -1;
+                s = in[ip++];
+                mlen += s;
+            } while (s == 255);
+        }
+        if (mlen > cap - op) return -1;
+        for (int64_t k = 0; k < mlen; ++k) out[op + k] = out[op + k - offset];
+        op += mlen;
+    }
+    return op;
+}
+
+/* Inverse bitshuffle of count elements (count a multiple of 8): plane p
+ * (bit p of an element, least significant first) holds count/8 bytes whose
+ * bit i of byte k is bit p of element 8k + i. Elements are little-endian. */
+static void bitunshuffle(const uint8_t *in, int64_t count, int elem_bytes, uint8_t *out) {
+    int64_t plane = count / 8;
+    memset(out, 0, (size_t)(count * elem_bytes));
+    for (int p = 0; p < 8 * elem_bytes; ++p)
+        for (int64_t e = 0; e < count; ++e)
+            if ((in[p * plane + e / 8] >> (e % 8)) & 1)
+                out[e * elem_bytes + p / 8] |= (uint8_t)(1u << (p % 8));
+}
+
+/* A Bitshuffle/LZ4 chunk as HDF5's bitshuffle filter writes it
+ * (device.rs:2062-2140 reads the same layout): big-endian u64 uncompressed
+ * bytes and u32 block bytes (0: 8192); every full block and then the
+ * remainder rounded down to 8 elements as a big-endian u32 compressed length
+ * and an LZ4 block of the bitshuffled elements; the last (< 8) elements
+ * verbatim. Decodes n_elems elements into out. 0, or -1 on malformed input. */
+int or_bslz4_decode(const uint8_t *chunk, int64_t len, int elem_bytes, int64_t n_elems,
+                    uint8_t *out) {
+    if (len < 12) return -1;
+    uint64_t total = be64(chunk);
+    if (total != (uint64_t)(n_elems * elem_bytes)) return -1;
+    int64_t block = be32(chunk + 8);
+    if (block == 0) block = 8192;
+    if (block % (8 * elem_bytes)) return -1;
+    int64_t block_elems = block / elem_bytes;
+    int64_t n_full = n_elems / block_elems, rem = n_elems % block_elems;
+    int64_t rem_comp = rem / 8 * 8, tail = rem % 8;
+    uint8_t *tmp = (uint8_t *)malloc((size_t)block);
+    if (!tmp) return -1;
+    int64_t off = 12;
+    int rc = 0;
+    for (int64_t b = 0; b <= n_full && rc == 0; ++b) {
+        int64_t elems = b < n_full ? block_elems : rem_comp;
+        if (elems == 0) break;
+        if (off + 4 > len) { rc = -1; break; }
+        int64_t clen = be32(chunk + off);
+        off += 4;
+        if (clen > len - off) { rc = -1; break; }
+        int64_t got = lz4_block_decode(chunk + off, clen, tmp, elems * elem_bytes);
+        if (got != elems * elem_bytes) { rc = -1; break; }
+        bitunshuffle(tmp, elems, elem_bytes, out + b * block_elems * elem_bytes);
+        off += clen;
+    }
+    if (rc == 0 && tail) {
+        int64_t raw = tail * elem_bytes;
+        if (off + raw > len) rc = -1;
+        else memcpy(out + (n_full * block_elems + rem_comp) * elem_bytes, chunk + off, (size_t)raw);
+    }
+    free(tmp);
+    return rc;
+}

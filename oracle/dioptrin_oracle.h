@@ -97,6 +97,9 @@ int or_pyfai_split2d(const double *poly, const or_grid2d *g, double sign, int64_
                      double *weights, int64_t cap);
 int or_build_2d(const or_poni *p, int64_t dim1, int64_t dim2, int method, int64_t n_ss,
                 int unit, const or_grid2d *g, or_lut *out);
+/* Bitshuffle/LZ4 chunk decoding (HDF5 bitshuffle filter layout). */
+int or_bslz4_decode(const uint8_t *chunk, int64_t len, int elem_bytes, int64_t n_elems,
+                    uint8_t *out);
 int or_build_counting1d(const double *radial, int64_t npix, int64_t n_points, int has_range,
                         double rmin, double rmax, or_lut *out);
 /* Supersampled 1D (supersampled.rs:517-593), exact per-sample path. */

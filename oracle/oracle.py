@@ -101,6 +101,7 @@ def _lib():
         lib.or_ps1d_fractions.argtypes = [P(Poni), i64, i64, i, i64, d, d, i, P(_Lut)]
         lib.or_build_counting1d.argtypes = [pd, i64, i64, i, d, d, P(_Lut)]
         lib.or_split1d.argtypes = [pd, i64, d, d, d, d, i, d, P(C.c_int64), pd, i64]
+        lib.or_bslz4_decode.argtypes = [C.c_void_p, i64, i, i64, C.c_void_p]
         lib.or_grid2d_new.argtypes = [i64, i64, d, d, d, d, P(Grid2d)]
         lib.or_grid2d_bin.argtypes = [P(Grid2d), d, d]
         lib.or_grid2d_bin.restype = i64
@@ -276,6 +277,16 @@ def build_2d(p: Poni, dim1: int, dim2: int, method: str, g: Grid2d, unit: str = 
                           C.byref(g), C.byref(lut)):
         raise MemoryError("oracle 2D build failed")
     return _take(lut)
+
+
+def bslz4_decode(chunk: bytes, dtype, n_elems: int) -> np.ndarray:
+    """Decode one Bitshuffle/LZ4 chunk into n_elems elements of dtype."""
+    dt = np.dtype(dtype)
+    out = np.zeros(n_elems, dt)
+    buf = np.frombuffer(bytes(chunk), np.uint8)
+    if _lib().or_bslz4_decode(buf.ctypes.data, len(buf), dt.itemsize, n_elems, out.ctypes.data):
+        raise ValueError("malformed Bitshuffle/LZ4 chunk")
+    return out
 
 
 def split1d(poly, n_points: int, radial_range, azimuthal_range=(-math.pi, math.pi),

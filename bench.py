@@ -331,6 +331,67 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def bslz4_leg(w, plan, frames, n_frames, flags, hi, hs, hd, peak, distinct: int = 16):
+    """Frames/s through dg_integrate_bslz4: raw HDF5 Bitshuffle/LZ4 chunks in
+    pinned HOST memory (the first `distinct` frames compressed by the
+    library's encoder, repeated to n_frames), only the compressed bytes
+    copied in, decoded and integrated on the device, results back. Also the
+    decode kernel's event-timed duration and its HBM roofline (compressed
+    bytes read + decoded bytes written per launch)."""
+    import numpy as np
+    import torch
+    import dioptrin_b200 as dg
+    from dioptrin_b200 import _native as N
+    L = N.lib()
+    src = frames[:distinct].cpu().numpy()
+    t0 = time.perf_counter()
+    chunks = [dg.bslz4_compress(f) for f in src]
+    enc_s = time.perf_counter() - t0
+    sizes = [len(c) for c in chunks]
+    pinned = torch.empty(sum(sizes), dtype=torch.uint8, pin_memory=True)
+    buf = pinned.numpy()
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    for k, c in enumerate(chunks):
+        buf[offs[k]:offs[k + 1]] = np.frombuffer(c, np.uint8)
+    base = pinned.data_ptr()
+    ptrs = (C.c_void_p * n_frames)(*[base + int(offs[k % distinct]) for k in range(n_frames)])
+    lens = (C.c_int64 * n_frames)(*[sizes[k % distinct] for k in range(n_frames)])
+    code = {"uint16": 0, "uint32": 1, "int32": 2}[w.dtype]
+    dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+    def call():
+        N.check(L.dg_integrate_bslz4(plan.handle, ptrs, lens, n_frames, code, flags, dp(hi),
+                                     dp(hs), dp(hd)))
+
+    call()
+    N.check(L.dg_plan_profile(plan.handle, 1))
+    N.check(L.dg_plan_decode_time(plan.handle, 1, None, None))
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        call()
+    dt = time.perf_counter() - t0
+    dms, dl = C.c_double(), C.c_int64()
+    N.check(L.dg_plan_decode_time(plan.handle, 1, C.byref(dms), C.byref(dl)))
+    N.check(L.dg_plan_profile(plan.handle, 0))
+    comp_step = int(sum(lens))
+    raw_step = n_frames * frames[0].numel() * frames.element_size()
+    per_launch_s = dms.value / 1000.0 / max(1, dl.value)
+    alg = (comp_step + raw_step) / max(1, dl.value / reps)
+    k_out = 1 + (1 if hs is not None else 0) + (1 if hd is not None else 0)
+    nb = hi.shape[1]
+    return {"value": round(n_frames * reps / dt, 2), "unit": "frames/s",
+            "h2d_bytes_per_step": comp_step, "d2h_bytes_per_step": int(n_frames * nb * k_out * 8),
+            "compression_ratio": round(raw_step / comp_step, 3),
+            "chunks": f"{distinct} distinct frames compressed by dg_bslz4_compress "
+                      f"({enc_s:.1f} s), 8192-byte blocks, repeated to {n_frames}",
+            "decode": {"kernel": "k_bslz4_decode", "launches_per_step": dl.value // reps,
+                       "ms_per_launch": round(per_launch_s * 1000, 4),
+                       "alg_bytes_per_launch": int(alg),
+                       "achieved": round(alg / per_launch_s / 1e9, 1), "unit": "GB/s",
+                       "frac": round(alg / per_launch_s / 1e9 / peak, 4)}}
+
+
 def main():
     args = parse()
     if args.serve:
@@ -508,6 +569,9 @@ def main():
         line["e2e"] = {"value": round(n_frames * reps / dt, 2), "unit": "frames/s",
                        "h2d_bytes_per_step": int(host.numel() * host.element_size()),
                        "d2h_bytes_per_step": int(n_frames * nb * k_out * 8)}
+        del host
+        if w.dtype in ("uint16", "uint32", "int32"):
+            line["e2e_bslz4"] = bslz4_leg(w, plan, frames, n_frames, flags, hi, hs, hd, peak)
         if world == 1:
             fr_np = frames[:16].cpu().numpy()
             rate, per_step, secs = cpu_reference(w, fr_np, os.cpu_count() or 1, 15.0, 3)

@@ -9,9 +9,10 @@ include/dioptrin_gpu.h. This package mirrors the reference's Python API:
 """
 from ._native import CudaUnavailableError, RequestTimeout
 from .integrator import (BatchIterator, BatchResult, Cuda1dPlan, Cuda2dPlan,
-                         IntegrationResult, Integrator, Poni, cuda_available, cuda_info)
+                         IntegrationResult, Integrator, Poni, bslz4_compress, cuda_available,
+                         cuda_info)
 from .server import RequestLoop
 
 __all__ = ["BatchIterator", "BatchResult", "Cuda1dPlan", "Cuda2dPlan", "CudaUnavailableError",
            "IntegrationResult", "Integrator", "Poni", "RequestLoop", "RequestTimeout",
-           "cuda_available", "cuda_info"]
+           "bslz4_compress", "cuda_available", "cuda_info"]

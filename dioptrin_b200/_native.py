@@ -18,6 +18,7 @@ METHODS = {"counting": 0, "pixel_split": 1, "pyfai_full": 2, "supersampled": 3}
 UNITS = {"2th_rad": 0, "2th_deg": 1, "q_A^-1": 2, "q_nm^-1": 3}
 PRECISIONS = {"f32": 0, "f32_compensated": 1, "f64": 2}
 DG_ERRORS, DG_AZIMUTHAL_STD = 1, 2
+DG_U16, DG_U32, DG_I32, DG_F32, DG_F64 = 0, 1, 2, 3, 4
 DG_PLAN_KEEP_TABLES = 1
 
 EXPORTS = [
@@ -25,6 +26,7 @@ EXPORTS = [
     "dg_plan_azimuthal", "dg_plan_export_table", "dg_integrate", "dg_integrate_device",
     "dg_integrate_device_plain", "dg_integrate_device_noalloc", "dg_plan_profile",
     "dg_plan_kernel_time", "dg_plan_autotune", "dg_plan_variant", "dg_eval_math",
+    "dg_integrate_bslz4", "dg_bslz4_bound", "dg_bslz4_compress", "dg_plan_decode_time",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
     "dg_device_info_get", "dg_last_error",
@@ -118,6 +120,12 @@ def lib():
                                        P(C.c_int32), pd, C.c_int32]
         L.dg_plan_variant.argtypes = [vp, C.c_int32, P(C.c_int32), P(C.c_int32)]
         L.dg_eval_math.argtypes = [C.c_int32, vp, vp, C.c_int64, vp]
+        L.dg_integrate_bslz4.argtypes = [vp, P(vp), P(C.c_int64), C.c_int64, C.c_int32,
+                                         C.c_uint32, pd, pd, pd]
+        L.dg_bslz4_bound.argtypes = [C.c_int64, C.c_int32, C.c_int32]
+        L.dg_bslz4_compress.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_int64,
+                                        P(C.c_int64)]
+        L.dg_plan_decode_time.argtypes = [vp, C.c_int32, pd, P(C.c_int64)]
         L.dg_server_create.argtypes = [P(ServerConfig), P(vp)]
         L.dg_server_destroy.argtypes = [vp]
         L.dg_server_register.argtypes = [vp, C.c_uint64, P(Geometry), P(Method), P(C.c_uint8),
@@ -132,6 +140,7 @@ def lib():
         for name in EXPORTS:
             if name != "dg_last_error":
                 getattr(L, name).restype = C.c_int
+        L.dg_bslz4_bound.restype = C.c_int64
         _LIB = L
         return L
 

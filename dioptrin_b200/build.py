@@ -32,6 +32,7 @@ SOURCES = {
     "dg_gather.cu": [],
     "dg_api.cu": [],
     "dg_server.cu": [],
+    "dg_bslz4.cu": [],
 }
 
 

@@ -181,7 +181,7 @@ int64_t dg_plan::device_bytes() const {
          gather.valid_std.bytes() + gather.partial.bytes() + gather.fl_unit.bytes() +
          gather.fl_px.bytes() + gather.fl_pair_a.bytes() + gather.fl_pair_b.bytes() +
          gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes();
-    b += stage_in.bytes() + stage_out.bytes();
+    b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes();
     return b;
 }
 
@@ -281,6 +281,7 @@ dg_status dg_plan_destroy(dg_plan *plan) {
             plan->gather = dg::GatherTable();
             plan->stage_in.release();
             plan->stage_out.release();
+            dg::bslz4_release(plan);
             if (plan->stream) cudaStreamDestroy(plan->stream);
             plan->stream = nullptr;
             if (prev >= 0) cudaSetDevice(prev);

@@ -220,6 +220,12 @@ void exclusive_scan_i64(const int64_t *in, int64_t *out, int64_t n, void *temp,
 
 }  // namespace dg
 
+struct dg_plan;
+namespace dg {
+// Frees the Bitshuffle/LZ4 staging, copy stream and events of a plan (dg_bslz4.cu).
+void bslz4_release(dg_plan *plan);
+}  // namespace dg
+
 struct dg_plan {
     std::mutex mu;
     int32_t device = 0;
@@ -241,8 +247,17 @@ struct dg_plan {
     // staging for host-memory calls
     dg::DeviceArray<unsigned char> stage_in;
     dg::DeviceArray<double> stage_out;
+    // compressed frames and their block descriptors (dg_integrate_bslz4)
+    dg::DeviceArray<unsigned char> stage_comp;
+    dg::DeviceArray<unsigned char> stage_desc;
+    cudaStream_t copy_stream = nullptr;  // compressed-frame copies
+    cudaEvent_t bs_copied[2] = {nullptr, nullptr};
+    cudaEvent_t bs_decoded[2] = {nullptr, nullptr};
+    dg::EventPool decode_events;  // decode-kernel timing (dg_plan_decode_time)
+    size_t decode_smem[2] = {0, 0};  // shared memory granted to the u16 / u32 decoders
     int64_t device_bytes() const;
     ~dg_plan() {
+        dg::bslz4_release(this);
         if (stream) cudaStreamDestroy(stream);
     }
 };

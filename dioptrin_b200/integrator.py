@@ -134,6 +134,50 @@ def _frame_array(image) -> np.ndarray:
     return a
 
 
+_BSLZ4_DTYPES = {"uint16": N.DG_U16, "u16": N.DG_U16, "uint32": N.DG_U32, "u32": N.DG_U32,
+                 "int32": N.DG_I32, "i32": N.DG_I32}
+
+
+def _bslz4_dtype(dtype) -> int:
+    key = np.dtype(dtype).name if not isinstance(dtype, str) else dtype
+    if key not in _BSLZ4_DTYPES:
+        raise TypeError(f"dtype must be 'uint16', 'uint32' or 'int32', got {dtype!r}")
+    return _BSLZ4_DTYPES[key]
+
+
+def _chunk_buffers(chunks) -> list:
+    """uint8 views of a list or tuple of byte buffers (python/cuda.rs:897-913)."""
+    if not isinstance(chunks, (list, tuple)):
+        raise TypeError(f"chunks must be a list or tuple of byte buffers, got "
+                        f"{type(chunks).__name__}")
+    out = []
+    for c in chunks:
+        try:
+            m = memoryview(c)
+        except TypeError as e:
+            raise TypeError(f"chunk must support the byte buffer protocol: {e}") from None
+        if not m.c_contiguous:
+            raise ValueError("chunk buffer must be C contiguous")
+        out.append(np.frombuffer(m.cast("B") if m.format != "B" or m.ndim != 1 else m,
+                                 np.uint8))
+    return out
+
+
+def bslz4_compress(frame: np.ndarray, block_bytes: int = 0) -> bytes:
+    """One raw HDF5 Bitshuffle/LZ4 chunk of a uint16, uint32 or int32 frame,
+    written by the library's host encoder (block_bytes 0: 8192-byte blocks)."""
+    a = np.ascontiguousarray(frame)
+    _bslz4_dtype(a.dtype)
+    cap = N.lib().dg_bslz4_bound(a.size, a.itemsize, block_bytes)
+    if cap < 0:
+        raise ValueError("invalid Bitshuffle/LZ4 arguments")
+    out = np.empty(cap, np.uint8)
+    n = C.c_int64(0)
+    N.check(N.lib().dg_bslz4_compress(a.ctypes.data, a.size, a.itemsize, block_bytes,
+                                      out.ctypes.data, cap, C.byref(n)))
+    return out[:n.value].tobytes()
+
+
 class Cuda1dPlan:
     """A fixed-mask table resident in HBM (src/integration/cuda.rs:374-618).
 
@@ -258,6 +302,36 @@ class Cuda1dPlan:
     def gather_variant(self, v: int) -> None:
         N.check(N.lib().dg_plan_variant(self._h, int(v), None, None))
 
+    def integrate_bslz4_stack(self, chunks, dtype: str = "uint32", errors: bool = False,
+                              azimuthal_std: bool = False):
+        """Decode raw HDF5 Bitshuffle/LZ4 chunks (one per frame) on the GPU
+        and integrate them (Cuda1dPlan::integrate_bslz4,
+        src/integration/cuda.rs:554-564); returns (I, sigma, std) arrays of
+        shape (n, n_bins) as integrate_stack does."""
+        code = _bslz4_dtype(dtype)
+        bufs = _chunk_buffers(chunks)
+        n = len(bufs)
+        nb = self.n_points * max(1, self.n_azimuthal)
+        flags = (N.DG_ERRORS if errors else 0) | (N.DG_AZIMUTHAL_STD if azimuthal_std else 0)
+        oi = np.empty((n, nb))
+        os_ = np.empty((n, nb)) if errors else None
+        od = np.empty((n, nb)) if azimuthal_std else None
+        if n == 0:
+            return oi, os_, od
+        ptrs = (C.c_void_p * n)(*[b.ctypes.data for b in bufs])
+        lens = (C.c_int64 * n)(*[b.nbytes for b in bufs])
+        N.check(N.lib().dg_integrate_bslz4(self._h, ptrs, lens, n, code, flags, _dp(oi),
+                                           _dp(os_), _dp(od)))
+        return oi, os_, od
+
+    def batch1d_bslz4(self, chunks, dtype: str = "uint32", *, errors: bool = False) -> list:
+        """Python Cuda1dPlan.batch1d_bslz4 (src/python/cuda.rs:880-930):
+        `chunks` is a list or tuple of byte buffers (bytes, bytearray,
+        memoryview, C-contiguous uint8 arrays), one raw chunk per frame."""
+        i, s, _ = self.integrate_bslz4_stack(chunks, dtype, errors)
+        return [IntegrationResult(self._radial, i[k], None if s is None else s[k])
+                for k in range(len(i))]
+
     def integrate1d(self, image: np.ndarray, *, errors: bool = False,
                     azimuthal_std: bool = False) -> IntegrationResult:
         a = _frame_array(image)
@@ -329,10 +403,24 @@ class Cuda2dPlan(Cuda1dPlan):
         i, s, _ = self.integrate_stack(stack, errors)
         return [self._result(i[k], None if s is None else s[k]) for k in range(len(i))]
 
+    def batch2d_bslz4(self, chunks, dtype: str = "uint32", *, errors: bool = False) -> list:
+        """Python Cuda2dPlan.batch2d_bslz4 (src/python/cuda.rs:1076-1125)."""
+        i, s, _ = self.integrate_bslz4_stack(chunks, dtype, errors)
+        return [self._result(i[k], None if s is None else s[k]) for k in range(len(i))]
+
+    def batch2d_bslz4_stack(self, chunks, dtype: str = "uint32", *, errors: bool = False):
+        """Python Cuda2dPlan.batch2d_bslz4_stack (src/python/cuda.rs:1176-1256):
+        one (n_frames, n_azimuthal, n_radial) float64 array, or (intensity,
+        errors) with errors=True."""
+        i, s, _ = self.integrate_bslz4_stack(chunks, dtype, errors)
+        shape = (len(i), self.n_azimuthal, self.n_points)
+        return (i.reshape(shape), s.reshape(shape)) if errors else i.reshape(shape)
+
     def integrate1d(self, *a, **k):
         raise TypeError("a 2D plan integrates with integrate2d")
 
     batch1d = integrate1d
+    batch1d_bslz4 = integrate1d
 
 
 class BatchIterator(Iterator[BatchResult]):

@@ -203,6 +203,45 @@ DG_EXPORT dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_
 DG_EXPORT dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current,
                                     int32_t *count);
 
+/* Bitshuffle/LZ4 frames. Replaces Cuda1dPlan::integrate_bslz4 and
+ * Cuda2dPlan::integrate_bslz4 / integrate_bslz4_into
+ * (src/integration/cuda.rs:554-564, :758-767, :843-863), whose chunks are
+ * `&[&[u8]]`: chunks[f] points to chunk_bytes[f] bytes of frame f's raw HDF5
+ * Bitshuffle/LZ4 chunk in HOST memory (a big-endian u64 of the frame's bytes,
+ * a big-endian u32 block size with 0 meaning 8192, then per block a
+ * big-endian u32 length and an LZ4 block of bitshuffled elements, the last
+ * n mod 8 elements verbatim). dtype is DG_U16, DG_U32 or DG_I32 (Bslz4Dtype,
+ * cuda.rs:338-342). Only the compressed bytes cross PCIe; the frames are
+ * decoded on the device and integrated as by dg_integrate, with identical
+ * results. Block sizes up to 48 KiB, multiples of 8 elements. A chunk whose
+ * header does not match the plan's frame size, whose blocks are truncated or
+ * exceed the LZ4 bound is rejected with DG_INVALID_INPUT before any device
+ * work (device.rs:2056-2178); malformed LZ4 data found while decoding returns
+ * DG_INVALID_INPUT ("corrupt or truncated Bitshuffle/LZ4 compressed block").
+ * Chunks may be pageable or pinned; pinned chunks copy asynchronously while
+ * the previous batch is decoded and integrated. Synchronous. */
+DG_EXPORT dg_status dg_integrate_bslz4(dg_plan *plan, const void *const *chunks,
+                                       const int64_t *chunk_bytes, int64_t n_frames,
+                                       int32_t dtype, uint32_t flags, double *out_intensity,
+                                       double *out_sigma, double *out_std);
+
+/* Host encoder of the same chunk format (bitshuffle, then LZ4 with greedy
+ * matching); it has no counterpart in the reference, whose chunks come from
+ * the detector's HDF5 files. Writes the chunk of n_elems elements of
+ * elem_bytes (2 or 4) bytes to out (capacity bytes; dg_bslz4_bound gives a
+ * sufficient capacity, or -1 for invalid arguments) and its size to
+ * *out_bytes. block_bytes 0 writes the default 8192-byte blocks. */
+DG_EXPORT int64_t dg_bslz4_bound(int64_t n_elems, int32_t elem_bytes, int32_t block_bytes);
+DG_EXPORT dg_status dg_bslz4_compress(const void *frame, int64_t n_elems, int32_t elem_bytes,
+                                      int32_t block_bytes, void *out, int64_t capacity,
+                                      int64_t *out_bytes);
+
+/* Decode-kernel time of dg_integrate_bslz4 calls made while dg_plan_profile is
+ * enabled: the summed CUDA-event time of the decode launches and their number
+ * since the last reset (waits for the last one). */
+DG_EXPORT dg_status dg_plan_decode_time(dg_plan *plan, int32_t reset, double *ms,
+                                        int64_t *launches);
+
 /* Evaluates one FP64 primitive of the device table builders on n values in
  * DEVICE memory of the current device, for parity checks against the C
  * library the reference calls (f64::atan2 and f64::sin, geometry.rs:684-692,

@@ -8,11 +8,13 @@ include/dioptrin_gpu.h. This package mirrors the reference's Python API:
 ``Integrator.prepare_cuda1d`` / ``prepare_cuda2d``.
 """
 from ._native import CudaUnavailableError, RequestTimeout
-from .integrator import (BatchIterator, BatchResult, Cuda1dPlan, Cuda2dPlan,
+from .integrator import (BatchIterator, BatchResult, Cuda1dPlan, Cuda2dPlan, Dynamic1dPlan,
+                         Dynamic1dWorker, IntermediateResult1d,
                          IntegrationResult, Integrator, Poni, bslz4_compress, cuda_available,
                          cuda_info)
 from .server import RequestLoop
 
 __all__ = ["BatchIterator", "BatchResult", "Cuda1dPlan", "Cuda2dPlan", "CudaUnavailableError",
+           "Dynamic1dPlan", "Dynamic1dWorker", "IntermediateResult1d",
            "IntegrationResult", "Integrator", "Poni", "RequestLoop", "RequestTimeout",
            "bslz4_compress", "cuda_available", "cuda_info"]

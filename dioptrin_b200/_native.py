@@ -27,6 +27,8 @@ EXPORTS = [
     "dg_integrate_device_plain", "dg_integrate_device_noalloc", "dg_plan_profile",
     "dg_plan_kernel_time", "dg_plan_autotune", "dg_plan_variant", "dg_eval_math",
     "dg_integrate_bslz4", "dg_bslz4_bound", "dg_bslz4_compress", "dg_plan_decode_time",
+    "dg_integrate_dynamic", "dg_integrate_dynamic_device", "dg_integrate_raw",
+    "dg_integrate_raw_device",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
     "dg_device_info_get", "dg_last_error",
@@ -126,6 +128,14 @@ def lib():
         L.dg_bslz4_compress.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_int64,
                                         P(C.c_int64)]
         L.dg_plan_decode_time.argtypes = [vp, C.c_int32, pd, P(C.c_int64)]
+        L.dg_integrate_dynamic.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64,
+                                           C.c_uint32, pd, pd]
+        L.dg_integrate_dynamic_device.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64,
+                                                  C.c_uint32, vp, vp, vp]
+        L.dg_integrate_raw.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64, C.c_uint32,
+                                       pd, pd, pd, pd]
+        L.dg_integrate_raw_device.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64,
+                                              C.c_uint32, vp, vp, vp, vp, vp]
         L.dg_server_create.argtypes = [P(ServerConfig), P(vp)]
         L.dg_server_destroy.argtypes = [vp]
         L.dg_server_register.argtypes = [vp, C.c_uint64, P(Geometry), P(Method), P(C.c_uint8),

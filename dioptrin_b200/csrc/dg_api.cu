@@ -180,8 +180,10 @@ int64_t dg_plan::device_bytes() const {
          gather.den_f32.bytes() +
          gather.valid_std.bytes() + gather.partial.bytes() + gather.fl_unit.bytes() +
          gather.fl_px.bytes() + gather.fl_pair_a.bytes() + gather.fl_pair_b.bytes() +
-         gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes();
-    b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes();
+         gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes() + gather.entry_raw.bytes() +
+         gather.cnt.bytes();
+    b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes() +
+         stage_mask.bytes();
     return b;
 }
 
@@ -281,6 +283,7 @@ dg_status dg_plan_destroy(dg_plan *plan) {
             plan->gather = dg::GatherTable();
             plan->stage_in.release();
             plan->stage_out.release();
+            plan->stage_mask.release();
             dg::bslz4_release(plan);
             if (plan->stream) cudaStreamDestroy(plan->stream);
             plan->stream = nullptr;
@@ -398,6 +401,156 @@ dg_status dg_integrate_device_plain(dg_plan *plan, const void *d_frames, int32_t
                            d_i + f * nb, (flags & DG_ERRORS) ? d_s + f * nb : nullptr,
                            (flags & DG_AZIMUTHAL_STD) ? d_d + f * nb : nullptr, s);
         }
+    });
+}
+
+namespace {
+
+// Arguments of the per-frame-mask and raw-sum calls.
+void check_masked(const dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                  const void *masks, int64_t mask_stride, uint32_t flags, bool raw,
+                  const void *o0, const void *o1, const void *o2, const void *o3) {
+    using dg::fail;
+    if (!plan) fail(DG_INVALID_INPUT, "plan must not be NULL");
+    (void)dtype_size(dtype);
+    if (n_frames < 0) fail(DG_INVALID_INPUT, "frame count must not be negative");
+    if (flags & DG_AZIMUTHAL_STD)
+        fail(DG_UNSUPPORTED, "azimuthal_std is not available with per-frame masks or raw sums");
+    if (flags & ~DG_ERRORS) fail(DG_INVALID_INPUT, "unknown flags");
+    if (!raw && !masks) fail(DG_INVALID_INPUT, "per-frame masks must not be NULL");
+    const int64_t npix = int64_t(plan->dim1) * plan->dim2;
+    if (mask_stride < 0 || (mask_stride != 0 && mask_stride < npix))
+        fail(DG_INVALID_INPUT, "mask_stride must be 0 (one mask for every frame) or at least the "
+                               "frame's " + std::to_string(npix) + " pixels");
+    if (n_frames == 0) return;
+    if (!frames) fail(DG_INVALID_INPUT, "frames must not be NULL");
+    if (!o0) fail(DG_INVALID_INPUT, raw ? "signal output must not be NULL"
+                                        : "intensity output must not be NULL");
+    if (raw) {
+        if (!o1 || !o3) fail(DG_INVALID_INPUT, "norm and count outputs must not be NULL");
+        if ((flags & DG_ERRORS) && !o2) fail(DG_INVALID_INPUT, "variance requested without an output");
+    } else if ((flags & DG_ERRORS) && !o1) {
+        fail(DG_INVALID_INPUT, "errors requested without an output");
+    }
+}
+
+// Host-memory form of the masked / raw calls: frames, masks and results
+// staged through the plan's buffers in chunks of max_batch_frames.
+void run_masked_host(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                     const uint8_t *masks, int64_t mask_stride, uint32_t flags, bool raw,
+                     double *o0, double *o1, double *o2, double *o3) {
+    std::lock_guard<std::mutex> lock(plan->mu);
+    DeviceScope scope(plan->device);
+    cudaStream_t s = plan->stream;
+    const int64_t npix = int64_t(plan->dim1) * plan->dim2;
+    const size_t es = dtype_size(dtype);
+    const int64_t nb = plan->n_bins;
+    const int64_t chunk = std::min<int64_t>(plan->max_batch_frames, n_frames);
+    const int nout = raw ? 4 : 2;
+    if (plan->stage_in.count < size_t(chunk * npix * es)) {
+        plan->stage_in.release();
+        plan->stage_in.alloc(size_t(chunk * npix * es));
+    }
+    if (plan->stage_out.count < size_t(chunk * nb * nout)) {
+        plan->stage_out.release();
+        plan->stage_out.alloc(size_t(chunk * nb * nout));
+    }
+    const int64_t mask_rows = masks ? (mask_stride ? chunk : 1) : 0;
+    if (plan->stage_mask.count < size_t(mask_rows * npix)) {
+        plan->stage_mask.release();
+        plan->stage_mask.alloc(size_t(mask_rows * npix));
+    }
+    dg::prepare_raw(plan->gather, plan->table, plan->norm.ptr, s);
+    if (masks && !mask_stride)
+        DG_CUDA(cudaMemcpyAsync(plan->stage_mask.ptr, masks, size_t(npix), cudaMemcpyHostToDevice, s));
+    for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
+        const int64_t nf = std::min<int64_t>(chunk, n_frames - f0);
+        DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr,
+                                static_cast<const unsigned char *>(frames) + f0 * npix * es,
+                                size_t(nf * npix * es), cudaMemcpyHostToDevice, s));
+        if (masks && mask_stride)
+            DG_CUDA(cudaMemcpy2DAsync(plan->stage_mask.ptr, size_t(npix), masks + f0 * mask_stride,
+                                      size_t(mask_stride), size_t(npix), size_t(nf),
+                                      cudaMemcpyHostToDevice, s));
+        double *d[4];
+        for (int k = 0; k < 4; ++k) d[k] = plan->stage_out.ptr + k * nf * nb;
+        double *h[4] = {o0, o1, o2, o3};
+        const bool used[4] = {true, raw || (flags & DG_ERRORS), raw && (flags & DG_ERRORS), raw};
+        dg::run_gather_raw(plan->gather, plan->stage_in.ptr, dtype, npix, nf,
+                           masks ? plan->stage_mask.ptr : nullptr, mask_stride ? npix : 0, flags,
+                           raw, d[0], used[1] ? d[1] : nullptr, used[2] ? d[2] : nullptr,
+                           used[3] ? d[3] : nullptr, s);
+        for (int k = 0; k < 4; ++k)
+            if (used[k])
+                DG_CUDA(cudaMemcpyAsync(h[k] + f0 * nb, d[k], size_t(nf * nb) * 8,
+                                        cudaMemcpyDeviceToHost, s));
+    }
+    DG_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+
+dg_status dg_integrate_dynamic(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                               const uint8_t *masks, int64_t mask_stride, uint32_t flags,
+                               double *out_intensity, double *out_sigma) {
+    return guarded([&] {
+        check_masked(plan, frames, dtype, n_frames, masks, mask_stride, flags, false,
+                     out_intensity, out_sigma, nullptr, nullptr);
+        if (n_frames == 0) return;
+        run_masked_host(plan, frames, dtype, n_frames, masks, mask_stride, flags, false,
+                        out_intensity, out_sigma, nullptr, nullptr);
+    });
+}
+
+dg_status dg_integrate_dynamic_device(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                      int64_t n_frames, const uint8_t *d_masks,
+                                      int64_t mask_stride, uint32_t flags, double *d_i,
+                                      double *d_s, void *stream) {
+    return guarded([&] {
+        check_masked(plan, d_frames, dtype, n_frames, d_masks, mask_stride, flags, false, d_i,
+                     d_s, nullptr, nullptr);
+        if (n_frames == 0) return;
+        check_device_alignment(d_frames, dtype, d_i, d_s, nullptr);
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        dg::prepare_raw(plan->gather, plan->table, plan->norm.ptr, s);
+        dg::run_gather_raw(plan->gather, d_frames, dtype, int64_t(plan->dim1) * plan->dim2,
+                           n_frames, d_masks, mask_stride, flags, false, d_i,
+                           (flags & DG_ERRORS) ? d_s : nullptr, nullptr, nullptr, s);
+    });
+}
+
+dg_status dg_integrate_raw(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
+                           const uint8_t *masks, int64_t mask_stride, uint32_t flags,
+                           double *out_signal, double *out_norm, double *out_variance,
+                           double *out_count) {
+    return guarded([&] {
+        check_masked(plan, frames, dtype, n_frames, masks, mask_stride, flags, true, out_signal,
+                     out_norm, out_variance, out_count);
+        if (n_frames == 0) return;
+        run_masked_host(plan, frames, dtype, n_frames, masks, mask_stride, flags, true,
+                        out_signal, out_norm, out_variance, out_count);
+    });
+}
+
+dg_status dg_integrate_raw_device(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                  int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride,
+                                  uint32_t flags, double *d_signal, double *d_norm,
+                                  double *d_variance, double *d_count, void *stream) {
+    return guarded([&] {
+        check_masked(plan, d_frames, dtype, n_frames, d_masks, mask_stride, flags, true,
+                     d_signal, d_norm, d_variance, d_count);
+        if (n_frames == 0) return;
+        check_device_alignment(d_frames, dtype, d_signal, d_norm, d_count);
+        check_device_alignment(d_frames, dtype, d_variance, nullptr, nullptr);
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        dg::prepare_raw(plan->gather, plan->table, plan->norm.ptr, s);
+        dg::run_gather_raw(plan->gather, d_frames, dtype, int64_t(plan->dim1) * plan->dim2,
+                           n_frames, d_masks, mask_stride, flags, true, d_signal, d_norm,
+                           (flags & DG_ERRORS) ? d_variance : nullptr, d_count, s);
     });
 }
 

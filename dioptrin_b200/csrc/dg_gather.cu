@@ -54,7 +54,10 @@ constexpr int kVariantCount = 7;
 constexpr int kSegMax = 256;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
-enum Mode { kIntensity = 0, kErrors = 1, kSpread = 2 };
+// kRaw: the per-frame-mask gather (entries {pixel, w, w*norm}); it sums
+// S = sum w*s, V = sum w^2*max(s,0), N = sum w*norm and C = sum w over the
+// entries whose pixel the frame's mask leaves unmasked.
+enum Mode { kIntensity = 0, kErrors = 1, kSpread = 2, kRaw = 3 };
 
 template <typename P>
 constexpr bool is_float_px() {
@@ -67,8 +70,10 @@ constexpr bool is_float_px() {
 // A = sum c*t = S - o*sum c*n is formed in the finalize.
 template <int MODE, typename P>
 struct NAcc {
-    static constexpr int value =
-        MODE == kIntensity ? 1 : MODE == kErrors ? 2 : (is_float_px<P>() ? 5 : 3);
+    static constexpr int value = MODE == kIntensity ? 1
+                                 : MODE == kErrors  ? 2
+                                 : MODE == kRaw     ? 4
+                                                    : (is_float_px<P>() ? 5 : 3);
 };
 
 template <typename P>
@@ -173,8 +178,10 @@ __global__ void __launch_bounds__(kThreads)
     k_gather(const int2 *__restrict__ units, const int4 *__restrict__ segs,
              const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
              const int32_t *__restrict__ first_valid, const P *__restrict__ frames,
-             int64_t n_pixels, int n_frames, int n_segments, double *__restrict__ partial) {
+             int64_t n_pixels, int n_frames, int n_segments, double *__restrict__ partial,
+             const uint8_t *__restrict__ masks, int64_t mask_stride) {
     constexpr int NA = NAcc<MODE, P>::value;
+    constexpr bool WIDE = MODE == kSpread || MODE == kRaw;  // 16-byte entries
     constexpr int GROUPS = 32 / SLICES;         // frame lane groups per warp
     constexpr int TASK_FRAMES = GROUPS * FPL;  // frames per task
     static_assert(kFlush % U == 0, "flush cadence must be a multiple of the unroll");
@@ -197,7 +204,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int i = 0; i < nseg; ++i) {
         const int4 sg = segs[seg0 + i];
         const int len = sg.z - sg.y, off = s_off[i];
-        if (MODE == kSpread) {
+        if (WIDE) {
             float4 *st = reinterpret_cast<float4 *>(smem) + off;
             for (int j = threadIdx.x; j < len; j += kThreads) st[j] = entry_std[sg.y + j];
         } else {
@@ -221,11 +228,13 @@ __global__ void __launch_bounds__(kThreads)
         const int row = sg.x, len = sg.z - sg.y, off = s_off[si];
         const int fbase = grp * TASK_FRAMES + fg * FPL;
         const P *fr[FPL];
+        const uint8_t *mk[FPL];
         bool fv[FPL];
 #pragma unroll
         for (int q = 0; q < FPL; ++q) {
             fv[q] = fbase + q < n_frames;
             fr[q] = frames + int64_t(fv[q] ? fbase + q : 0) * n_pixels;
+            mk[q] = MODE == kRaw ? masks + int64_t(fv[q] ? fbase + q : 0) * mask_stride : nullptr;
         }
         float origin[FPL];
 #pragma unroll
@@ -243,7 +252,43 @@ __global__ void __launch_bounds__(kThreads)
         // the segment end contribute zero without touching the frame.
         auto step = [&](int j0, auto check) {
             constexpr bool CHECK = decltype(check)::value;
-            if (MODE == kSpread) {
+            if (MODE == kRaw) {
+                float4 e[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int j = j0 + SLICES * u;
+                    if (CHECK)
+                        e[u] = j < len ? reinterpret_cast<const float4 *>(smem)[off + j]
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+                    else
+                        e[u] = reinterpret_cast<const float4 *>(smem)[off + j];
+                }
+                float sv[U][FPL];
+                bool live[U][FPL];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int q = 0; q < FPL; ++q) {
+                        const uint32_t col = uint32_t(__float_as_int(e[u].x));
+                        const bool in = !CHECK || j0 + SLICES * u < len;
+                        sv[u][q] = in ? load_px<P>(fr[q], col) : 0.f;
+                        live[u][q] = in && __ldg(mk[q] + col) == 0;
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+#pragma unroll
+                    for (int q = 0; q < FPL; ++q) {
+                        // a masked pixel adds nothing, whatever its value
+                        const float c = live[u][q] ? e[u].y : 0.f;
+                        const float cn = live[u][q] ? e[u].z : 0.f;
+                        const float v = live[u][q] ? sv[u][q] : 0.f;
+                        acc[q][0].fma(c, v);
+                        acc[q][1].fma(__fmul_rn(c, c), is_unsigned_px<P>() ? v : fmaxf(v, 0.f));
+                        acc[q][2].add(cn);
+                        acc[q][3].add(c);
+                    }
+                }
+            } else if (MODE == kSpread) {
                 float4 e[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
@@ -928,6 +973,15 @@ __global__ void k_finalize(const double *__restrict__ partial, const int32_t *__
         for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
     }
     int64_t o = int64_t(f) * n_rows + r;
+    if (MODE == kRaw) {  // denominators of this frame's mask
+        const double n = v[2];
+        out_i[o] = n == 0.0 ? 0.0 : v[0] / n;
+        if (out_s) {
+            const double q = n == 0.0 ? 0.0 : v[1] / (n * n);
+            out_s[o] = sqrt(q > 0.0 ? q : 0.0);
+        }
+        return;
+    }
     if (MODE != kSpread) {
         double n = den[r];
         out_i[o] = n == 0.0 ? 0.0 : v[0] / n;
@@ -960,6 +1014,52 @@ __global__ void k_finalize(const double *__restrict__ partial, const int32_t *__
     const double m2 = v[2] - mean * a1;
     const double q = m2 / sw;
     out_d[o] = sqrt(q > 0.0 ? q : 0.0);
+}
+
+// Raw sums per (frame, row) (IntermediateResult1d, lut/integrate.rs:372-379):
+// S and V from the partial sums; N and C from them too for the per-frame-mask
+// gather, else the plan's strict FP64 denominator and weight sum.
+template <int MODE>
+__global__ void k_finalize_raw(const double *__restrict__ partial,
+                               const int32_t *__restrict__ row_seg,
+                               const int32_t *__restrict__ seg_ids, const double *__restrict__ den,
+                               const double *__restrict__ cnt, int n_rows, int n_frames,
+                               double *__restrict__ out_sig, double *__restrict__ out_norm,
+                               double *__restrict__ out_var, double *__restrict__ out_cnt) {
+    constexpr int NA = NAcc<MODE, float>::value;
+    int64_t id = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    if (id >= int64_t(n_rows) * n_frames) return;
+    int f = int(id % n_frames), r = int(id / n_frames);
+    double v[NA];
+    for (int a = 0; a < NA; ++a) v[a] = 0.0;
+    for (int k = row_seg[r]; k < row_seg[r + 1]; ++k) {
+        const double *p = partial + int64_t(seg_ids[k]) * NA * n_frames + f;
+        for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
+    }
+    const int64_t o = int64_t(f) * n_rows + r;
+    out_sig[o] = v[0];
+    if (out_var) out_var[o] = NA > 1 ? v[1] : 0.0;
+    out_norm[o] = MODE == kRaw ? v[NA > 2 ? 2 : 0] : den[r];
+    out_cnt[o] = MODE == kRaw ? v[NA > 3 ? 3 : 0] : cnt[r];
+}
+
+// Entries for the per-frame-mask gather, {pixel, w, w*norm} in FP32 (the
+// product formed in FP64), and the strict FP64 weight sum of every row.
+__global__ void k_pack_raw(const int64_t *__restrict__ row_ptr, int n_rows,
+                           const int32_t *__restrict__ col, const double *__restrict__ w,
+                           const double *__restrict__ norm, float4 *__restrict__ entry_raw,
+                           double *__restrict__ cnt) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    double sum = 0.0;
+    for (int64_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+        const int32_t j = col[k];
+        const double c = w[k];
+        sum += c;
+        entry_raw[k] = make_float4(__int_as_float(j), __double2float_rn(c),
+                                   __double2float_rn(c * norm[j]), 0.f);
+    }
+    cnt[r] = sum;
 }
 
 // Packs the masked f64 table into the gather's entry formats and computes
@@ -1036,17 +1136,23 @@ void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, doub
 // its partial sums in `partial`.
 template <int MODE, typename P>
 void launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pixels, int nf,
-                   double *partial, cudaStream_t s) {
-    if (variant == 5 || variant == 6) {
-        if (variant == 5) launch_fl<MODE, P, 4, false>(t, fp, n_pixels, nf, partial, s);
-        else launch_fl<MODE, P, 4, true>(t, fp, n_pixels, nf, partial, s);
-        DG_CUDA(cudaGetLastError());
-        return;
+                   double *partial, cudaStream_t s, const uint8_t *masks = nullptr,
+                   int64_t mask_stride = 0) {
+    if constexpr (MODE == kRaw) {
+        if (variant == 5 || variant == 6) variant = 2;  // entry-lane mappings only
+    } else {
+        if (variant == 5 || variant == 6) {
+            if (variant == 5) launch_fl<MODE, P, 4, false>(t, fp, n_pixels, nf, partial, s);
+            else launch_fl<MODE, P, 4, true>(t, fp, n_pixels, nf, partial, s);
+            DG_CUDA(cudaGetLastError());
+            return;
+        }
     }
-    const size_t smem = size_t(t.unit_cap) * (MODE == kSpread ? 16 : 8);
-#define DG_GATHER_ARGS                                                                        \
-    t.unit.ptr, t.seg.ptr, t.entry.ptr, t.entry_std.ptr, t.first_valid.ptr, fp, n_pixels, nf, \
-        t.n_segments, partial
+    const size_t smem = size_t(t.unit_cap) * (MODE == kSpread || MODE == kRaw ? 16 : 8);
+    const float4 *wide = MODE == kRaw ? t.entry_raw.ptr : t.entry_std.ptr;
+#define DG_GATHER_ARGS                                                                     \
+    t.unit.ptr, t.seg.ptr, t.entry.ptr, wide, t.first_valid.ptr, fp, n_pixels, nf, t.n_segments, \
+        partial, masks, mask_stride
     switch (variant) {
     case 0: k_gather<MODE, P, 32, 4, 4><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
     case 1: k_gather<MODE, P, 32, 2, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
@@ -1346,6 +1452,100 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
             case DG_I32: finalize_typed<int32_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
             case DG_F32: finalize_typed<float>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
             case DG_F64: finalize_typed<double>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            }
+        }
+    }
+}
+
+void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s) {
+    if (t.cnt.ptr) return;
+    t.entry_raw.alloc(std::max<size_t>(size_t(table.nnz), 1));
+    t.cnt.alloc(std::max<size_t>(size_t(table.n_rows), 1));
+    if (table.n_rows > 0)
+        k_pack_raw<<<unsigned((table.n_rows + 127) / 128), 128, 0, s>>>(
+            table.row_ptr.ptr, int(table.n_rows), table.col.ptr, table.w.ptr, d_norm,
+            t.entry_raw.ptr, t.cnt.ptr);
+    DG_CUDA(cudaGetLastError());
+}
+
+namespace {
+
+template <typename P>
+void launch_raw(GatherTable &t, const void *frames, int64_t n_pixels, int nf, int mode,
+                const uint8_t *masks, int64_t mask_stride, cudaStream_t s) {
+    const P *fp = static_cast<const P *>(frames);
+    if (mode == kRaw)
+        launch_gather<kRaw, P>(t, t.variant, fp, n_pixels, nf, t.partial.ptr, s, masks, mask_stride);
+    else if (mode == kErrors)
+        launch_gather<kErrors, P>(t, t.variant, fp, n_pixels, nf, t.partial.ptr, s);
+    else
+        launch_gather<kIntensity, P>(t, t.variant, fp, n_pixels, nf, t.partial.ptr, s);
+}
+
+}  // namespace
+
+void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
+                    int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride, uint32_t flags,
+                    bool raw, double *o0, double *o1, double *o2, double *o3, cudaStream_t s) {
+    if (n_frames <= 0) return;
+    if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
+    if (!t.cnt.ptr) fail(DG_DEVICE, "raw-sum entries were not prepared");
+    const bool errors = (flags & DG_ERRORS) != 0;
+    const int mode = d_masks ? kRaw : errors ? kErrors : kIntensity;
+    const int64_t chunk = 256;
+    const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 5;
+    if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+    const size_t esize = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
+    for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
+        const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
+        const void *fp = static_cast<const unsigned char *>(d_frames) + f0 * n_pixels * esize;
+        const uint8_t *mp = d_masks ? d_masks + f0 * mask_stride : nullptr;
+        if (t.n_units > 0) {
+            std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
+            if (t.profile) {
+                EventPool &p = t.events;
+                if (p.used == p.events.size()) {
+                    std::pair<cudaEvent_t, cudaEvent_t> e{};
+                    DG_CUDA(cudaEventCreate(&e.first));
+                    DG_CUDA(cudaEventCreate(&e.second));
+                    p.events.push_back(e);
+                }
+                ev = &p.events[p.used++];
+                DG_CUDA(cudaEventRecord(ev->first, s));
+            }
+            ++t.launches;
+            switch (dtype) {
+            case DG_U16: launch_raw<uint16_t>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
+            case DG_U32: launch_raw<uint32_t>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
+            case DG_I32: launch_raw<int32_t>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
+            case DG_F32: launch_raw<float>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
+            case DG_F64: launch_raw<double>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
+            }
+            if (ev) DG_CUDA(cudaEventRecord(ev->second, s));
+        }
+        if (t.n_rows == 0) continue;
+        ++t.launches;
+        const int64_t off = f0 * t.n_rows;
+        auto at = [&](double *o) { return o ? o + off : nullptr; };
+        const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);
+        if (raw) {
+#define DG_RAW_ARGS                                                                          \
+    t.partial.ptr, t.row_seg.ptr, t.seg_ids.ptr, t.den.ptr, t.cnt.ptr, t.n_rows, nf, at(o0), \
+        at(o1), errors ? at(o2) : nullptr, at(o3)
+            if (mode == kRaw) k_finalize_raw<kRaw><<<blocks, 256, 0, s>>>(DG_RAW_ARGS);
+            else if (mode == kErrors) k_finalize_raw<kErrors><<<blocks, 256, 0, s>>>(DG_RAW_ARGS);
+            else k_finalize_raw<kIntensity><<<blocks, 256, 0, s>>>(DG_RAW_ARGS);
+#undef DG_RAW_ARGS
+            DG_CUDA(cudaGetLastError());
+        } else {
+            if (mode != kRaw) fail(DG_INVALID_INPUT, "normalised results need per-frame masks");
+            double *oi = at(o0), *os = errors ? at(o1) : nullptr;
+            switch (dtype) {
+            case DG_U16: launch_finalize<kRaw, uint16_t>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
+            case DG_U32: launch_finalize<kRaw, uint32_t>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
+            case DG_I32: launch_finalize<kRaw, int32_t>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
+            case DG_F32: launch_finalize<kRaw, float>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
+            case DG_F64: launch_finalize<kRaw, double>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
             }
         }
     }

@@ -182,6 +182,10 @@ struct GatherTable {
     DeviceArray<float4> fl_pair_s;    // pair_a with the spread's weights, when they differ
     const float4 *fl_pair_as = nullptr;  // the spread's pair_a (fl_pair_s or fl_pair_a)
     DeviceArray<int32_t> fl_seg_org;  // per segment: its origin pixel's index in the unit list
+    // Raw-sum and per-frame-mask gathers, built on first use (prepare_raw):
+    // {pixel bits, w, w*norm, 0} per entry and the FP64 weight sum per row.
+    DeviceArray<float4> entry_raw;
+    DeviceArray<double> cnt;
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
     bool profile = false;
@@ -200,6 +204,17 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                 int64_t n_frames, uint32_t flags, int precision, double *d_i, double *d_sigma,
                 double *d_std, cudaStream_t stream);
+// Raw sums and per-frame masks. prepare_raw builds the entries once (from the
+// plan's masked f64 table and per-pixel norm). run_gather_raw: with d_masks
+// (n_frames masks mask_stride bytes apart, 0 = one mask for every frame;
+// nonzero bytes mask a pixel) sums over the unmasked entries of each frame,
+// else over the table; raw: o0..o3 = signal, norm, variance (DG_ERRORS),
+// count; otherwise o0, o1 = intensity and sigma (DG_ERRORS) normalised by
+// the frame's own denominators (needs d_masks).
+void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s);
+void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
+                    int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride, uint32_t flags,
+                    bool raw, double *o0, double *o1, double *o2, double *o3, cudaStream_t s);
 // Number of gather kernel launches run_gather enqueues (for launch counting).
 int gather_launches_per_call();
 // Lane-mapping variants of the gather, and the per-plan autotuner: times each
@@ -247,6 +262,7 @@ struct dg_plan {
     // staging for host-memory calls
     dg::DeviceArray<unsigned char> stage_in;
     dg::DeviceArray<double> stage_out;
+    dg::DeviceArray<unsigned char> stage_mask;  // per-frame masks (dg_integrate_dynamic / _raw)
     // compressed frames and their block descriptors (dg_integrate_bslz4)
     dg::DeviceArray<unsigned char> stage_comp;
     dg::DeviceArray<unsigned char> stage_desc;

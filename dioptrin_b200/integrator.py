@@ -104,6 +104,20 @@ class IntegrationResult:
         lambda s: None if s.azimuthal_array is None else s.azimuthal_array.tolist())
 
 
+class IntermediateResult1d:
+    """Sums before division (IntermediateResult1d, src/lut/integrate.rs:372-379):
+    per bin sum_signal = sum w*s, sum_norm = sum w*norm, sum_variance =
+    sum w^2*max(s,0) (None unless requested) and count = sum w. ``bins`` is the
+    radial axis (the bin index order of a 2D plan's rows otherwise)."""
+
+    def __init__(self, bins, sum_signal, sum_norm, sum_variance, count):
+        self.bins = np.asarray(bins)
+        self.sum_signal = np.asarray(sum_signal)
+        self.sum_norm = np.asarray(sum_norm)
+        self.sum_variance = None if sum_variance is None else np.asarray(sum_variance)
+        self.count = np.asarray(count)
+
+
 class BatchResult:
     """One batch item (dioptrin.pyi:243-275)."""
 
@@ -332,6 +346,70 @@ class Cuda1dPlan:
         return [IntegrationResult(self._radial, i[k], None if s is None else s[k])
                 for k in range(len(i))]
 
+    def _stack_and_masks(self, frames, masks):
+        stack = np.ascontiguousarray(frames)
+        if stack.dtype not in _DTYPES:
+            raise TypeError(f"unsupported dtype {stack.dtype}")
+        if stack.ndim == 2:
+            stack = stack[None]
+        if tuple(stack.shape[1:]) != self.shape:
+            raise ValueError(f"frames of shape {stack.shape[1:]} do not match plan {self.shape}")
+        if masks is None:
+            return stack, None, 0
+        m = np.ascontiguousarray(masks)
+        if m.dtype == np.bool_:
+            m = m.view(np.uint8)
+        if m.dtype != np.uint8:
+            raise TypeError(f"masks must be uint8 (or bool), got {m.dtype}")
+        if m.shape == self.shape:
+            return stack, m, 0
+        if m.shape != stack.shape:
+            raise ValueError(f"masks of shape {m.shape} match neither the plan {self.shape} "
+                             f"nor the frames {stack.shape}")
+        return stack, m, self.shape[0] * self.shape[1]
+
+    def integrate_dynamic_stack(self, frames, masks, errors: bool = False):
+        """Integrate frames with per-frame masks (MaskMode::Dynamic,
+        src/integration/dynamic.rs:159-196): `masks` is one (dim1, dim2)
+        uint8 mask for every frame or one per frame; nonzero masks a pixel.
+        Denominators are summed over each frame's unmasked entries. Returns
+        (I, sigma) arrays of shape (n, n_bins), sigma None unless errors."""
+        if masks is None:
+            raise ValueError("per-frame masks are required")
+        stack, m, stride = self._stack_and_masks(frames, masks)
+        n = stack.shape[0]
+        nb = self.n_points * max(1, self.n_azimuthal)
+        oi = np.empty((n, nb))
+        os_ = np.empty((n, nb)) if errors else None
+        N.check(N.lib().dg_integrate_dynamic(self._h, stack.ctypes.data, _DTYPES[stack.dtype], n,
+                                             m.ctypes.data, stride,
+                                             N.DG_ERRORS if errors else 0, _dp(oi), _dp(os_)))
+        return oi, os_
+
+    def integrate_raw_stack(self, frames, masks=None, with_variance: bool = False) -> list:
+        """Raw sums of every frame (Integrator::integrate1d_raw*,
+        src/integration/methods.rs:299-360) as IntermediateResult1d; masks
+        None uses the plan's own mask, else per-frame masks as in
+        integrate_dynamic_stack."""
+        stack, m, stride = self._stack_and_masks(frames, masks)
+        n = stack.shape[0]
+        nb = self.n_points * max(1, self.n_azimuthal)
+        out = [np.empty((n, nb)) for _ in range(4)]
+        if not with_variance:
+            out[2] = None
+        N.check(N.lib().dg_integrate_raw(self._h, stack.ctypes.data, _DTYPES[stack.dtype], n,
+                                         None if m is None else m.ctypes.data, stride,
+                                         N.DG_ERRORS if with_variance else 0, _dp(out[0]),
+                                         _dp(out[1]), _dp(out[2]), _dp(out[3])))
+        bins = self._radial if not self.n_azimuthal else np.arange(nb, dtype=np.float64)
+        return [IntermediateResult1d(bins, out[0][k], out[1][k],
+                                     None if out[2] is None else out[2][k], out[3][k])
+                for k in range(n)]
+
+    def integrate1d_raw(self, image, *, with_variance: bool = False,
+                        mask=None) -> IntermediateResult1d:
+        return self.integrate_raw_stack(_frame_array(image), mask, with_variance)[0]
+
     def integrate1d(self, image: np.ndarray, *, errors: bool = False,
                     azimuthal_std: bool = False) -> IntegrationResult:
         a = _frame_array(image)
@@ -421,6 +499,65 @@ class Cuda2dPlan(Cuda1dPlan):
 
     batch1d = integrate1d
     batch1d_bslz4 = integrate1d
+
+
+class Dynamic1dPlan:
+    """A geometry-only table for frames with their own masks
+    (src/integration/dynamic.rs:9-16; Python Dynamic1dPlan,
+    src/python/dynamic.rs:9-50), resident on the device."""
+
+    def __init__(self, plan: Cuda1dPlan):
+        self._plan = plan
+
+    @property
+    def shape(self):
+        return self._plan.shape
+
+    @property
+    def n_points(self) -> int:
+        return self._plan.n_points
+
+    @property
+    def shared_plan_id(self) -> int:
+        return int(self._plan.handle or 0)
+
+    @property
+    def cuda_plan(self) -> Cuda1dPlan:
+        return self._plan
+
+    def worker(self, num_threads: int = 1) -> "Dynamic1dWorker":
+        if num_threads <= 0:
+            raise ValueError("num_threads must be positive")
+        return Dynamic1dWorker(self._plan)
+
+    def close(self) -> None:
+        self._plan.close()
+
+
+class Dynamic1dWorker:
+    """Dynamic1dWorker (src/python/dynamic.rs:52-110): integrates a frame
+    with its complete uint8 mask; calls share the plan and keep no state."""
+
+    def __init__(self, plan: Cuda1dPlan):
+        self._plan = plan
+
+    def integrate1d(self, image, mask=None, *, errors: bool = False,
+                    azimuthal_std: bool = False) -> IntegrationResult:
+        a = _frame_array(image)
+        if tuple(a.shape) != self._plan.shape:
+            raise ValueError("image shape does not match prepared plan")
+        if azimuthal_std:
+            raise ValueError("azimuthal_std is not available on the device with per-frame masks")
+        if mask is None:
+            mask = np.zeros(self._plan.shape, np.uint8)
+        i, s = self._plan.integrate_dynamic_stack(a, mask, errors)
+        return IntegrationResult(self._plan.radial_array, i[0], None if s is None else s[0])
+
+    def batch1d(self, images, masks, *, errors: bool = False) -> list:
+        """Many frames with one mask each (or one shared (dim1, dim2) mask)."""
+        i, s = self._plan.integrate_dynamic_stack(images, masks, errors)
+        return [IntegrationResult(self._plan.radial_array, i[k], None if s is None else s[k])
+                for k in range(len(i))]
 
 
 class BatchIterator(Iterator[BatchResult]):
@@ -689,6 +826,31 @@ class Integrator:
                                        azimuthal_range, errors: bool = False) -> IntegrationResult:
         """Integrator::integrate2d_on_azimuthal_range (src/integration/grid.rs:439)."""
         return self.integrate2d(image, n_radial, n_azimuthal, errors, azimuthal_range)
+
+    def prepare_dynamic1d(self, shape, n_points: int, *, precision: str = "f32_compensated",
+                          device: int = 0, max_batch_bytes: Optional[int] = None
+                          ) -> "Dynamic1dPlan":
+        """Integrator::prepare_dynamic1d (src/integration/dynamic.rs:29-65): one
+        geometry table without the stored mask, for frames that each bring
+        their complete mask. Built and kept on the device."""
+        saved = self._mask
+        self._mask = None
+        try:
+            plan = self.prepare_cuda1d(shape, n_points, precision=precision, device=device,
+                                       max_batch_bytes=max_batch_bytes)
+        finally:
+            self._mask = saved
+        return Dynamic1dPlan(plan)
+
+    def integrate1d_raw(self, image, n_points: int) -> IntermediateResult1d:
+        """Integrator::integrate1d_raw (src/integration/methods.rs:318-326)."""
+        a = _frame_array(image)
+        return self._plan(a.shape, n_points).integrate1d_raw(a)
+
+    def integrate1d_raw_with_variance(self, image, n_points: int) -> IntermediateResult1d:
+        """Integrator::integrate1d_raw_with_variance (methods.rs:329-337)."""
+        a = _frame_array(image)
+        return self._plan(a.shape, n_points).integrate1d_raw(a, with_variance=True)
 
     def _plan(self, shape, n_points: int) -> Cuda1dPlan:
         key = (tuple(shape), int(n_points))

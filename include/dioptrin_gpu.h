@@ -203,6 +203,50 @@ DG_EXPORT dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_
 DG_EXPORT dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current,
                                     int32_t *count);
 
+/* Per-frame masks (MaskMode::Dynamic). Replaces Dynamic1dPlan::integrate
+ * (src/integration/dynamic.rs:159-196; the per-row sums with a mask check,
+ * src/lut/prepared.rs:1011-1118), which the reference's GPU plans reject
+ * (src/integration/cuda.rs:1036-1040). masks holds n_frames uint8 masks of
+ * dim1 * dim2 bytes, mask_stride bytes apart (0: one mask for every frame);
+ * a nonzero byte masks its pixel. Each bin sums w*s, w^2*max(s,0) and
+ * w*norm over the entries whose pixel is unmasked in that frame, so
+ * denominators follow the frame's mask: I = 0 where the denominator is 0,
+ * else S/N; sigma likewise (normalize_bin, prepared.rs:985-996). A plan made
+ * for per-frame masks is created without a mask (the reference's
+ * prepare_dynamic1d excludes the stored mask); a plan mask, if given, is
+ * applied as well. DG_ERRORS only: azimuthal_std is DG_UNSUPPORTED here.
+ * Frames, masks and results in HOST memory; the _device form takes DEVICE
+ * memory and enqueues on `stream` (NULL: the plan's own) without
+ * synchronising. */
+DG_EXPORT dg_status dg_integrate_dynamic(dg_plan *plan, const void *frames, int32_t dtype,
+                                         int64_t n_frames, const uint8_t *masks,
+                                         int64_t mask_stride, uint32_t flags,
+                                         double *out_intensity, double *out_sigma);
+DG_EXPORT dg_status dg_integrate_dynamic_device(dg_plan *plan, const void *d_frames,
+                                                int32_t dtype, int64_t n_frames,
+                                                const uint8_t *d_masks, int64_t mask_stride,
+                                                uint32_t flags, double *d_intensity,
+                                                double *d_sigma, void *stream);
+
+/* Raw sums before division, for merging several detectors. Replaces
+ * Integrator::integrate1d_raw / integrate1d_raw_with_variance
+ * (src/integration/methods.rs:299-360), whose IntermediateResult1d
+ * (src/lut/integrate.rs:372-379) holds per bin sum_signal = sum w*s,
+ * sum_norm = sum w*norm, sum_variance = sum w^2*max(s,0) (with DG_ERRORS)
+ * and count = sum w. masks NULL: the plan's own mask, with sum_norm and
+ * count the plan's FP64 sums; otherwise per-frame masks as in
+ * dg_integrate_dynamic. Outputs are n_frames * n_bins doubles each
+ * (out_variance may be NULL without DG_ERRORS). */
+DG_EXPORT dg_status dg_integrate_raw(dg_plan *plan, const void *frames, int32_t dtype,
+                                     int64_t n_frames, const uint8_t *masks, int64_t mask_stride,
+                                     uint32_t flags, double *out_signal, double *out_norm,
+                                     double *out_variance, double *out_count);
+DG_EXPORT dg_status dg_integrate_raw_device(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                            int64_t n_frames, const uint8_t *d_masks,
+                                            int64_t mask_stride, uint32_t flags,
+                                            double *d_signal, double *d_norm,
+                                            double *d_variance, double *d_count, void *stream);
+
 /* Bitshuffle/LZ4 frames. Replaces Cuda1dPlan::integrate_bslz4 and
  * Cuda2dPlan::integrate_bslz4 / integrate_bslz4_into
  * (src/integration/cuda.rs:554-564, :758-767, :843-863), whose chunks are

@@ -1474,6 +1474,32 @@ void or_integrate_strict(const or_lut *lut, const double *den, const double *sig
     }
 }
 
+/* Raw per-row sums with a mask check, strict sequential order: row()
+ * (prepared.rs:1011-1118) with SIGNAL, NORM, VAR and COUNT; an entry whose
+ * pixel has a nonzero mask byte is skipped. S = sum w*s, N = sum w*norm,
+ * V = sum w*w*max(s, 0) (f64::max: a NaN signal gives 0), C = sum w. */
+void or_raw_sums(const or_lut *lut, const uint8_t *mask, const double *norm,
+                 const double *signal, double *out_s, double *out_n, double *out_v,
+                 double *out_c) {
+    for (int64_t r = 0; r < lut->n_rows; ++r) {
+        double s = 0.0, n = 0.0, v = 0.0, c = 0.0;
+        for (int64_t k = lut->row_ptr[r]; k < lut->row_ptr[r + 1]; ++k) {
+            int64_t j = lut->col[k];
+            if (mask && mask[j]) continue;
+            double w = lut->w ? lut->w[k] : 1.0, x = signal[j];
+            double var = (x != x) ? 0.0 : (x > 0.0 ? x : 0.0);
+            s = s + w * x;
+            v = v + w * w * var;
+            n = n + w * norm[j];
+            c += w;
+        }
+        out_s[r] = s;
+        out_n[r] = n;
+        out_v[r] = v;
+        out_c[r] = c;
+    }
+}
+
 /* integrate_with_columns (azimuthal.rs:48-118). */
 void or_azimuthal_std(const or_lut *lut, const uint8_t *mask, const double *norm,
                       const double *signal, const double *variance, double *intensity,

@@ -113,6 +113,9 @@ void or_denominators(const or_lut *lut, const double *norm, double *den);
 /* Strict f64 row gather + normalize_bin (prepared.rs:985-1118). */
 void or_integrate_strict(const or_lut *lut, const double *den, const double *signal,
                          int errors, double *intensity, double *sigma);
+void or_raw_sums(const or_lut *lut, const uint8_t *mask, const double *norm,
+                 const double *signal, double *out_s, double *out_n, double *out_v,
+                 double *out_c);
 /* Raw strict sums S = Σ w·s and V = Σ w²·max(s,0) per row. */
 void or_row_sums(const or_lut *lut, const double *signal, double *sum_signal,
                  double *sum_variance);

@@ -116,6 +116,7 @@ def _lib():
         lib.or_denominators.argtypes = [P(_Lut), pd, pd]
         lib.or_integrate_strict.argtypes = [P(_Lut), pd, pd, i, pd, pd]
         lib.or_row_sums.argtypes = [P(_Lut), pd, pd, pd]
+        lib.or_raw_sums.argtypes = [P(_Lut), pu8, pd, pd, pd, pd, pd, pd]
         lib.or_azimuthal_std.argtypes = [P(_Lut), pu8, pd, pd, pd, pd, pd, pd]
         lib.or_integrate_frames_mt.argtypes = [P(_Lut), pd, P(_Lut), pu8, pd, C.c_void_p, i,
                                                i64, i64, i, i, i, pd, pd, pd]
@@ -389,6 +390,18 @@ def row_sums(lut: Lut, signal: np.ndarray):
     src = lut._c()
     _lib().or_row_sums(C.byref(src), _dp(signal), _dp(s), _dp(v))
     return s, v
+
+
+def raw_sums(lut: Lut, mask: Optional[np.ndarray], norm: np.ndarray, signal: np.ndarray):
+    """(S, N, V, C) per row over the entries whose pixel is unmasked
+    (row(), src/lut/prepared.rs:1011-1118, strict order)."""
+    signal = np.ascontiguousarray(signal, np.float64).ravel()
+    norm = np.ascontiguousarray(norm, np.float64).ravel()
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8).ravel()
+    out = [np.empty(lut.n_rows) for _ in range(4)]
+    src = lut._c()
+    _lib().or_raw_sums(C.byref(src), _u8(m), _dp(norm), _dp(signal), *[_dp(o) for o in out])
+    return tuple(out)
 
 
 def azimuthal_std(lut: Lut, mask: Optional[np.ndarray], norm: np.ndarray,

@@ -10,11 +10,12 @@ include/dioptrin_gpu.h. This package mirrors the reference's Python API:
 from ._native import CudaUnavailableError, RequestTimeout
 from .integrator import (BatchIterator, BatchResult, Cuda1dPlan, Cuda2dPlan, Dynamic1dPlan,
                          Dynamic1dWorker, IntermediateResult1d,
-                         IntegrationResult, Integrator, Poni, bslz4_compress, cuda_available,
+                         IntegrationResult, Integrator, Poni, alloc_pinned, bslz4_compress,
+                         cuda_available, is_pinned,
                          cuda_info)
 from .server import RequestLoop
 
 __all__ = ["BatchIterator", "BatchResult", "Cuda1dPlan", "Cuda2dPlan", "CudaUnavailableError",
            "Dynamic1dPlan", "Dynamic1dWorker", "IntermediateResult1d",
            "IntegrationResult", "Integrator", "Poni", "RequestLoop", "RequestTimeout",
-           "bslz4_compress", "cuda_available", "cuda_info"]
+           "alloc_pinned", "bslz4_compress", "cuda_available", "cuda_info", "is_pinned"]

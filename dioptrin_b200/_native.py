@@ -20,6 +20,7 @@ PRECISIONS = {"f32": 0, "f32_compensated": 1, "f64": 2}
 DG_ERRORS, DG_AZIMUTHAL_STD = 1, 2
 DG_U16, DG_U32, DG_I32, DG_F32, DG_F64 = 0, 1, 2, 3, 4
 DG_PLAN_KEEP_TABLES = 1
+DG_PLAN_FLIP_VERTICAL = 2
 
 EXPORTS = [
     "dg_plan_create", "dg_plan_destroy", "dg_plan_query", "dg_plan_radial",
@@ -28,7 +29,7 @@ EXPORTS = [
     "dg_plan_kernel_time", "dg_plan_autotune", "dg_plan_variant", "dg_eval_math",
     "dg_integrate_bslz4", "dg_bslz4_bound", "dg_bslz4_compress", "dg_plan_decode_time",
     "dg_integrate_dynamic", "dg_integrate_dynamic_device", "dg_integrate_raw",
-    "dg_integrate_raw_device",
+    "dg_integrate_raw_device", "dg_host_alloc", "dg_host_free", "dg_host_is_pinned",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
     "dg_device_info_get", "dg_last_error",
@@ -132,6 +133,9 @@ def lib():
                                            C.c_uint32, pd, pd]
         L.dg_integrate_dynamic_device.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64,
                                                   C.c_uint32, vp, vp, vp]
+        L.dg_host_alloc.argtypes = [C.c_int32, C.c_int64, P(vp)]
+        L.dg_host_free.argtypes = [vp]
+        L.dg_host_is_pinned.argtypes = [vp]
         L.dg_integrate_raw.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64, C.c_uint32,
                                        pd, pd, pd, pd]
         L.dg_integrate_raw_device.argtypes = [vp, vp, C.c_int32, C.c_int64, vp, C.c_int64,
@@ -151,6 +155,7 @@ def lib():
             if name != "dg_last_error":
                 getattr(L, name).restype = C.c_int
         L.dg_bslz4_bound.restype = C.c_int64
+        L.dg_host_is_pinned.restype = C.c_int32
         _LIB = L
         return L
 

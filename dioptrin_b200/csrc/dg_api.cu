@@ -97,6 +97,8 @@ void check_config(const dg_geometry *g, const dg_method *m, int32_t dim1, int32_
     if (!g || !m) fail(DG_INVALID_INPUT, "geometry and method must not be NULL");
     if (n_radial <= 0) fail(DG_INVALID_INPUT, "n_points must be between 1 and 2147483647");
     if (n_azimuthal < 0) fail(DG_INVALID_INPUT, "n_azimuthal must not be negative");
+    if (m->flags & ~(DG_PLAN_KEEP_TABLES | DG_PLAN_FLIP_VERTICAL))
+        fail(DG_INVALID_INPUT, "unknown plan flags");
     if (n_azimuthal > 0 && int64_t(n_radial) * n_azimuthal > INT32_MAX)
         fail(DG_INVALID_INPUT, "2D bin count must be in 1..=2147483647");
     if (dim1 <= 0 || dim2 <= 0)
@@ -228,6 +230,7 @@ dg_status dg_plan_create(const dg_geometry *geometry, const dg_method *method,
             dg::compact_table(built.full, any ? d_mask.ptr : nullptr, int32_t(npix), s, plan->table);
             dg::make_gather_table(plan->table, built.norm.ptr, dim1, dim2, kStripRows, s,
                                   plan->gather);
+            if (method->flags & DG_PLAN_FLIP_VERTICAL) dg::flip_gather_rows(plan->gather, dim1, dim2, s);
             DG_CUDA(cudaEventRecord(e1, s));
             DG_CUDA(cudaEventSynchronize(e1));
             float ms = 0;
@@ -552,6 +555,41 @@ dg_status dg_integrate_raw_device(dg_plan *plan, const void *d_frames, int32_t d
                            n_frames, d_masks, mask_stride, flags, true, d_signal, d_norm,
                            (flags & DG_ERRORS) ? d_variance : nullptr, d_count, s);
     });
+}
+
+dg_status dg_host_alloc(int32_t device, int64_t bytes, void **out) {
+    return guarded([&] {
+        if (!out) dg::fail(DG_INVALID_INPUT, "out must not be NULL");
+        *out = nullptr;
+        if (bytes <= 0) dg::fail(DG_INVALID_INPUT, "pinned allocation size must be positive");
+        check_device(device);
+        DeviceScope scope(device);
+        void *p = nullptr;
+        const cudaError_t e = cudaHostAlloc(&p, size_t(bytes), cudaHostAllocPortable);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            dg::fail(DG_DEVICE, "pinned host allocation of " + std::to_string(bytes) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+        }
+        *out = p;
+    });
+}
+
+dg_status dg_host_free(void *ptr) {
+    return guarded([&] {
+        if (ptr) DG_CUDA(cudaFreeHost(ptr));
+    });
+}
+
+int32_t dg_host_is_pinned(const void *ptr) {
+    if (!ptr) return 0;
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeHost ? 1 : 0;
 }
 
 dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,

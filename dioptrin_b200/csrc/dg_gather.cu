@@ -1048,7 +1048,7 @@ __global__ void k_finalize_raw(const double *__restrict__ partial,
 __global__ void k_pack_raw(const int64_t *__restrict__ row_ptr, int n_rows,
                            const int32_t *__restrict__ col, const double *__restrict__ w,
                            const double *__restrict__ norm, float4 *__restrict__ entry_raw,
-                           double *__restrict__ cnt) {
+                           double *__restrict__ cnt, int flip_rows, int flip_cols) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
     double sum = 0.0;
@@ -1056,7 +1056,13 @@ __global__ void k_pack_raw(const int64_t *__restrict__ row_ptr, int n_rows,
         const int32_t j = col[k];
         const double c = w[k];
         sum += c;
-        entry_raw[k] = make_float4(__int_as_float(j), __double2float_rn(c),
+        // the frame's pixel (rows flipped for InputOrder::FlipVertical)
+        int32_t jf = j;
+        if (flip_rows) {
+            const int32_t rr = j / flip_cols;
+            jf = (flip_rows - 1 - rr) * flip_cols + (j - rr * flip_cols);
+        }
+        entry_raw[k] = make_float4(__int_as_float(jf), __double2float_rn(c),
                                    __double2float_rn(c * norm[j]), 0.f);
     }
     cnt[r] = sum;
@@ -1457,6 +1463,45 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
     }
 }
 
+namespace {
+
+// Row flip of a pixel index for frames stored bottom row first.
+__device__ __forceinline__ int32_t flip_px(int32_t j, int rows, int cols) {
+    const int32_t r = j / cols, c = j - r * cols;
+    return (rows - 1 - r) * cols + c;
+}
+
+// InputOrder::FlipVertical: every pixel index the gathers load through,
+// remapped in place (entry order, and so every sum, unchanged). Pixel-list
+// slots past a unit's pixel count hold no index and may hold anything; values
+// outside the frame are left alone.
+__global__ void k_flip_rows(int2 *__restrict__ entry, float4 *__restrict__ entry_std, int64_t nnz,
+                            int32_t *__restrict__ px, int64_t n_px, int rows, int cols) {
+    const int64_t npix = int64_t(rows) * cols;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nnz + n_px;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        if (i < nnz) {
+            entry[i].x = flip_px(entry[i].x, rows, cols);
+            entry_std[i].x = __int_as_float(flip_px(__float_as_int(entry_std[i].x), rows, cols));
+        } else {
+            const int32_t v = px[i - nnz];
+            if (v >= 0 && v < npix) px[i - nnz] = flip_px(v, rows, cols);
+        }
+    }
+}
+
+}  // namespace
+
+void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s) {
+    t.flip_rows = dim1;
+    t.flip_cols = dim2;
+    const int64_t n_px = t.fl_px.ptr ? int64_t(t.fl_px.count) : 0;
+    if (t.nnz + n_px == 0) return;
+    k_flip_rows<<<148 * 8, 256, 0, s>>>(t.entry.ptr, t.entry_std.ptr, t.nnz, t.fl_px.ptr, n_px,
+                                        dim1, dim2);
+    DG_CUDA(cudaGetLastError());
+}
+
 void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s) {
     if (t.cnt.ptr) return;
     t.entry_raw.alloc(std::max<size_t>(size_t(table.nnz), 1));
@@ -1464,7 +1509,7 @@ void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, c
     if (table.n_rows > 0)
         k_pack_raw<<<unsigned((table.n_rows + 127) / 128), 128, 0, s>>>(
             table.row_ptr.ptr, int(table.n_rows), table.col.ptr, table.w.ptr, d_norm,
-            t.entry_raw.ptr, t.cnt.ptr);
+            t.entry_raw.ptr, t.cnt.ptr, t.flip_rows, t.flip_cols);
     DG_CUDA(cudaGetLastError());
 }
 

@@ -187,6 +187,7 @@ struct GatherTable {
     DeviceArray<float4> entry_raw;
     DeviceArray<double> cnt;
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
+    int32_t flip_rows = 0, flip_cols = 0;  // frames stored bottom row first (0: detector order)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
     bool profile = false;
     EventPool events;
@@ -211,6 +212,9 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
 // else over the table; raw: o0..o3 = signal, norm, variance (DG_ERRORS),
 // count; otherwise o0, o1 = intensity and sigma (DG_ERRORS) normalised by
 // the frame's own denominators (needs d_masks).
+// InputOrder::FlipVertical: remaps the pixel indices of a built gather table
+// to frames whose rows come in reverse order (entry order unchanged).
+void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s);
 void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s);
 void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                     int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride, uint32_t flags,

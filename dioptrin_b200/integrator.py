@@ -192,6 +192,44 @@ def bslz4_compress(frame: np.ndarray, block_bytes: int = 0) -> bytes:
     return out[:n.value].tobytes()
 
 
+class _PinnedHost:
+    """Page-locked host memory from dg_host_alloc, freed with its last view."""
+
+    def __init__(self, device: int, nbytes: int):
+        p = C.c_void_p()
+        N.check(N.lib().dg_host_alloc(int(device), int(nbytes), C.byref(p)))
+        self.ptr, self.nbytes = p.value, int(nbytes)
+
+    def __del__(self):
+        ptr, self.ptr = getattr(self, "ptr", None), None
+        if ptr:
+            try:
+                N.lib().dg_host_free(C.c_void_p(ptr))
+            except Exception:
+                pass
+
+
+def alloc_pinned(shape, dtype, device: int = 0) -> np.ndarray:
+    """A writable NumPy array in page-locked host memory: host-memory calls
+    copy from it by DMA, without the driver's staging copy."""
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape)) * dt.itemsize
+    owner = _PinnedHost(device, max(n, 1))
+    buf = (C.c_uint8 * max(n, 1)).from_address(owner.ptr)
+    buf._owner = owner
+    return np.frombuffer(buf, np.uint8)[:n].view(dt).reshape(shape)
+
+
+def is_pinned(a) -> bool:
+    """Whether an array's memory is page-locked (is_pinned_host,
+    src/integration/cuda/device.rs:1055-1078)."""
+    ptr = a.ctypes.data if isinstance(a, np.ndarray) else int(a)
+    return bool(N.lib().dg_host_is_pinned(C.c_void_p(ptr)))
+
+
+_INPUT_ORDERS = {"detector": 0, "flip_vertical": 1}
+
+
 class Cuda1dPlan:
     """A fixed-mask table resident in HBM (src/integration/cuda.rs:374-618).
 
@@ -409,6 +447,19 @@ class Cuda1dPlan:
     def integrate1d_raw(self, image, *, with_variance: bool = False,
                         mask=None) -> IntermediateResult1d:
         return self.integrate_raw_stack(_frame_array(image), mask, with_variance)[0]
+
+    def alloc_pinned_batch(self, n_frames: int, dtype=None) -> np.ndarray:
+        """Python Cuda1dPlan.alloc_pinned_batch (src/python/cuda.rs:808-870): a
+        writable (n_frames, dim1, dim2) array in page-locked host memory
+        (float32 unless dtype is given) for readers to decode into; integrating
+        from it copies by DMA."""
+        dt = np.dtype("float32" if dtype is None else dtype)
+        if dt not in _DTYPES:
+            raise TypeError(f"dtype must be native uint16, uint32, int32, float32 or float64, "
+                            f"got {dt}")
+        if n_frames < 0:
+            raise ValueError("n_frames must not be negative")
+        return alloc_pinned((int(n_frames),) + self.shape, dt, self.device)
 
     def integrate1d(self, image: np.ndarray, *, errors: bool = False,
                     azimuthal_std: bool = False) -> IntegrationResult:
@@ -724,7 +775,10 @@ class Integrator:
 
     # -- plans --
     def _method_struct(self, precision: str, device: int, max_batch_bytes: int,
-                       keep_tables: bool) -> N.Method:
+                       keep_tables: bool, input_order: str = "detector") -> N.Method:
+        if input_order not in _INPUT_ORDERS:
+            raise ValueError(f"input_order must be 'detector' or 'flip_vertical', got "
+                             f"{input_order!r}")
         m = N.Method()
         m.kind = N.METHODS[self._method]
         m.n_ss = self._n_ss
@@ -737,14 +791,17 @@ class Integrator:
         m.precision = N.PRECISIONS[precision]
         m.device = device
         m.max_batch_bytes = max_batch_bytes
-        m.flags = N.DG_PLAN_KEEP_TABLES if keep_tables else 0
+        m.flags = (N.DG_PLAN_KEEP_TABLES if keep_tables else 0) | (
+            N.DG_PLAN_FLIP_VERTICAL if input_order == "flip_vertical" else 0)
         return m
 
     def prepare_cuda1d(self, shape, n_points: int, *, precision: str = "f32_compensated",
                        device: int = 0, max_batch_bytes: Optional[int] = None,
-                       keep_tables: bool = False) -> Cuda1dPlan:
+                       keep_tables: bool = False, input_order: str = "detector") -> Cuda1dPlan:
         """Integrator::prepare_cuda1d (src/integration/cuda.rs:1089): the
-        table is built on the device and kept there."""
+        table is built on the device and kept there. input_order
+        "flip_vertical" takes frames bottom row first
+        (Cuda1dOptions::with_input_order, cuda.rs:174-182)."""
         if precision not in N.PRECISIONS:
             raise ValueError(f"unknown CUDA precision {precision!r}")
         if device < 0:
@@ -755,7 +812,8 @@ class Integrator:
         if self._mask is not None and self._mask.shape != (dim1, dim2):
             raise ValueError(f"image shape ({dim1}, {dim2}) does not match mask shape "
                              f"{self._mask.shape}")
-        m = self._method_struct(precision, device, max_batch_bytes or 0, keep_tables)
+        m = self._method_struct(precision, device, max_batch_bytes or 0, keep_tables,
+                                input_order)
         h = C.c_void_p()
         mask = (None if self._mask is None
                 else self._mask.ctypes.data_as(C.POINTER(C.c_uint8)))
@@ -767,7 +825,7 @@ class Integrator:
                        azimuthal_range=None, azimuthal_bracket: Optional[float] = None,
                        precision: str = "f32_compensated", device: int = 0,
                        max_batch_bytes: Optional[int] = None,
-                       keep_tables: bool = False) -> Cuda2dPlan:
+                       keep_tables: bool = False, input_order: str = "detector") -> Cuda2dPlan:
         """Integrator::prepare_cuda2d (src/integration/cuda.rs:1111-1157): the
         2D table on the shared grid of the method (default or explicit radial
         and azimuthal edges) is built on the device and kept there."""
@@ -791,7 +849,8 @@ class Integrator:
         if self._mask is not None and self._mask.shape != (dim1, dim2):
             raise ValueError(f"image shape ({dim1}, {dim2}) does not match mask shape "
                              f"{self._mask.shape}")
-        m = self._method_struct(precision, device, max_batch_bytes or 0, keep_tables)
+        m = self._method_struct(precision, device, max_batch_bytes or 0, keep_tables,
+                                input_order)
         h = C.c_void_p()
         mask = (None if self._mask is None
                 else self._mask.ctypes.data_as(C.POINTER(C.c_uint8)))
@@ -828,8 +887,8 @@ class Integrator:
         return self.integrate2d(image, n_radial, n_azimuthal, errors, azimuthal_range)
 
     def prepare_dynamic1d(self, shape, n_points: int, *, precision: str = "f32_compensated",
-                          device: int = 0, max_batch_bytes: Optional[int] = None
-                          ) -> "Dynamic1dPlan":
+                          device: int = 0, max_batch_bytes: Optional[int] = None,
+                          input_order: str = "detector") -> "Dynamic1dPlan":
         """Integrator::prepare_dynamic1d (src/integration/dynamic.rs:29-65): one
         geometry table without the stored mask, for frames that each bring
         their complete mask. Built and kept on the device."""
@@ -837,7 +896,7 @@ class Integrator:
         self._mask = None
         try:
             plan = self.prepare_cuda1d(shape, n_points, precision=precision, device=device,
-                                       max_batch_bytes=max_batch_bytes)
+                                       max_batch_bytes=max_batch_bytes, input_order=input_order)
         finally:
             self._mask = saved
         return Dynamic1dPlan(plan)

@@ -62,6 +62,14 @@ enum { DG_PRECISION_F32 = 0, DG_PRECISION_F32_COMPENSATED = 1, DG_PRECISION_F64 
 
 /* Plan-creation flags. */
 #define DG_PLAN_KEEP_TABLES 1u /* keep the unmasked f64 CSR for dg_plan_export_table */
+/* InputOrder::FlipVertical (src/integration/fixed.rs:18-23, applied to the
+ * uploaded columns as in src/integration/cuda/device.rs:506-528): frames
+ * arrive bottom row first (top-to-bottom raw HDF5 frames); the plan's pixel
+ * indices are remapped once at creation, so results equal those of the
+ * row-flipped frames in detector order, bit for bit. Per-frame masks follow
+ * the frames' order; the plan mask, exported tables and radial axes stay in
+ * detector order. */
+#define DG_PLAN_FLIP_VERTICAL 2u
 
 /* Poni (src/poni.rs:13-24); SI units, angles in radians. */
 typedef struct dg_geometry {
@@ -202,6 +210,17 @@ DG_EXPORT dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_
                                      int32_t *variant, double *ms, int32_t n_ms);
 DG_EXPORT dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current,
                                     int32_t *count);
+
+/* Page-locked host buffers for frames. Replaces Cuda1dPlan's pinned staging
+ * (alloc_pinned_batch, src/python/cuda.rs:808-870; is_pinned_host,
+ * src/integration/cuda/device.rs:1055-1078): a reader decodes straight into
+ * the buffer and the host-memory calls copy from it by DMA, asynchronously.
+ * dg_host_alloc makes `bytes` of pinned memory usable from every device
+ * (allocated while `device` is current); dg_host_free releases it;
+ * dg_host_is_pinned is 1 for page-locked host memory, else 0 (any pointer). */
+DG_EXPORT dg_status dg_host_alloc(int32_t device, int64_t bytes, void **out);
+DG_EXPORT dg_status dg_host_free(void *ptr);
+DG_EXPORT int32_t dg_host_is_pinned(const void *ptr);
 
 /* Per-frame masks (MaskMode::Dynamic). Replaces Dynamic1dPlan::integrate
  * (src/integration/dynamic.rs:159-196; the per-row sums with a mask check,

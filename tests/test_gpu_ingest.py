@@ -1,0 +1,118 @@
+"""Host-side ingestion around the gather: frames stored bottom row first
+(InputOrder::FlipVertical, src/integration/fixed.rs:18-23; remapped columns,
+src/integration/cuda/device.rs:506-528) and page-locked frame buffers
+(alloc_pinned_batch, src/python/cuda.rs:808-870; is_pinned_host,
+device.rs:1055-1078).
+
+A FlipVertical plan remaps pixel indices only, so on row-flipped frames it
+must reproduce the detector-order plan bit for bit, for every lane mapping,
+Bitshuffle/LZ4 chunks, per-frame masks and raw sums."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (53, 61)
+PONI = dict(pixel1=172e-6, pixel2=172e-6, distance=0.05, poni1=15.3 * 172e-6,
+            poni2=40.7 * 172e-6, rot1=0.03, rot2=-0.01, rot3=0.02, wavelength=1e-10)
+
+
+@pytest.fixture(scope="module")
+def dg():
+    import dioptrin_b200 as d
+    if not d.cuda_available():
+        pytest.fail("CUDA device required for -m gpu tests: " + str(d.cuda_info()))
+    return d
+
+
+def _integrator(dg, mask=True):
+    it = dg.Integrator.from_poni_dict(PONI, method="pixel_split", polarization_factor=0.97)
+    if mask:
+        m = np.zeros(SHAPE, np.uint8)
+        m[3, :] = 1       # near the top: must follow the flip
+        m[:, 17] = 1
+        it.set_mask(m)
+    return it
+
+
+def _eq(a, b):
+    for x, y in zip(a, b):
+        assert (x is None) == (y is None)
+        if x is not None:
+            assert np.array_equal(x, y, equal_nan=True)
+
+
+def _count(plan):
+    import ctypes as C
+    from dioptrin_b200 import _native as N
+    cnt = C.c_int32(0)
+    N.check(N.lib().dg_plan_variant(plan.handle, -1, None, C.byref(cnt)))
+    return cnt.value
+
+
+def test_flip_vertical_is_bit_exact_for_every_mapping(dg):
+    it = _integrator(dg)
+    det = it.prepare_cuda1d(SHAPE, 70)
+    flip = it.prepare_cuda1d(SHAPE, 70, input_order="flip_vertical")
+    assert np.array_equal(det.radial_array, flip.radial_array)
+    frames = np.random.default_rng(1).poisson(40.0, (5,) + SHAPE).astype(np.float32)
+    frames[2, 5, 9] = np.nan
+    flipped = np.ascontiguousarray(frames[:, ::-1, :])
+    for v in range(_count(det)):
+        det.gather_variant = v
+        flip.gather_variant = v
+        for flags in [(False, False), (True, False), (True, True)]:
+            _eq(flip.integrate_stack(flipped, *flags), det.integrate_stack(frames, *flags))
+    det.close()
+    flip.close()
+
+
+def test_flip_vertical_bslz4_dynamic_raw_and_2d(dg):
+    it = _integrator(dg)
+    det = it.prepare_cuda1d(SHAPE, 70)
+    flip = it.prepare_cuda1d(SHAPE, 70, input_order="flip_vertical")
+    frames = np.random.default_rng(2).poisson(30.0, (4,) + SHAPE).astype(np.uint32)
+    flipped = np.ascontiguousarray(frames[:, ::-1, :])
+    # Bitshuffle/LZ4 chunks of the stored (flipped) frames
+    _eq(flip.integrate_bslz4_stack([dg.bslz4_compress(f) for f in flipped], "uint32", True),
+        det.integrate_bslz4_stack([dg.bslz4_compress(f) for f in frames], "uint32", True))
+    # raw sums with the plan mask
+    for a, b in zip(flip.integrate_raw_stack(flipped, with_variance=True),
+                    det.integrate_raw_stack(frames, with_variance=True)):
+        _eq((a.sum_signal, a.sum_norm, a.sum_variance, a.count),
+            (b.sum_signal, b.sum_norm, b.sum_variance, b.count))
+    # per-frame masks travel with the frames
+    masks = (np.random.default_rng(3).random((4,) + SHAPE) < 0.1).astype(np.uint8)
+    fm = np.ascontiguousarray(masks[:, ::-1, :])
+    ddet = _integrator(dg, mask=False).prepare_dynamic1d(SHAPE, 70)
+    dflip = _integrator(dg, mask=False).prepare_dynamic1d(SHAPE, 70, input_order="flip_vertical")
+    _eq(dflip.cuda_plan.integrate_dynamic_stack(flipped, fm, True),
+        ddet.cuda_plan.integrate_dynamic_stack(frames, masks, True))
+    # 2D
+    d2 = it.prepare_cuda2d(SHAPE, 24, 16)
+    f2 = it.prepare_cuda2d(SHAPE, 24, 16, input_order="flip_vertical")
+    _eq(f2.integrate_stack(flipped, True), d2.integrate_stack(frames, True))
+    with pytest.raises(ValueError):
+        it.prepare_cuda1d(SHAPE, 70, input_order="upside_down")
+    for p in (det, flip, d2, f2):
+        p.close()
+    ddet.close()
+    dflip.close()
+
+
+@pytest.mark.parametrize("dtype", [None, "uint16", "int32", "float64"])
+def test_pinned_batches(dg, dtype):
+    plan = _integrator(dg).prepare_cuda1d(SHAPE, 70)
+    buf = plan.alloc_pinned_batch(6, dtype)
+    assert buf.shape == (6,) + SHAPE and buf.flags.writeable
+    assert buf.dtype == np.dtype(dtype or "float32")
+    assert dg.is_pinned(buf) and not dg.is_pinned(np.empty(10))
+    src = np.random.default_rng(4).poisson(25.0, (6,) + SHAPE).astype(buf.dtype)
+    buf[:] = src
+    _eq(plan.integrate_stack(buf, True, True), plan.integrate_stack(src.copy(), True, True))
+    res = plan.batch1d(buf, errors=True)
+    assert np.array_equal(res[3].intensity_array, plan.integrate_stack(src, True)[0][3])
+    with pytest.raises(TypeError):
+        plan.alloc_pinned_batch(2, "int8")
+    del buf
+    plan.close()

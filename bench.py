@@ -331,6 +331,72 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def masked_legs(w, plan, frames, stream, peak, reps: int = 3) -> dict:
+    """Device-resident frames through the per-frame-mask gather
+    (dg_integrate_dynamic_device: a uint8 mask per frame, denominators summed
+    per frame, I and sigma) and the raw-sum path with the plan's mask
+    (dg_integrate_raw_device: signal, norm, variance, count). Frames/s and
+    the gather kernel's event-timed HBM roofline: per launch, the entries
+    (16 B {pixel, w, w*norm} for the masked gather, the plan's own table
+    bytes otherwise), frames, masks and four FP64 partial sums per segment."""
+    import numpy as np
+    import torch
+    from dioptrin_b200 import _native as N
+    L = N.lib()
+    n, npix = frames.shape[0], frames[0].numel()
+    nb = w.n_points * max(1, w.n_azimuthal)
+    gen = torch.Generator(device=frames.device)
+    gen.manual_seed(w.seed + 7)
+    masks = (torch.rand((n,) + w.shape, generator=gen, device=frames.device) < 0.02)
+    masks = masks.to(torch.uint8)
+    masks |= torch.from_numpy(w.mask()).to(frames.device)[None]
+    outs = [torch.empty((n, nb), dtype=torch.float64, device=frames.device) for _ in range(4)]
+    code = {"uint16": 0, "uint32": 1, "int32": 2, "float32": 3, "float64": 4}[w.dtype]
+    sp = C.c_void_p(stream.cuda_stream)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    info = plan.info()
+
+    def dynamic():
+        N.check(L.dg_integrate_dynamic_device(plan.handle, ptr(frames), code, n, ptr(masks), npix,
+                                              N.DG_ERRORS, ptr(outs[0]), ptr(outs[1]), sp))
+
+    def raw():
+        N.check(L.dg_integrate_raw_device(plan.handle, ptr(frames), code, n, None, 0, N.DG_ERRORS,
+                                          ptr(outs[0]), ptr(outs[1]), ptr(outs[2]), ptr(outs[3]),
+                                          sp))
+
+    res = {}
+    for name, fn, table_bytes, extra in (
+            ("dynamic_masks", dynamic, info.table_entries * 16, n * npix),
+            ("raw_sums", raw, None, 0)):
+        fn()
+        torch.cuda.synchronize()
+        N.check(L.dg_plan_profile(plan.handle, 1))
+        N.check(L.dg_plan_kernel_time(plan.handle, 1, None, None, None))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        gms, gl, launches = C.c_double(), C.c_int64(), C.c_int64()
+        N.check(L.dg_plan_kernel_time(plan.handle, 1, C.byref(gms), C.byref(gl),
+                                      C.byref(launches)))
+        N.check(L.dg_plan_profile(plan.handle, 0))
+        if table_bytes is None:
+            table_bytes = info.table_entries * 8 + (nb + 1) * 4 + nb * 8
+        alg = table_bytes + n * npix * frames.element_size() + extra + n * nb * 4 * 8
+        per = gms.value / 1000.0 / max(1, gl.value)
+        res[name] = {"value": round(n * reps / (e0.elapsed_time(e1) / 1000.0), 2),
+                     "unit": "frames/s", "frames": n,
+                     "kernel_ms_per_launch": round(per * 1000, 4),
+                     "alg_bytes_per_launch": int(alg),
+                     "achieved": round(alg / per / 1e9, 1), "unit_roofline": "GB/s",
+                     "frac": round(alg / per / 1e9 / peak, 4)}
+    res["dynamic_masks"]["masks"] = "uint8 per frame: the plan mask plus 2% random pixels"
+    return res
+
+
 def bslz4_leg(w, plan, frames, n_frames, flags, hi, hs, hd, peak, distinct: int = 16):
     """Frames/s through dg_integrate_bslz4: raw HDF5 Bitshuffle/LZ4 chunks in
     pinned HOST memory (the first `distinct` frames compressed by the
@@ -547,6 +613,8 @@ def main():
                          "unit": "frames/s", "frames": nplain * reps,
                          "gather_variant": plan.gather_variant}
         plan.gather_variant = batch_variant
+        if not w.n_azimuthal:
+            line.update(masked_legs(w, plan, frames, stream, peak))
         # end to end through the public host API: pinned host frames in,
         # results back, every step
         host = torch.empty(frames.shape, dtype=frames.dtype, pin_memory=True)

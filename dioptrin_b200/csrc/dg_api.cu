@@ -183,7 +183,8 @@ int64_t dg_plan::device_bytes() const {
          gather.valid_std.bytes() + gather.partial.bytes() + gather.fl_unit.bytes() +
          gather.fl_px.bytes() + gather.fl_pair_a.bytes() + gather.fl_pair_b.bytes() +
          gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes() + gather.entry_raw.bytes() +
-         gather.cnt.bytes();
+         gather.cnt.bytes() + gather.bt_item.bytes() + gather.bt_meta.bytes() + gather.bt_org.bytes() +
+         gather.bt_pair_a.bytes() + gather.bt_pair_as.bytes() + gather.bt_pair_b.bytes();
     b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes() +
          stage_mask.bytes();
     return b;

@@ -37,6 +37,11 @@
 #include <climits>
 #include <type_traits>
 
+#include <array>
+#include <atomic>
+#include <memory>
+#include <thread>
+
 #include "dg_internal.h"
 
 namespace dg {
@@ -49,8 +54,9 @@ constexpr int kFlush = 16;  // terms per lane between double-word folds
 // mappings, as (entry slices per frame group, frames per lane, entries per
 // lane per step): 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2);
 // frame-lane mappings (k_gather_fl), 2 CTAs per SM (5) or 1 CTA per SM with
-// the next frames prefetched while the current ones are summed (6).
-constexpr int kVariantCount = 7;
+// the next frames prefetched while the current ones are summed (6); bin
+// tiles (k_gather_bins, 7), which write the results themselves.
+constexpr int kVariantCount = 8;
 constexpr int kSegMax = 256;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
@@ -947,6 +953,318 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Bin-tile gather (mapping 7). A tile is kBtRows consecutive rows (bins) of the
+// table and 32 frames (lane = frame). The tile's entries, merged over its rows
+// in pixel order, are cut into chunks of at most kBtDCap distinct pixels and
+// kBtPCap entry pairs; a row's entries inside a chunk are a contiguous run of
+// its CSR row. The CTA walks the tile's chunks in order with three buffers:
+// while chunk k is summed, chunk k+2's pixels (4-byte cp.async into frame rows
+// kBtStride words apart) and entry pairs (16-byte cp.async) are in flight;
+// one barrier per chunk. Warp w owns row w of the tile and keeps its sums in
+// registers for the whole tile (double-word FP32, folded
+// every kFlFlushPairs pairs of the row), then normalises and writes the
+// results itself: no partial sums, no finalize launch. Every row is summed in
+// the same order for every frame and batch.
+
+#ifndef DG_BT_ROWS
+#define DG_BT_ROWS 24
+#endif
+constexpr int kBtRows = DG_BT_ROWS;      // rows per tile
+constexpr int kBtWarps = kBtRows;        // warps per CTA; warp w owns row w
+constexpr int kBtDCap = 384;             // distinct pixels per chunk
+constexpr int kBtStride = kBtDCap + 1;   // odd frame-row stride; column kBtDCap stays 0
+constexpr int kBtPCap = 640;             // entry pairs per chunk
+constexpr int kBtBufs = 3;
+// Per-chunk record, fixed size: {pixels D, pairs, first pair, 0}, the rows'
+// pair offsets (kBtRows + 1, padded to a multiple of 4 words), then D pixel
+// indices.
+constexpr int kBtMetaHead = (4 + kBtRows + 1 + 3) / 4 * 4;
+constexpr int kBtMetaWords = kBtMetaHead + kBtDCap;  // 408 words, 1632 bytes
+constexpr int kBtMetaBufs = 5;
+static_assert(kBtMetaWords % 4 == 0, "records are copied in 16-byte pieces");
+static_assert(kBtRows + 1 <= kBtMetaHead - 4, "row offsets fit the record head");
+static_assert(kBtRows <= 32, "tile rows are packed in 5 bits at plan time");
+static_assert(kBtRows == kBtWarps, "a warp owns one row of a tile");
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+template <int MODE, typename P>
+constexpr size_t bt_buf_bytes() {
+    return size_t(32) * kBtStride * 4 + size_t(kBtPCap) * (MODE == kSpread ? 32 : 16);
+}
+
+template <int MODE, typename P, int U2>
+__global__ void __launch_bounds__(kBtWarps * 32, 1)
+    k_gather_bins(const int4 *__restrict__ items, const int32_t *__restrict__ meta,
+                  const float4 *__restrict__ pair_a, const float4 *__restrict__ pair_b,
+                  const int4 *__restrict__ org, const float4 *__restrict__ entry_std,
+                  const double *__restrict__ den, const double *__restrict__ den_std,
+                  const double *__restrict__ den_f32, const int32_t *__restrict__ valid_std,
+                  const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_rows,
+                  double *__restrict__ out_i, double *__restrict__ out_s,
+                  double *__restrict__ out_d) {
+    using S = StagedPx<P>;
+    constexpr int NA = NAcc<MODE, P>::value;
+    constexpr bool SPREAD = MODE == kSpread;
+    constexpr size_t BUF = bt_buf_bytes<MODE, P>();
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int groups = (n_frames + 31) / 32;
+    const int4 it = items[blockIdx.x / groups];
+    const int f0 = (blockIdx.x % groups) * 32, nv = min(32, n_frames - f0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int row0 = it.x, nrows = it.y, ch0 = it.z, nch = it.w;
+
+    auto pxbuf = [&](int b) { return reinterpret_cast<S *>(smem + size_t(b) * BUF); };
+    auto pabuf = [&](int b) {
+        return reinterpret_cast<float4 *>(smem + size_t(b) * BUF + size_t(32) * kBtStride * 4);
+    };
+    auto mbuf = [&](int c) {
+        return reinterpret_cast<int32_t *>(smem + size_t(kBtBufs) * BUF) +
+               (c % kBtMetaBufs) * kBtMetaWords;
+    };
+    // Copy chunk c's record into its record buffer (part of the open group).
+    auto stage_meta = [&](int c) {
+        if (c < nch) {
+            const int4 *src = reinterpret_cast<const int4 *>(meta + int64_t(ch0 + c) * kBtMetaWords);
+            int4 *dst = reinterpret_cast<int4 *>(mbuf(c));
+            for (int j = tid; j < kBtMetaWords / 4; j += kBtWarps * 32) cp_async16(dst + j, src + j);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    // Column kBtDCap of every frame row is read by padding pairs and holds 0.
+    for (int j = tid; j < kBtBufs * 32; j += kBtWarps * 32)
+        pxbuf(j / 32)[(j % 32) * kBtStride + kBtDCap] = S(0);
+
+    // Stage chunk c (of this tile) into buffer b as one commit group; its
+    // record is in shared memory already.
+    auto stage = [&](int c, int b) {
+        if (c < nch) {
+            const int32_t *mb = mbuf(c);
+            const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
+            S *dst = pxbuf(b);
+            const P *base = frames + int64_t(f0) * n_pixels;
+            for (int k = tid; k < ch.y; k += kBtWarps * 32) {
+                const P *src = base + mb[kBtMetaHead + k];
+                if constexpr (sizeof(P) == 4) {
+#pragma unroll 8
+                    for (int f = 0; f < nv; ++f)
+                        cp_async4(dst + f * kBtStride + k, src + int64_t(f) * n_pixels);
+                } else {
+#pragma unroll 8
+                    for (int f = 0; f < nv; ++f)
+                        dst[f * kBtStride + k] = load_px<P>(src + int64_t(f) * n_pixels, 0u);
+                }
+            }
+            float4 *pa = pabuf(b);
+            for (int j = tid; j < ch.w; j += kBtWarps * 32) {
+                cp_async16(pa + j, pair_a + ch.z + j);
+                if (SPREAD) cp_async16(pa + kBtPCap + j, pair_b + ch.z + j);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+
+    // This warp's row: accumulators, fold counter, origin.
+    Acc2 acc0[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) acc0[a].zero();
+    int since0 = 0;
+    float org0 = 0.f;
+    const int ra = warp;  // row of the tile
+    const int4 oa = ra < nrows ? org[row0 + ra] : make_int4(-1, 0, -1, 0);
+
+    // Pipeline: records two chunks ahead of their pixels, pixels two chunks
+    // ahead of their sums; commit order M0 M1 | P0 M2 P1 M3 | P2 M4 | P3 M5 ...
+    stage_meta(0);
+    stage_meta(1);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    stage(0, 0);
+    stage_meta(2);
+    stage(1, 1);
+    stage_meta(3);
+    for (int c = 0; c < nch; ++c) {
+        // complete: P(c) and M(c+2); pending: P(c+1), M(c+3)
+        asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+        __syncthreads();
+        stage(c + 2, (c + 2) % kBtBufs);
+        stage_meta(c + 4);
+        const int b = c % kBtBufs;
+        const S *px = pxbuf(b) + lane * kBtStride;
+        const float4 *s_pa = pabuf(b);
+        const float4 *s_pb = s_pa + kBtPCap;
+        const int32_t *cp = mbuf(c) + 4;
+
+        auto run_row = [&](int r, const int4 &o, Acc2 *acc, int &since, float &orgv) {
+            if (r >= nrows) return;
+            if constexpr (SPREAD) {
+                if (o.x == c) {
+                    // Origin o = s/n of the row's first valid entry (row_origin):
+                    // its pixel is in this chunk; a non-finite float pixel there
+                    // sends the lane to the row's next entries in global memory.
+                    const float so = float(px[o.y]);
+                    orgv = __fdiv_rn(so, entry_std[o.z].z);
+                    if (is_float_px<P>() && !isfinite(so)) {
+                        const int fi = min(f0 + lane, n_frames - 1);
+                        orgv = row_origin<P>(entry_std, o.z, o.w, frames + int64_t(fi) * n_pixels);
+                    }
+                }
+            }
+            const f2 norg = pk(-orgv, -orgv);
+            const int p0 = cp[r], p1 = cp[r + 1];
+            auto body = [&](int p, auto unroll) {
+                constexpr int UU = decltype(unroll)::value;
+                float4 ea[UU], eb[UU];
+#pragma unroll
+                for (int u = 0; u < UU; ++u) {
+                    ea[u] = s_pa[p + u];
+                    if constexpr (SPREAD) eb[u] = s_pb[p + u];
+                }
+                float v0[UU], v1[UU];
+#pragma unroll
+                for (int u = 0; u < UU; ++u) {
+                    v0[u] = float(px[__float_as_int(ea[u].x)]);
+                    v1[u] = float(px[__float_as_int(ea[u].y)]);
+                }
+#pragma unroll
+                for (int u = 0; u < UU; ++u) {
+                    const f2 cc = pk(ea[u].z, ea[u].w);
+                    if constexpr (SPREAD && is_float_px<P>()) {
+                        if (!(isfinite(v0[u]) && isfinite(v1[u]))) {
+                            const bool ok0 = isfinite(v0[u]), ok1 = isfinite(v1[u]);
+                            const float x0 = ok0 ? v0[u] : 0.f, x1 = ok1 ? v1[u] : 0.f;
+                            const f2 ce = pk(ok0 ? ea[u].z : 0.f, ok1 ? ea[u].w : 0.f);
+                            const f2 x = pk(x0, x1), n = pk(eb[u].x, eb[u].y);
+                            const f2 cre = pk(ok0 ? eb[u].z : 0.f, ok1 ? eb[u].w : 0.f);
+                            acc[0].p = fma2(ce, x, acc[0].p);
+                            acc[1].p = fma2(mul2(ce, ce), pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f)),
+                                            acc[1].p);
+                            const f2 t = fma2(norg, n, x);
+                            acc[2].p = fma2(mul2(cre, t), t, acc[2].p);
+                            acc[NA - 2].p = add2(acc[NA - 2].p,
+                                                 pk(ok0 ? 0.f : __fmul_rn(ea[u].z, eb[u].x),
+                                                    ok1 ? 0.f : __fmul_rn(ea[u].w, eb[u].y)));
+                            acc[NA - 1].p = add2(acc[NA - 1].p,
+                                                 pk(!ok0 && ea[u].z > 0.f ? 1.f : 0.f,
+                                                    !ok1 && ea[u].w > 0.f ? 1.f : 0.f));
+                            continue;
+                        }
+                    }
+                    const f2 x = pk(v0[u], v1[u]);
+                    acc[0].p = fma2(cc, x, acc[0].p);
+                    if constexpr (MODE != kIntensity) {
+                        const f2 xp = is_unsigned_px<P>()
+                                          ? x
+                                          : pk(fmaxf(v0[u], 0.f), fmaxf(v1[u], 0.f));
+                        acc[1].p = fma2(mul2(cc, cc), xp, acc[1].p);
+                    }
+                    if constexpr (SPREAD) {
+                        const f2 n = pk(eb[u].x, eb[u].y), cr = pk(eb[u].z, eb[u].w);
+                        const f2 t = fma2(norg, n, x);
+                        acc[2].p = fma2(mul2(cr, t), t, acc[2].p);
+                    }
+                }
+            };
+            int p = p0;
+            for (; p + U2 <= p1; p += U2) {
+                body(p, std::integral_constant<int, U2>{});
+                since += U2;
+                if (since >= kFlFlushPairs) {
+                    since = 0;
+#pragma unroll
+                    for (int a = 0; a < NA; ++a) acc[a].flush();
+                }
+            }
+            for (; p < p1; ++p) {
+                body(p, std::integral_constant<int, 1>{});
+                if (++since >= kFlFlushPairs) {
+                    since = 0;
+#pragma unroll
+                    for (int a = 0; a < NA; ++a) acc[a].flush();
+                }
+            }
+        };
+        run_row(ra, oa, acc0, since0, org0);
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+
+    // Normalise (normalize_bin, prepared.rs:985-996; the spread's closing
+    // formulas, azimuthal.rs:96-104), as k_finalize does from partial sums.
+    auto finish = [&](int rl, Acc2 *acc, float orgv) {
+        if (rl >= nrows || lane >= nv) return;
+        const int r = row0 + rl;
+        double v[NA];
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+            acc[a].flush();
+            v[a] = acc[a].value();
+        }
+        const int64_t o = int64_t(f0 + lane) * n_rows + r;
+        if constexpr (!SPREAD) {
+            const double n = den[r];
+            out_i[o] = n == 0.0 ? 0.0 : v[0] / n;
+            if (MODE == kErrors) {
+                const double q = n == 0.0 ? 0.0 : v[1] / (n * n);
+                out_s[o] = sqrt(q > 0.0 ? q : 0.0);
+            }
+        } else {
+            int valid = valid_std[r];
+            double sw = den_std[r], wf = den_f32[r];
+            if (NA == 5) {
+                valid -= int(v[NA - 1] + 0.5);
+                sw -= v[NA - 2];
+                wf -= v[NA - 2];
+            }
+            if (valid <= 0 || !(sw > 0.0)) {
+                out_i[o] = 0.0;
+                if (out_s) out_s[o] = 0.0;
+                out_d[o] = __longlong_as_double(0x7ff8000000000000ll);
+                return;
+            }
+            const double a1 = v[0] - double(orgv) * wf;
+            out_i[o] = v[0] / sw;
+            if (out_s) out_s[o] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
+            const double mean = a1 / sw;
+            const double m2 = v[2] - mean * a1;
+            const double q = m2 / sw;
+            out_d[o] = sqrt(q > 0.0 ? q : 0.0);
+        }
+    };
+    finish(ra, acc0, org0);
+}
+
+// Bin-tile entry pairs from the plan-time layout: per pair {slot 0, slot 1,
+// entry 0, entry 1} (entry -1: padding, slot kBtDCap) to A {slot 0, slot 1,
+// c0, c1} with the table's FP32 weights, AS the same with the spread's
+// weights, B {n0, n1, c0/n0, c1/n1}.
+__global__ void k_bt_fill(const int4 *__restrict__ desc, int64_t n_pairs,
+                          const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
+                          float4 *__restrict__ pair_a, float4 *__restrict__ pair_as,
+                          float4 *__restrict__ pair_b) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pairs;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int4 d = desc[i];
+        float c[2] = {0.f, 0.f}, cs[2] = {0.f, 0.f}, n[2] = {1.f, 1.f}, cr[2] = {0.f, 0.f};
+        const int k[2] = {d.z, d.w};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (k[h] < 0) continue;
+            c[h] = __int_as_float(entry[k[h]].y);
+            const float4 es = entry_std[k[h]];
+            cs[h] = es.y;
+            n[h] = es.z;
+            cr[h] = es.w;
+        }
+        pair_a[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), c[0], c[1]);
+        pair_as[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), cs[0], cs[1]);
+        pair_b[i] = make_float4(n[0], n[1], cr[0], cr[1]);
+    }
+}
+
 // One thread per (frame, row): fold the row's segment partials in strip
 // order in FP64 and normalise (normalize_bin, prepared.rs:985-996; the
 // spread's closing formulas, azimuthal.rs:96-104).
@@ -1141,17 +1459,47 @@ void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, doub
 // Launches lane-mapping variant `variant` of the gather (kVariantCount) with
 // its partial sums in `partial`.
 template <int MODE, typename P>
-void launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pixels, int nf,
+void launch_bins(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, double *oi,
+                 double *os, double *od, cudaStream_t s) {
+    constexpr size_t smem =
+        size_t(kBtBufs) * bt_buf_bytes<MODE, P>() + size_t(kBtMetaBufs) * kBtMetaWords * 4;
+    auto kern = k_gather_bins<MODE, P, (kBtRows > 24 ? 2 : 4)>;
+    DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const int groups = (nf + 31) / 32;
+    const int64_t grid = int64_t(t.bt_n_items) * groups;
+    if (grid > INT32_MAX) fail(DG_UNSUPPORTED, "too many bin tiles for one launch");
+    kern<<<unsigned(grid), kBtWarps * 32, smem, s>>>(
+        t.bt_item.ptr, t.bt_meta.ptr,
+        MODE == kSpread ? t.bt_pair_as.ptr : t.bt_pair_a.ptr, t.bt_pair_b.ptr, t.bt_org.ptr,
+        t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr, t.valid_std.ptr, fp, n_pixels,
+        nf, t.n_rows, oi, os, od);
+}
+
+// Launches lane mapping `variant`; returns true when the kernel wrote the
+// normalised results to oi/os/od itself (mapping 7), false when it left
+// partial sums for k_finalize. Mapping 7 needs the outputs; callers without
+// them (raw sums) get the frame-lane or an entry-lane mapping instead.
+template <int MODE, typename P>
+bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pixels, int nf,
                    double *partial, cudaStream_t s, const uint8_t *masks = nullptr,
-                   int64_t mask_stride = 0) {
+                   int64_t mask_stride = 0, double *oi = nullptr, double *os = nullptr,
+                   double *od = nullptr) {
     if constexpr (MODE == kRaw) {
-        if (variant == 5 || variant == 6) variant = 2;  // entry-lane mappings only
+        if (variant >= 5) variant = 2;  // entry-lane mappings only
     } else {
+        if (variant == 7) {
+            if (oi && t.bt_n_items > 0) {
+                launch_bins<MODE, P>(t, fp, n_pixels, nf, oi, os, od, s);
+                DG_CUDA(cudaGetLastError());
+                return true;
+            }
+            variant = t.fl_n_units > 0 ? 5 : 2;
+        }
         if (variant == 5 || variant == 6) {
             if (variant == 5) launch_fl<MODE, P, 4, false>(t, fp, n_pixels, nf, partial, s);
             else launch_fl<MODE, P, 4, true>(t, fp, n_pixels, nf, partial, s);
             DG_CUDA(cudaGetLastError());
-            return;
+            return false;
         }
     }
     const size_t smem = size_t(t.unit_cap) * (MODE == kSpread || MODE == kRaw ? 16 : 8);
@@ -1168,15 +1516,22 @@ void launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pix
     }
 #undef DG_GATHER_ARGS
     DG_CUDA(cudaGetLastError());
+    return false;
 }
 
 template <typename P>
-void launch_typed(GatherTable &t, const void *frames, int64_t n_pixels, int n_frames, int mode,
+bool launch_typed(const GatherTable &t, int variant, const void *frames, int64_t n_pixels,
+                  int n_frames, int mode, double *partial, double *oi, double *os, double *od,
                   cudaStream_t s) {
     const P *fp = static_cast<const P *>(frames);
-    if (mode == kSpread) launch_gather<kSpread, P>(t, t.variant, fp, n_pixels, n_frames, t.partial.ptr, s);
-    else if (mode == kErrors) launch_gather<kErrors, P>(t, t.variant, fp, n_pixels, n_frames, t.partial.ptr, s);
-    else launch_gather<kIntensity, P>(t, t.variant, fp, n_pixels, n_frames, t.partial.ptr, s);
+    if (mode == kSpread)
+        return launch_gather<kSpread, P>(t, variant, fp, n_pixels, n_frames, partial, s, nullptr,
+                                         0, oi, os, od);
+    if (mode == kErrors)
+        return launch_gather<kErrors, P>(t, variant, fp, n_pixels, n_frames, partial, s, nullptr,
+                                         0, oi, os, od);
+    return launch_gather<kIntensity, P>(t, variant, fp, n_pixels, n_frames, partial, s, nullptr,
+                                        0, oi, os, od);
 }
 
 template <int MODE, typename P>
@@ -1309,6 +1664,209 @@ void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<
     out.fl_n_units = int32_t(fl.size());
 }
 
+// Bin tiles (k_gather_bins) at plan time, on the host: for every run of
+// kBtRows rows, the rows' entries merged in pixel order and cut into chunks of
+// at most kBtDCap distinct pixels and kBtPCap pairs (a new pixel that would
+// exceed either opens the next chunk, so a chunk is a pixel-index interval
+// and each row's entries in it are a contiguous run of its CSR row). Tiles
+// are ordered largest first. Each row's origin (its first entry valid for the
+// spread) is located as {chunk within the tile, slot}.
+void build_bin_tiles(GatherTable &out, const DeviceCsr &table, const std::vector<int64_t> &rp,
+                     cudaStream_t s) {
+    const int64_t nb = table.n_rows;
+    out.bt_n_items = 0;
+    if (nb == 0 || table.nnz == 0) return;
+    std::vector<int32_t> col(static_cast<size_t>(table.nnz)), fv(static_cast<size_t>(nb));
+    DG_CUDA(cudaMemcpyAsync(col.data(), table.col.ptr, col.size() * 4, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaMemcpyAsync(fv.data(), out.first_valid.ptr, fv.size() * 4, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
+    const int64_t n_items = (nb + kBtRows - 1) / kBtRows;
+    struct Tile {
+        std::vector<int4> chunks;      // {px offset, D, pair offset, pairs} (tile-relative)
+        std::vector<int32_t> cpair;    // per chunk kBtRows + 1
+        std::vector<int32_t> px;
+        std::vector<int4> pairs;       // {slot0, slot1, entry0, entry1}
+        std::vector<int4> org;         // per row
+        int64_t entries = 0;
+    };
+    std::vector<Tile> tiles(static_cast<size_t>(n_items));
+    auto build = [&](int64_t ti) {
+        Tile &T = tiles[size_t(ti)];
+        const int64_t r0 = ti * kBtRows, r1 = std::min<int64_t>(nb, r0 + kBtRows);
+        const int nr = int(r1 - r0);
+        // Entries merged in pixel order, rows ascending within a pixel: keys
+        // pixel << 32 | row << 27 | position in row; each row is sorted
+        // already, so four rounds of pairwise merges order the tile.
+        const int64_t n_e = rp[size_t(r1)] - rp[size_t(r0)];
+        std::vector<uint64_t> ka(static_cast<size_t>(n_e)), kb(static_cast<size_t>(n_e));
+        std::vector<int64_t> bounds(static_cast<size_t>(kBtRows) + 1, 0);
+        for (int j = 0; j < nr; ++j) {
+            const int64_t b = rp[size_t(r0 + j)], e = rp[size_t(r0 + j) + 1];
+            if (e - b >= (int64_t(1) << 27)) fail(DG_UNSUPPORTED, "a bin too large for bin tiles");
+            uint64_t *o = ka.data() + (b - rp[size_t(r0)]);
+            for (int64_t k = b; k < e; ++k)
+                o[k - b] = (uint64_t(uint32_t(col[size_t(k)])) << 32) | (uint64_t(j) << 27) |
+                           uint64_t(k - b);
+            bounds[size_t(j) + 1] = e - rp[size_t(r0)];
+        }
+        for (int j = nr; j < kBtRows; ++j) bounds[size_t(j) + 1] = n_e;
+        for (int width = 1; width < kBtRows; width *= 2) {
+            for (int j = 0; j < kBtRows; j += 2 * width) {
+                const int64_t a0 = bounds[size_t(j)], a1 = bounds[size_t(std::min(j + width, kBtRows))],
+                              a2 = bounds[size_t(std::min(j + 2 * width, kBtRows))];
+                std::merge(ka.begin() + a0, ka.begin() + a1, ka.begin() + a1, ka.begin() + a2,
+                           kb.begin() + a0);
+            }
+            ka.swap(kb);
+        }
+        struct Ent {
+            int32_t px, row, k;
+        };
+        std::vector<Ent> m(static_cast<size_t>(n_e));
+        for (int64_t i = 0; i < n_e; ++i) {
+            const uint64_t key = ka[size_t(i)];
+            const int j = int((key >> 27) & 31u);
+            m[size_t(i)] = {int32_t(key >> 32), j, int32_t(rp[size_t(r0 + j)] + int64_t(key & ((1u << 27) - 1)))};
+        }
+        T.entries = n_e;
+        T.pairs.reserve(size_t(n_e / 2 + 64));
+        T.px.reserve(size_t(n_e / 2 + 64));
+        T.org.assign(size_t(nr), make_int4(-1, 0, -1, 0));
+        std::vector<std::vector<std::pair<int32_t, int32_t>>> run(static_cast<size_t>(nr));  // (slot, entry)
+        std::vector<int32_t> chunk_px;
+        auto close = [&]() {
+            if (chunk_px.empty()) return;
+            const int ci = int(T.chunks.size());
+            int4 ch = make_int4(int(T.px.size()), int(chunk_px.size()), int(T.pairs.size()), 0);
+            T.px.insert(T.px.end(), chunk_px.begin(), chunk_px.end());
+            int po = 0;
+            for (int j = 0; j < kBtRows; ++j) {
+                T.cpair.push_back(po);
+                if (j >= nr) continue;
+                const auto &rv = run[size_t(j)];
+                for (size_t e = 0; e < rv.size(); e += 2) {
+                    const bool two = e + 1 < rv.size();
+                    T.pairs.push_back(make_int4(rv[e].first, two ? rv[e + 1].first : kBtDCap,
+                                                rv[e].second, two ? rv[e + 1].second : -1));
+                    ++po;
+                }
+                for (const auto &se : rv)
+                    if (se.second == fv[size_t(r0 + j)]) T.org[size_t(j)] = make_int4(ci, se.first, se.second, 0);
+            }
+            T.cpair.push_back(po);
+            ch.w = po;
+            T.chunks.push_back(ch);
+            chunk_px.clear();
+            for (auto &rv : run) rv.clear();
+        };
+        int pairs = 0;
+        for (size_t i = 0; i < m.size();) {
+            size_t e = i;
+            while (e < m.size() && m[e].px == m[i].px) ++e;
+            // pairs after adding this pixel's entries
+            int add = 0;
+            for (size_t q = i; q < e; ++q) add += (run[size_t(m[q].row)].size() % 2 == 0) ? 1 : 0;
+            if (!chunk_px.empty() &&
+                (int(chunk_px.size()) + 1 > kBtDCap || pairs + add > kBtPCap)) {
+                close();
+                pairs = 0;
+                add = int(e - i);
+            }
+            const int slot = int(chunk_px.size());
+            chunk_px.push_back(m[i].px);
+            for (size_t q = i; q < e; ++q) run[size_t(m[q].row)].push_back({slot, m[q].k});
+            pairs += add;
+            i = e;
+        }
+        close();
+        for (int j = 0; j < nr; ++j)
+            if (T.org[size_t(j)].x >= 0) T.org[size_t(j)].w = int(rp[size_t(r0 + j) + 1]);
+    };
+    const int nt = int(std::min<int64_t>(
+        n_items, std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
+    auto parallel = [&](auto &&fn) {
+        std::vector<std::thread> pool;
+        std::atomic<int64_t> next{0};
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&]() {
+                for (int64_t i; (i = next.fetch_add(1)) < n_items;) fn(i);
+            });
+        for (auto &th : pool) th.join();
+    };
+    parallel(build);
+    // Largest tiles first; then flatten.
+    std::vector<int64_t> order(static_cast<size_t>(n_items));
+    for (int64_t i = 0; i < n_items; ++i) order[size_t(i)] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+        return tiles[size_t(a)].entries > tiles[size_t(b)].entries;
+    });
+    // Output offsets of every tile, then the tiles copied in parallel.
+    std::vector<int64_t> o_ch(size_t(n_items) + 1, 0), o_px(size_t(n_items) + 1, 0),
+        o_pr(size_t(n_items) + 1, 0);
+    for (int64_t i = 0; i < n_items; ++i) {
+        const Tile &T = tiles[size_t(order[size_t(i)])];
+        o_ch[size_t(i) + 1] = o_ch[size_t(i)] + int64_t(T.chunks.size());
+        o_px[size_t(i) + 1] = o_px[size_t(i)] + int64_t(T.px.size());
+        o_pr[size_t(i) + 1] = o_pr[size_t(i)] + int64_t(T.pairs.size());
+    }
+    if (o_pr[size_t(n_items)] > INT32_MAX || o_px[size_t(n_items)] > INT32_MAX)
+        fail(DG_UNSUPPORTED, "table too large for bin tiles");
+    // default-initialised (not zeroed): every element is written below
+    const size_t n_chunks = size_t(o_ch[size_t(n_items)]), n_pairs = size_t(o_pr[size_t(n_items)]);
+    std::vector<int4> items(static_cast<size_t>(n_items)), org(static_cast<size_t>(nb));
+    std::unique_ptr<int32_t[]> meta(new int32_t[std::max<size_t>(n_chunks * kBtMetaWords, 1)]);
+    std::unique_ptr<int4[]> pairs(new int4[std::max<size_t>(n_pairs, 1)]);
+    auto flatten = [&](int64_t i) {
+        const int64_t ti = order[size_t(i)];
+        Tile &T = tiles[size_t(ti)];
+        const int64_t c0 = o_ch[size_t(i)], pr0 = o_pr[size_t(i)];
+        for (size_t c = 0; c < T.chunks.size(); ++c) {
+            const int4 ch = T.chunks[c];
+            int32_t *rec = meta.get() + (size_t(c0) + c) * kBtMetaWords;
+            rec[0] = ch.y;
+            rec[1] = ch.w;
+            rec[2] = int32_t(ch.z + pr0);
+            rec[3] = 0;
+            for (int j = 0; j < kBtMetaHead - 4; ++j)
+                rec[4 + j] = j <= kBtRows ? T.cpair[c * (kBtRows + 1) + size_t(j)] : 0;
+            std::copy(T.px.begin() + ch.x, T.px.begin() + ch.x + ch.y, rec + kBtMetaHead);
+            std::fill(rec + kBtMetaHead + ch.y, rec + kBtMetaWords, 0);
+        }
+        std::copy(T.pairs.begin(), T.pairs.end(), pairs.get() + pr0);
+        const int64_t r0 = ti * kBtRows;
+        const int nr = int(std::min<int64_t>(nb, r0 + kBtRows) - r0);
+        for (int j = 0; j < nr; ++j) org[size_t(r0 + j)] = T.org[size_t(j)];
+        items[size_t(i)] = make_int4(int(r0), nr, int(c0), int(T.chunks.size()));
+        T = Tile();
+    };
+    parallel(flatten);
+    out.bt_n_items = int32_t(items.size());
+    out.bt_item.alloc(items.size());
+    out.bt_meta.alloc(std::max<size_t>(n_chunks * kBtMetaWords, 1));
+    out.bt_org.alloc(org.size());
+    out.bt_pair_a.alloc(std::max<size_t>(n_pairs, 1));
+    out.bt_pair_as.alloc(std::max<size_t>(n_pairs, 1));
+    out.bt_pair_b.alloc(std::max<size_t>(n_pairs, 1));
+    DeviceArray<int4> desc;
+    desc.alloc(std::max<size_t>(n_pairs, 1));
+    DG_CUDA(cudaMemcpyAsync(out.bt_item.ptr, items.data(), items.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, s));
+    if (n_chunks)
+        DG_CUDA(cudaMemcpyAsync(out.bt_meta.ptr, meta.get(), n_chunks * kBtMetaWords * 4,
+                                cudaMemcpyHostToDevice, s));
+    DG_CUDA(cudaMemcpyAsync(out.bt_org.ptr, org.data(), org.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice, s));
+    if (n_pairs) {
+        DG_CUDA(cudaMemcpyAsync(desc.ptr, pairs.get(), n_pairs * sizeof(int4),
+                                cudaMemcpyHostToDevice, s));
+        k_bt_fill<<<148 * 8, 256, 0, s>>>(desc.ptr, int64_t(n_pairs), out.entry.ptr,
+                                         out.entry_std.ptr, out.bt_pair_a.ptr, out.bt_pair_as.ptr,
+                                         out.bt_pair_b.ptr);
+        DG_CUDA(cudaGetLastError());
+    }
+    DG_CUDA(cudaStreamSynchronize(s));
+}
+
 void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1, int32_t dim2,
                        int32_t strip_rows, cudaStream_t s, GatherTable &out) {
     out.n_rows = int32_t(table.n_rows);
@@ -1406,6 +1964,7 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     build_fl_units(out, table, segs, [&](int cap, int max_segs, std::vector<int4> &fl) {
         group(cap, max_segs, [&](int first, int n) { fl.push_back(make_int4(first, n, 0, 0)); });
     }, s);
+    build_bin_tiles(out, table, rp, s);
 }
 
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
@@ -1424,6 +1983,10 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
     for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
         const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
         const void *fp = static_cast<const unsigned char *>(d_frames) + f0 * n_pixels * esize;
+        double *oi = d_i + f0 * t.n_rows;
+        double *os = d_sigma ? d_sigma + f0 * t.n_rows : nullptr;
+        double *od = d_std ? d_std + f0 * t.n_rows : nullptr;
+        bool done = false;  // results written by the gather itself (bin tiles)
         if (t.n_units > 0) {
             std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
             if (t.profile) {
@@ -1438,19 +2001,17 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
                 DG_CUDA(cudaEventRecord(ev->first, s));
             }
             ++t.launches;
+            double *pp = t.partial.ptr;
             switch (dtype) {
-            case DG_U16: launch_typed<uint16_t>(t, fp, n_pixels, nf, mode, s); break;
-            case DG_U32: launch_typed<uint32_t>(t, fp, n_pixels, nf, mode, s); break;
-            case DG_I32: launch_typed<int32_t>(t, fp, n_pixels, nf, mode, s); break;
-            case DG_F32: launch_typed<float>(t, fp, n_pixels, nf, mode, s); break;
-            case DG_F64: launch_typed<double>(t, fp, n_pixels, nf, mode, s); break;
+            case DG_U16: done = launch_typed<uint16_t>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
+            case DG_U32: done = launch_typed<uint32_t>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
+            case DG_I32: done = launch_typed<int32_t>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
+            case DG_F32: done = launch_typed<float>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
+            case DG_F64: done = launch_typed<double>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
             }
             if (ev) DG_CUDA(cudaEventRecord(ev->second, s));
         }
-        double *oi = d_i + f0 * t.n_rows;
-        double *os = d_sigma ? d_sigma + f0 * t.n_rows : nullptr;
-        double *od = d_std ? d_std + f0 * t.n_rows : nullptr;
-        if (t.n_rows > 0) {
+        if (t.n_rows > 0 && !done) {
             ++t.launches;
             switch (dtype) {
             case DG_U16: finalize_typed<uint16_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
@@ -1490,15 +2051,29 @@ __global__ void k_flip_rows(int2 *__restrict__ entry, float4 *__restrict__ entry
     }
 }
 
+// The same for the pixel indices of bin-tile chunk records (D of them each).
+__global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int rows, int cols) {
+    for (int64_t r = blockIdx.x; r < n_rec; r += gridDim.x) {
+        int32_t *rec = meta + r * kBtMetaWords;
+        const int d = rec[0];
+        for (int k = threadIdx.x; k < d; k += blockDim.x)
+            rec[kBtMetaHead + k] = flip_px(rec[kBtMetaHead + k], rows, cols);
+    }
+}
+
 }  // namespace
 
 void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s) {
     t.flip_rows = dim1;
     t.flip_cols = dim2;
     const int64_t n_px = t.fl_px.ptr ? int64_t(t.fl_px.count) : 0;
-    if (t.nnz + n_px == 0) return;
-    k_flip_rows<<<148 * 8, 256, 0, s>>>(t.entry.ptr, t.entry_std.ptr, t.nnz, t.fl_px.ptr, n_px,
-                                        dim1, dim2);
+    if (t.nnz + n_px > 0)
+        k_flip_rows<<<148 * 8, 256, 0, s>>>(t.entry.ptr, t.entry_std.ptr, t.nnz, t.fl_px.ptr,
+                                            n_px, dim1, dim2);
+    DG_CUDA(cudaGetLastError());
+    // the pixel lists of the bin-tile chunk records
+    const int64_t n_rec = t.bt_n_items > 0 ? int64_t(t.bt_meta.count) / kBtMetaWords : 0;
+    if (n_rec > 0) k_flip_meta<<<148 * 4, 256, 0, s>>>(t.bt_meta.ptr, n_rec, dim1, dim2);
     DG_CUDA(cudaGetLastError());
 }
 
@@ -1598,13 +2173,14 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
 
 namespace {
 
+// One integration with mapping `variant`: the gather and, unless it wrote the
+// results itself, the finalize (the autotuner compares whole integrations).
 template <typename P>
 void launch_mode(GatherTable &t, int variant, int mode, const void *frames, int64_t n_pixels,
-                 int nf, cudaStream_t s) {
-    const P *fp = static_cast<const P *>(frames);
-    if (mode == kSpread) launch_gather<kSpread, P>(t, variant, fp, n_pixels, nf, t.partial.ptr, s);
-    else if (mode == kErrors) launch_gather<kErrors, P>(t, variant, fp, n_pixels, nf, t.partial.ptr, s);
-    else launch_gather<kIntensity, P>(t, variant, fp, n_pixels, nf, t.partial.ptr, s);
+                 int nf, double *oi, double *os, double *od, cudaStream_t s) {
+    if (!launch_typed<P>(t, variant, frames, n_pixels, nf, mode, t.partial.ptr, oi, os, od, s) &&
+        t.n_rows > 0)
+        finalize_typed<P>(t, mode, frames, n_pixels, nf, oi, os, od, s);
 }
 
 }  // namespace
@@ -1614,6 +2190,7 @@ int gather_variant_count() { return kVariantCount; }
 bool gather_variant_available(const GatherTable &t, int variant) {
     if (variant < 0 || variant >= kVariantCount) return false;
     if (variant == 5 || variant == 6) return t.fl_n_units > 0;
+    if (variant == 7) return t.bt_n_items > 0;
     return true;
 }
 
@@ -1629,6 +2206,11 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
     if (each) each->assign(size_t(kVariantCount), 0.0);
     if (t.n_units == 0) return t.variant;
+    DeviceArray<double> outs;
+    outs.alloc(size_t(std::max<int64_t>(1, int64_t(t.n_rows) * nf * 3)));
+    double *oi = outs.ptr, *os = oi + int64_t(t.n_rows) * nf, *od = os + int64_t(t.n_rows) * nf;
+    if (!(flags & DG_ERRORS)) os = nullptr;
+    if (!(flags & DG_AZIMUTHAL_STD)) od = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
     DG_CUDA(cudaEventCreate(&a));
     DG_CUDA(cudaEventCreate(&b));
@@ -1644,11 +2226,11 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
             for (int rep = 0; rep < 4; ++rep) {
                 DG_CUDA(cudaEventRecord(a, s));
                 switch (dtype) {
-                case DG_U16: launch_mode<uint16_t>(t, v, mode, d_frames, n_pixels, nf, s); break;
-                case DG_U32: launch_mode<uint32_t>(t, v, mode, d_frames, n_pixels, nf, s); break;
-                case DG_I32: launch_mode<int32_t>(t, v, mode, d_frames, n_pixels, nf, s); break;
-                case DG_F32: launch_mode<float>(t, v, mode, d_frames, n_pixels, nf, s); break;
-                case DG_F64: launch_mode<double>(t, v, mode, d_frames, n_pixels, nf, s); break;
+                case DG_U16: launch_mode<uint16_t>(t, v, mode, d_frames, n_pixels, nf, oi, os, od, s); break;
+                case DG_U32: launch_mode<uint32_t>(t, v, mode, d_frames, n_pixels, nf, oi, os, od, s); break;
+                case DG_I32: launch_mode<int32_t>(t, v, mode, d_frames, n_pixels, nf, oi, os, od, s); break;
+                case DG_F32: launch_mode<float>(t, v, mode, d_frames, n_pixels, nf, oi, os, od, s); break;
+                case DG_F64: launch_mode<double>(t, v, mode, d_frames, n_pixels, nf, oi, os, od, s); break;
                 }
                 DG_CUDA(cudaEventRecord(b, s));
                 DG_CUDA(cudaEventSynchronize(b));
@@ -1728,12 +2310,10 @@ template <typename P>
 void noalloc_launch(const GatherTable &t, double *partial, const void *frames, int64_t n_pixels,
                     int nf, int mode, double *oi, double *os, double *od, cudaStream_t s) {
     const P *fp = static_cast<const P *>(frames);
-    if (t.n_units > 0) {
-        if (mode == kSpread) launch_gather<kSpread, P>(t, t.variant, fp, n_pixels, nf, partial, s);
-        else if (mode == kErrors) launch_gather<kErrors, P>(t, t.variant, fp, n_pixels, nf, partial, s);
-        else launch_gather<kIntensity, P>(t, t.variant, fp, n_pixels, nf, partial, s);
-    }
-    if (t.n_rows > 0) {
+    bool done = false;
+    if (t.n_units > 0) done = launch_typed<P>(t, t.variant, frames, n_pixels, nf, mode, partial,
+                                              oi, os, od, s);
+    if (t.n_rows > 0 && !done) {
         const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);
 #define DG_NOALLOC_FINALIZE(M)                                                                 \
     k_finalize<M, P><<<blocks, 256, 0, s>>>(                                                   \

@@ -186,6 +186,13 @@ struct GatherTable {
     // {pixel bits, w, w*norm, 0} per entry and the FP64 weight sum per row.
     DeviceArray<float4> entry_raw;
     DeviceArray<double> cnt;
+    // Bin tiles (k_gather_bins): runs of 16 rows, their entries cut into
+    // pixel-interval chunks; see dg_gather.cu.
+    int32_t bt_n_items = 0;
+    DeviceArray<int4> bt_item;        // {first row, rows, first chunk, chunks}, largest first
+    DeviceArray<int32_t> bt_meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
+    DeviceArray<int4> bt_org;         // per row {chunk in tile (-1: none), slot, entry, row end}
+    DeviceArray<float4> bt_pair_a, bt_pair_as, bt_pair_b;
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     int32_t flip_rows = 0, flip_cols = 0;  // frames stored bottom row first (0: detector order)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).

@@ -4,9 +4,10 @@
 Workload (default): Eiger-4M-shaped detector (2167 x 2070, 75 um pixels,
 tilted, module gaps + 2% dead pixels masked), 256 seeded uint32 frames,
 PixelSplit, 2000 radial bins, errors + azimuthal spread. One step integrates
-the 256 frames already resident in HBM with one batched gather launch (plus
-its finalize pass). Frames are Poisson-sampled on the device from a seeded
-ring pattern; no dataset is read.
+the 256 frames already resident in HBM with one batched gather launch (plus a
+finalize pass for the lane mappings that leave partial sums; the bin-tile
+mapping writes the results itself). Frames are Poisson-sampled on the device
+from a seeded ring pattern; no dataset is read.
 
 Reported on one JSON line (rank 0):
   value     whole-job frames/s, device-resident frames, max over ranks
@@ -40,10 +41,12 @@ sys.path.insert(0, ROOT)
 METRIC = "eiger4m_1d_frames_per_s"
 
 # DRAM bytes (read + write) of one gather launch from an ncu capture, keyed by
-# (workload, gather mapping, frames per launch): a 32-frame launch captured in
-# full, its frame and partial-sum bytes scaled to 256 frames
-# (profiles/k_gather_fl_eiger4m_32frames_full.md).
-MEASURED_TRAFFIC = {("eiger4m_ps2000_b256", 6, 256): 5_533_000_000}
+# (workload, gather mapping, frames per launch): the bin-tile mapping captured
+# at full size (dram__bytes_read.sum + dram__bytes_write.sum, one pass:
+# profiles/k_gather_bins_eiger4m_b256.md); the frame-lane mapping from a
+# 32-frame capture with frame and partial-sum bytes scaled to 256 frames.
+MEASURED_TRAFFIC = {("eiger4m_ps2000_b256", 7, 256): 5_722_000_000,
+                    ("eiger4m_ps2000_b256", 6, 256): 5_533_000_000}
 
 
 def parse():
@@ -515,9 +518,11 @@ def main():
 
     # Per-plan autotune of the gather's lane mapping on the resident frames
     # (outside the timed region, like the plan build).
+    t_tune = time.perf_counter()
     with torch.cuda.stream(stream):
         variant, variant_ms = plan.autotune(frames, errors=w.errors,
                                             azimuthal_std=w.azimuthal_std)
+    tune_ms = (time.perf_counter() - t_tune) * 1000.0
     if args.variant is not None:
         plan.gather_variant = args.variant
         variant = args.variant
@@ -589,6 +594,7 @@ def main():
         "clocks": clk,
         "gpu_launches": int(launches.value),
         "build_ms": round(info.build_ms, 2),
+        "autotune_ms_wall": round(tune_ms, 1),
     }
     if w.kind == "precision" and rank == 0:
         torch.cuda.synchronize()

@@ -668,6 +668,7 @@ dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype, i
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        dg::ensure_bin_tiles(plan->gather, plan->table, s);
         std::vector<double> each;
         const int v = dg::autotune_gather(plan->gather, d_frames, dtype,
                                           int64_t(plan->dim1) * plan->dim2, n_frames, flags, s,
@@ -683,6 +684,10 @@ dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current, int32_t 
         std::lock_guard<std::mutex> lock(plan->mu);
         if (set >= dg::gather_variant_count())
             dg::fail(DG_INVALID_INPUT, "gather mapping " + std::to_string(set) + " does not exist");
+        if (set >= 0 && dg::gather_variant_needs_tiles(set)) {
+            DeviceScope scope(plan->device);
+            dg::ensure_bin_tiles(plan->gather, plan->table, plan->stream);
+        }
         if (set >= 0 && !dg::gather_variant_available(plan->gather, set))
             dg::fail(DG_UNSUPPORTED, "gather mapping " + std::to_string(set) +
                                          " is not available for this plan");

@@ -1671,11 +1671,12 @@ void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<
 // and each row's entries in it are a contiguous run of its CSR row). Tiles
 // are ordered largest first. Each row's origin (its first entry valid for the
 // spread) is located as {chunk within the tile, slot}.
-void build_bin_tiles(GatherTable &out, const DeviceCsr &table, const std::vector<int64_t> &rp,
-                     cudaStream_t s) {
+void build_bin_tiles(GatherTable &out, const DeviceCsr &table, cudaStream_t s) {
     const int64_t nb = table.n_rows;
     out.bt_n_items = 0;
     if (nb == 0 || table.nnz == 0) return;
+    std::vector<int64_t> rp(static_cast<size_t>(nb) + 1);
+    DG_CUDA(cudaMemcpyAsync(rp.data(), table.row_ptr.ptr, rp.size() * 8, cudaMemcpyDeviceToHost, s));
     std::vector<int32_t> col(static_cast<size_t>(table.nnz)), fv(static_cast<size_t>(nb));
     DG_CUDA(cudaMemcpyAsync(col.data(), table.col.ptr, col.size() * 4, cudaMemcpyDeviceToHost, s));
     DG_CUDA(cudaMemcpyAsync(fv.data(), out.first_valid.ptr, fv.size() * 4, cudaMemcpyDeviceToHost, s));
@@ -1867,6 +1868,24 @@ void build_bin_tiles(GatherTable &out, const DeviceCsr &table, const std::vector
     DG_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+__global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int rows, int cols);
+}  // namespace
+
+void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, cudaStream_t s) {
+    if (t.bt_built) return;
+    build_bin_tiles(t, table, s);
+    if (t.flip_rows && t.bt_n_items > 0) {
+        k_flip_meta<<<148 * 4, 256, 0, s>>>(t.bt_meta.ptr, int64_t(t.bt_meta.count) / kBtMetaWords,
+                                            t.flip_rows, t.flip_cols);
+        DG_CUDA(cudaGetLastError());
+        DG_CUDA(cudaStreamSynchronize(s));
+    }
+    t.bt_built = true;
+}
+
+bool gather_variant_needs_tiles(int variant) { return variant == 7; }
+
 void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1, int32_t dim2,
                        int32_t strip_rows, cudaStream_t s, GatherTable &out) {
     out.n_rows = int32_t(table.n_rows);
@@ -1964,7 +1983,6 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     build_fl_units(out, table, segs, [&](int cap, int max_segs, std::vector<int4> &fl) {
         group(cap, max_segs, [&](int first, int n) { fl.push_back(make_int4(first, n, 0, 0)); });
     }, s);
-    build_bin_tiles(out, table, rp, s);
 }
 
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
@@ -2071,10 +2089,7 @@ void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s
         k_flip_rows<<<148 * 8, 256, 0, s>>>(t.entry.ptr, t.entry_std.ptr, t.nnz, t.fl_px.ptr,
                                             n_px, dim1, dim2);
     DG_CUDA(cudaGetLastError());
-    // the pixel lists of the bin-tile chunk records
-    const int64_t n_rec = t.bt_n_items > 0 ? int64_t(t.bt_meta.count) / kBtMetaWords : 0;
-    if (n_rec > 0) k_flip_meta<<<148 * 4, 256, 0, s>>>(t.bt_meta.ptr, n_rec, dim1, dim2);
-    DG_CUDA(cudaGetLastError());
+    // bin tiles are built later (ensure_bin_tiles) and flipped then
 }
 
 void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s) {

@@ -188,6 +188,7 @@ struct GatherTable {
     DeviceArray<double> cnt;
     // Bin tiles (k_gather_bins): runs of 16 rows, their entries cut into
     // pixel-interval chunks; see dg_gather.cu.
+    bool bt_built = false;            // built on first use (ensure_bin_tiles)
     int32_t bt_n_items = 0;
     DeviceArray<int4> bt_item;        // {first row, rows, first chunk, chunks}, largest first
     DeviceArray<int32_t> bt_meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
@@ -222,6 +223,10 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
 // InputOrder::FlipVertical: remaps the pixel indices of a built gather table
 // to frames whose rows come in reverse order (entry order unchanged).
 void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s);
+// Bin tiles for lane mapping 7, built from the plan's masked table on first
+// use (the autotuner, or selecting the mapping); idempotent.
+void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, cudaStream_t s);
+bool gather_variant_needs_tiles(int variant);
 void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s);
 void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                     int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride, uint32_t flags,

@@ -19,6 +19,7 @@ UNITS = {"2th_rad": 0, "2th_deg": 1, "q_A^-1": 2, "q_nm^-1": 3}
 PRECISIONS = {"f32": 0, "f32_compensated": 1, "f64": 2}
 DG_ERRORS, DG_AZIMUTHAL_STD = 1, 2
 DG_U16, DG_U32, DG_I32, DG_F32, DG_F64 = 0, 1, 2, 3, 4
+DG_SUBMIT_BORROW = 256
 DG_PLAN_KEEP_TABLES = 1
 DG_PLAN_FLIP_VERTICAL = 2
 
@@ -77,7 +78,7 @@ class ServerConfig(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "submitted", "completed", "failed", "launches", "coalesced_frames", "plan_builds",
-        "plan_hits", "plan_evictions", "cache_bytes")]
+        "plan_hits", "plan_evictions", "cache_bytes", "batch_us", "build_us")]
 
 
 class DeviceInfo(C.Structure):

@@ -668,7 +668,8 @@ dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype, i
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
-        dg::ensure_bin_tiles(plan->gather, plan->table, s);
+        // bin tiles pay off only with enough frames to fill the GPU
+        if (n_frames > dg::kBinTileMinFrames) dg::ensure_bin_tiles(plan->gather, plan->table, s);
         std::vector<double> each;
         const int v = dg::autotune_gather(plan->gather, d_frames, dtype,
                                           int64_t(plan->dim1) * plan->dim2, n_frames, flags, s,

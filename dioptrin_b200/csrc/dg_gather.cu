@@ -2233,7 +2233,8 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     float best_t = 3.4e38f;
     try {
         for (int v = 0; v < kVariantCount; ++v) {
-            if (!gather_variant_available(t, v)) {
+            if (!gather_variant_available(t, v) ||
+                (gather_variant_needs_tiles(v) && n_frames <= kBinTileMinFrames)) {
                 if (each) (*each)[size_t(v)] = -1.0;
                 continue;
             }

@@ -227,6 +227,9 @@ void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s
 // use (the autotuner, or selecting the mapping); idempotent.
 void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, cudaStream_t s);
 bool gather_variant_needs_tiles(int variant);
+// The autotuner times the bin-tile mapping only for batches of more frames
+// than this (one tile per CTA: smaller batches leave SMs idle).
+constexpr int64_t kBinTileMinFrames = 64;
 void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s);
 void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                     int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride, uint32_t flags,

@@ -76,8 +76,9 @@ struct Request {
     uint64_t ticket = 0, key = 0;
     int32_t dtype = 0;
     uint32_t flags = 0;
-    void *frame = nullptr;  // pinned, frame_bytes long
+    void *frame = nullptr;  // pinned, frame_bytes long (the caller's with DG_SUBMIT_BORROW)
     size_t frame_bytes = 0;
+    bool borrowed = false;
     Clock::time_point submitted;
     double latency_us = 0;
     std::vector<double> out_i, out_s, out_d;
@@ -123,10 +124,31 @@ struct dg_server {
     PinnedPool pinned;
     std::vector<CacheEntry> retired;  // stale plans still in use
     uint64_t next_generation = 1;
+    std::unordered_map<uint64_t, int> building;  // keys a worker is building now
+    std::unordered_map<uint64_t, int32_t> tuned;  // key -> lane mapping its last plan used
 
     // Returns a plan for `key` with a user reference, building it on a miss and
     // evicting idle LRU plans to stay within the byte budget. Called unlocked.
-    dg_plan *acquire(uint64_t key, std::string &err, dg_status &st) {
+    // A new plan's lane mapping, tuned for the small coalesced launches of the
+    // loop on zero frames of the request's type (timing does not depend on
+    // the values); left at the default if anything fails.
+    void tune(dg_plan *plan, int32_t dtype, uint32_t flags) {
+        const int64_t nf = std::max(1, std::min(8, cfg.max_coalesce));
+        const size_t bytes = size_t(plan->dim1) * plan->dim2 * px_size(dtype) * size_t(nf);
+        void *d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return;
+        }
+        cudaMemsetAsync(d, 0, bytes, plan->stream);
+        if (dg_plan_autotune(plan, d, dtype, nf, flags & (DG_ERRORS | DG_AZIMUTHAL_STD), nullptr,
+                             nullptr, nullptr, 0) != DG_OK)
+            (void)last_error_text();
+        cudaFree(d);
+    }
+
+    dg_plan *acquire(uint64_t key, int32_t dtype, uint32_t flags, std::string &err,
+                     dg_status &st) {
         PlanSpec spec;
         {
             std::unique_lock<std::mutex> lock(mu);
@@ -139,7 +161,17 @@ struct dg_server {
                 return it->second.plan;
             }
             if (it != cache.end()) retire_locked(it);
+            building[key]++;
         }
+        struct Built {
+            dg_server *s;
+            uint64_t key;
+            ~Built() {
+                std::lock_guard<std::mutex> lock(s->mu);
+                if (--s->building[key] == 0) s->building.erase(key);
+            }
+        } built{this, key};
+        const auto t_build = Clock::now();
         dg_plan *plan = nullptr;
         st = dg_plan_create(&spec.geometry, &spec.method, spec.mask.empty() ? nullptr : spec.mask.data(),
                             spec.dim1, spec.dim2, spec.n_radial, spec.n_azimuthal,
@@ -147,6 +179,26 @@ struct dg_server {
         if (st != DG_OK) {
             err = last_error_text();
             return nullptr;
+        }
+        // A rebuilt key (new PONI, same shape and bins) keeps the mapping its
+        // previous plan was tuned to; a new key is tuned once.
+        int32_t known = -1;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            auto t = tuned.find(key);
+            if (t != tuned.end()) known = t->second;
+        }
+        if (known < 0 || dg_plan_variant(plan, known, nullptr, nullptr) != DG_OK) {
+            tune(plan, dtype, flags);
+            int32_t v = 0;
+            dg_plan_variant(plan, -1, &v, nullptr);
+            std::lock_guard<std::mutex> lock(mu);
+            tuned[key] = v;
+        }
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            stats.build_us += int64_t(
+                std::chrono::duration<double, std::micro>(Clock::now() - t_build).count());
         }
         dg_plan_info info{};
         dg_plan_query(plan, &info);
@@ -245,8 +297,16 @@ struct dg_server {
                                  [&] { return stop || !queue.empty(); });
                 if (stop && queue.empty()) break;
                 if (queue.empty()) continue;
-                Request *head = queue.front();
-                queue.pop_front();
+                // the oldest request whose plan no other worker is building
+                auto hit = queue.begin();
+                while (hit != queue.end() && building.count((*hit)->key)) ++hit;
+                if (hit == queue.end()) {
+                    lock.unlock();
+                    std::this_thread::sleep_for(std::chrono::microseconds(200));
+                    continue;
+                }
+                Request *head = *hit;
+                queue.erase(hit);
                 batch.push_back(head);
                 for (auto it = queue.begin(); it != queue.end() &&
                                               int(batch.size()) < cfg.max_coalesce;) {
@@ -262,7 +322,7 @@ struct dg_server {
             Request *head = batch.front();
             std::string err;
             dg_status st = DG_OK;
-            dg_plan *plan = acquire(head->key, err, st);
+            dg_plan *plan = acquire(head->key, head->dtype, head->flags, err, st);
             if (plan) {
                 const size_t fb = head->frame_bytes;
                 const int64_t nb = plan->n_bins;
@@ -290,6 +350,7 @@ struct dg_server {
                         out_cap = 0;
                     }
                 }
+                const auto t_batch = Clock::now();
                 if (!d_in || !d_out) {
                     st = DG_DEVICE;
                     err = "request loop staging allocation failed";
@@ -328,6 +389,9 @@ struct dg_server {
                     }
                 }
                 release(head->key, plan);
+                std::lock_guard<std::mutex> lock(mu);
+                stats.batch_us += int64_t(
+                    std::chrono::duration<double, std::micro>(Clock::now() - t_batch).count());
             }
             {
                 std::unique_lock<std::mutex> lock(mu);
@@ -342,7 +406,7 @@ struct dg_server {
                         std::chrono::duration<double, std::micro>(now - r->submitted).count();
                     if (st == DG_OK) stats.completed++;
                     else stats.failed++;
-                    pinned.put(r->frame_bytes, r->frame);
+                    if (!r->borrowed) pinned.put(r->frame_bytes, r->frame);
                     r->frame = nullptr;
                     inflight--;
                 }
@@ -436,7 +500,10 @@ dg_status dg_server_submit(dg_server *server, uint64_t key, const void *frame, i
                            uint32_t flags, int32_t wait_ms, uint64_t *ticket) {
     if (!server || !frame || !ticket) return server_fail(DG_INVALID_INPUT, "NULL argument");
     if (dtype < DG_U16 || dtype > DG_F64) return server_fail(DG_INVALID_INPUT, "unknown dtype");
-    if (flags & ~(DG_ERRORS | DG_AZIMUTHAL_STD)) return server_fail(DG_INVALID_INPUT, "unknown flags");
+    if (flags & ~(DG_ERRORS | DG_AZIMUTHAL_STD | DG_SUBMIT_BORROW))
+        return server_fail(DG_INVALID_INPUT, "unknown flags");
+    const bool borrow = (flags & DG_SUBMIT_BORROW) != 0;
+    flags &= ~DG_SUBMIT_BORROW;
     std::unique_lock<std::mutex> lock(server->mu);
     auto spec = server->specs.find(key);
     if (spec == server->specs.end()) return server_fail(DG_INVALID_INPUT, "unregistered plan key");
@@ -453,7 +520,8 @@ dg_status dg_server_submit(dg_server *server, uint64_t key, const void *frame, i
     r->flags = flags;
     r->submitted = Clock::now();
     r->frame_bytes = bytes;
-    r->frame = server->pinned.get(bytes);
+    r->borrowed = borrow;
+    r->frame = borrow ? const_cast<void *>(frame) : server->pinned.get(bytes);
     if (!r->frame) {
         lock.lock();
         server->inflight--;
@@ -461,7 +529,7 @@ dg_status dg_server_submit(dg_server *server, uint64_t key, const void *frame, i
         server->cv_slot.notify_one();
         return server_fail(DG_DEVICE, "pinned staging allocation failed");
     }
-    std::memcpy(r->frame, frame, bytes);
+    if (!borrow) std::memcpy(r->frame, frame, bytes);
     lock.lock();
     r->ticket = server->next_ticket++;
     *ticket = r->ticket;

@@ -4,11 +4,13 @@ device-resident plans held in an HBM cache bounded by bytes."""
 from __future__ import annotations
 
 import ctypes as C
+import threading
 from typing import Optional
 
 import numpy as np
 
 from . import _native as N
+from ._native import RequestTimeout
 from .integrator import _DTYPES, Integrator, _dp
 
 
@@ -21,6 +23,8 @@ class RequestLoop:
         N.check(N.lib().dg_server_create(C.byref(cfg), C.byref(self._h)))
         self._bins: dict = {}
         self._shapes: dict = {}
+        self._borrowed: dict = {}  # ticket -> borrowed frame, until polled
+        self._lock = threading.Lock()
 
     def register(self, key: int, integrator: Integrator, shape, n_points: int,
                  precision: str = "f32_compensated", n_azimuthal: int = 0,
@@ -41,16 +45,28 @@ class RequestLoop:
         self._shapes[key] = (dim1, dim2)
 
     def submit(self, key: int, frame: np.ndarray, errors: bool = False,
-               azimuthal_std: bool = False, wait_ms: int = 10000) -> int:
-        a = np.ascontiguousarray(frame)
+               azimuthal_std: bool = False, wait_ms: int = 10000, *,
+               borrow: bool = False) -> int:
+        """Queues one frame for plan `key`. With borrow=True the frame is not
+        copied: it must not change until its result is polled (the loop keeps
+        a reference until then); page-locked frames (alloc_pinned,
+        Cuda1dPlan.alloc_pinned_batch) go to the device by DMA."""
+        a = frame if borrow else np.ascontiguousarray(frame)
+        if borrow and not (isinstance(a, np.ndarray) and a.flags.c_contiguous):
+            raise ValueError("a borrowed frame must be a C-contiguous array")
         if a.dtype not in _DTYPES:
             raise TypeError(f"unsupported dtype {a.dtype}")
         if a.shape != self._shapes[key]:
             raise ValueError("frame shape does not match the registered plan")
         flags = (N.DG_ERRORS if errors else 0) | (N.DG_AZIMUTHAL_STD if azimuthal_std else 0)
+        if borrow:
+            flags |= N.DG_SUBMIT_BORROW
         t = C.c_uint64()
         N.check(N.lib().dg_server_submit(self._h, key, a.ctypes.data, _DTYPES[a.dtype], flags,
                                          wait_ms, C.byref(t)))
+        if borrow:
+            with self._lock:
+                self._borrowed[t.value] = a
         return t.value
 
     def poll(self, ticket: int, key: int, errors: bool = False, azimuthal_std: bool = False,
@@ -61,9 +77,20 @@ class RequestLoop:
         os_ = np.empty(nb) if errors else None
         od = np.empty(nb) if azimuthal_std else None
         lat = C.c_double()
-        N.check(N.lib().dg_server_poll(self._h, ticket, wait_ms, _dp(oi), _dp(os_), _dp(od),
-                                       C.byref(lat)))
+        try:
+            N.check(N.lib().dg_server_poll(self._h, ticket, wait_ms, _dp(oi), _dp(os_), _dp(od),
+                                           C.byref(lat)))
+        except RequestTimeout:
+            raise  # still in flight: keep a borrowed frame alive
+        except Exception:
+            self._release(ticket)
+            raise
+        self._release(ticket)
         return oi, os_, od, lat.value
+
+    def _release(self, ticket: int) -> None:
+        with self._lock:
+            self._borrowed.pop(ticket, None)
 
     def stats(self) -> dict:
         s = N.ServerStats()

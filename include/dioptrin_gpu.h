@@ -59,6 +59,11 @@ enum { DG_PRECISION_F32 = 0, DG_PRECISION_F32_COMPENSATED = 1, DG_PRECISION_F64 
 /* Integration flags. */
 #define DG_ERRORS 1u        /* propagated Poisson sigma (integrate1d_with_errors) */
 #define DG_AZIMUTHAL_STD 2u /* weighted population spread (integrate1d_with_azimuthal_std) */
+/* dg_server_submit only: the frame is not copied at submission; it must stay
+ * valid and unchanged until the request completes (dg_server_poll), and is
+ * copied to the device straight from the caller's memory (page-locked memory
+ * from dg_host_alloc gives an asynchronous DMA). */
+#define DG_SUBMIT_BORROW 256u
 
 /* Plan-creation flags. */
 #define DG_PLAN_KEEP_TABLES 1u /* keep the unmasked f64 CSR for dg_plan_export_table */
@@ -331,6 +336,8 @@ typedef struct dg_server_config {
 typedef struct dg_server_stats {
     int64_t submitted, completed, failed, launches, coalesced_frames;
     int64_t plan_builds, plan_hits, plan_evictions, cache_bytes;
+    int64_t batch_us;  /* workers' time from a batch's first copy to its results */
+    int64_t build_us;  /* time spent building (and tuning) plans */
 } dg_server_stats;
 
 DG_EXPORT dg_status dg_server_create(const dg_server_config *config, dg_server **out);

@@ -70,16 +70,40 @@ def test_mixed_stream_results_equal_the_frames_alone(dg):
                 assert b is None
             else:
                 assert np.array_equal(a, b, equal_nan=True), (idx, key)
-    # the Integrator path of the same configurations
+    # the Integrator path of the same configurations (the loop tunes its own
+    # plans' lane mappings, which round differently within the tolerance)
     for idx in (0, 1, 2):
         key, it, shape, nb, na, dt, err, std = cfgs[idx]
         frame = work[idx][1]
         if na:
             r = it.integrate2d(frame, nb, na, err)
-            np.testing.assert_allclose(mixed[idx][0], r.intensity_array, rtol=1e-12)
         else:
             r = it.integrate1d(frame, nb, err, azimuthal_std=std)
-            np.testing.assert_allclose(mixed[idx][0], r.intensity_array, rtol=1e-12)
+        want = r.intensity_array
+        np.testing.assert_allclose(mixed[idx][0], want, rtol=1e-5,
+                                   atol=1e-5 * np.abs(want).max())
+    loop.close()
+
+
+def test_borrowed_pinned_frames(dg):
+    loop = dg.RequestLoop(max_inflight_frames=32, max_coalesce=8)
+    key, it, shape, nb, na, dt, err, std = _configs(dg)[0]
+    loop.register(key, it, shape, nb, n_azimuthal=na)
+    rng = np.random.default_rng(3)
+    frames = [rng.poisson(50.0, shape).astype(dt) for _ in range(12)]
+    pinned = dg.alloc_pinned((12,) + shape, dt)
+    pinned[:] = np.stack(frames)
+    tickets = [loop.submit(key, pinned[k], errors=err, azimuthal_std=std, borrow=True)
+               for k in range(12)]
+    got = [loop.poll(t, key, errors=err, azimuthal_std=std) for t in tickets]
+    for k in range(12):
+        t = loop.submit(key, frames[k], errors=err, azimuthal_std=std)
+        ref = loop.poll(t, key, errors=err, azimuthal_std=std)
+        for a, b in zip(got[k][:3], ref[:3]):
+            assert np.array_equal(a, b, equal_nan=True)
+    assert not loop._borrowed
+    with pytest.raises(ValueError):
+        loop.submit(key, pinned[0][:, ::2], borrow=True)
     loop.close()
 
 
@@ -96,6 +120,6 @@ def test_reregistered_plan_is_rebuilt(dg):
     b = loop.poll(loop.submit(7, frame), 7)[0]
     assert loop.stats()["plan_builds"] == 2
     ref = moved.integrate1d(frame, 30).intensity_array
-    np.testing.assert_allclose(b, ref, rtol=1e-12)
+    np.testing.assert_allclose(b, ref, rtol=1e-5)  # the loop's plan has its own mapping
     assert not np.array_equal(a, b)
     loop.close()

@@ -183,8 +183,7 @@ int64_t dg_plan::device_bytes() const {
          gather.valid_std.bytes() + gather.partial.bytes() + gather.fl_unit.bytes() +
          gather.fl_px.bytes() + gather.fl_pair_a.bytes() + gather.fl_pair_b.bytes() +
          gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes() + gather.entry_raw.bytes() +
-         gather.cnt.bytes() + gather.bt_item.bytes() + gather.bt_meta.bytes() + gather.bt_org.bytes() +
-         gather.bt_pair_a.bytes() + gather.bt_pair_as.bytes() + gather.bt_pair_b.bytes();
+         gather.cnt.bytes() + gather.bt[0].bytes() + gather.bt[1].bytes();
     b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes() +
          stage_mask.bytes();
     return b;
@@ -669,7 +668,8 @@ dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype, i
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
         // bin tiles pay off only with enough frames to fill the GPU
-        if (n_frames > dg::kBinTileMinFrames) dg::ensure_bin_tiles(plan->gather, plan->table, s);
+        if (n_frames > dg::kBinTileMinFrames)
+            for (int v : {7, 8}) dg::ensure_bin_tiles(plan->gather, plan->table, v, s);
         std::vector<double> each;
         const int v = dg::autotune_gather(plan->gather, d_frames, dtype,
                                           int64_t(plan->dim1) * plan->dim2, n_frames, flags, s,
@@ -687,7 +687,7 @@ dg_status dg_plan_variant(dg_plan *plan, int32_t set, int32_t *current, int32_t 
             dg::fail(DG_INVALID_INPUT, "gather mapping " + std::to_string(set) + " does not exist");
         if (set >= 0 && dg::gather_variant_needs_tiles(set)) {
             DeviceScope scope(plan->device);
-            dg::ensure_bin_tiles(plan->gather, plan->table, plan->stream);
+            dg::ensure_bin_tiles(plan->gather, plan->table, set, plan->stream);
         }
         if (set >= 0 && !dg::gather_variant_available(plan->gather, set))
             dg::fail(DG_UNSUPPORTED, "gather mapping " + std::to_string(set) +

@@ -55,8 +55,9 @@ constexpr int kFlush = 16;  // terms per lane between double-word folds
 // lane per step): 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2);
 // frame-lane mappings (k_gather_fl), 2 CTAs per SM (5) or 1 CTA per SM with
 // the next frames prefetched while the current ones are summed (6); bin
-// tiles (k_gather_bins, 7), which write the results themselves.
-constexpr int kVariantCount = 8;
+// tiles (k_gather_bins: 7, one frame per lane; 8, two), which write the
+// results themselves.
+constexpr int kVariantCount = 9;
 constexpr int kSegMax = 256;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
@@ -954,51 +955,68 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
-// Bin-tile gather (mapping 7). A tile is kBtRows consecutive rows (bins) of the
-// table and 32 frames (lane = frame). The tile's entries, merged over its rows
-// in pixel order, are cut into chunks of at most kBtDCap distinct pixels and
-// kBtPCap entry pairs; a row's entries inside a chunk are a contiguous run of
-// its CSR row. The CTA walks the tile's chunks in order with three buffers:
-// while chunk k is summed, chunk k+2's pixels (4-byte cp.async into frame rows
-// kBtStride words apart) and entry pairs (16-byte cp.async) are in flight;
-// one barrier per chunk. Warp w owns row w of the tile and keeps its sums in
-// registers for the whole tile (double-word FP32, folded
-// every kFlFlushPairs pairs of the row), then normalises and writes the
-// results itself: no partial sums, no finalize launch. Every row is summed in
-// the same order for every frame and batch.
+// Bin-tile gathers (mappings 7 and 8). A tile is ROWS consecutive rows
+// (bins) of the table and 32 * F2 frames (lane = frame; F2 frames per lane,
+// 32 apart). The tile's entries, merged over its rows in pixel order, are cut
+// into chunks of at most DCap distinct pixels and PCap entry pairs; a row's
+// entries inside a chunk are a contiguous run of its CSR row. The CTA walks
+// the tile's chunks in order with three buffers: while chunk k is summed,
+// chunk k+2's pixels (4-byte cp.async into frame rows Stride words apart) and
+// entry pairs (16-byte cp.async) are in flight; one barrier per chunk. Warp
+// w owns row w of the tile and keeps its sums in registers for the whole tile
+// (double-word FP32, folded every kFlFlushPairs pairs of the row), then
+// normalises and writes the results itself: no partial sums, no finalize
+// launch. Every row is summed in the same order for every frame and batch.
+// With two frames per lane (mapping 8) every entry pair read from shared
+// memory serves 64 frames: half the broadcast reads per frame, at half the
+// chunk size.
 
-#ifndef DG_BT_ROWS
-#define DG_BT_ROWS 24
-#endif
-constexpr int kBtRows = DG_BT_ROWS;      // rows per tile
-constexpr int kBtWarps = kBtRows;        // warps per CTA; warp w owns row w
-constexpr int kBtDCap = 384;             // distinct pixels per chunk
-constexpr int kBtStride = kBtDCap + 1;   // odd frame-row stride; column kBtDCap stays 0
-constexpr int kBtPCap = 640;             // entry pairs per chunk
 constexpr int kBtBufs = 3;
-// Per-chunk record, fixed size: {pixels D, pairs, first pair, 0}, the rows'
-// pair offsets (kBtRows + 1, padded to a multiple of 4 words), then D pixel
-// indices.
-constexpr int kBtMetaHead = (4 + kBtRows + 1 + 3) / 4 * 4;
-constexpr int kBtMetaWords = kBtMetaHead + kBtDCap;  // 408 words, 1632 bytes
 constexpr int kBtMetaBufs = 5;
-static_assert(kBtMetaWords % 4 == 0, "records are copied in 16-byte pieces");
-static_assert(kBtRows + 1 <= kBtMetaHead - 4, "row offsets fit the record head");
-static_assert(kBtRows <= 32, "tile rows are packed in 5 bits at plan time");
-static_assert(kBtRows == kBtWarps, "a warp owns one row of a tile");
+
+// One bin-tile layout: rows per tile (= warps per CTA: warp w owns row w),
+// chunk capacities, frames per lane and pairs per unrolled step. Per-chunk
+// record, fixed size: {pixels D, pairs, first pair, 0}, the rows' pair
+// offsets (ROWS + 1, padded to a multiple of 4 words), then D pixel indices.
+template <int ROWS, int DCAP, int PCAP, int F2, int U2>
+struct BtCfg {
+    static constexpr int kRows = ROWS;
+    static constexpr int kThreads = ROWS * 32;
+    static constexpr int kU2 = U2;
+    static_assert(ROWS <= 32, "tile rows are packed in 5 bits at plan time");
+    static constexpr int kDCap = DCAP;          // distinct pixels per chunk
+    static constexpr int kStride = DCAP + 1;    // odd frame-row stride; column DCAP stays 0
+    static constexpr int kPCap = PCAP;          // entry pairs per chunk
+    static constexpr int kF2 = F2;              // frames per lane
+    static constexpr int kFrames = 32 * F2;     // frames per CTA
+    static constexpr int kMetaHead = (4 + ROWS + 1 + 3) / 4 * 4;
+    static constexpr int kMetaWords = kMetaHead + DCAP;
+    static_assert(kMetaWords % 4 == 0, "records are copied in 16-byte pieces");
+    static_assert(kStride % 2 == 1, "frame rows must start in different banks");
+    template <int MODE>
+    static constexpr size_t buf_bytes() {
+        return size_t(kFrames) * kStride * 4 + size_t(PCAP) * (MODE == kSpread ? 32 : 16);
+    }
+    template <int MODE>
+    static constexpr size_t smem_bytes() {
+        return size_t(kBtBufs) * buf_bytes<MODE>() + size_t(kBtMetaBufs) * kMetaWords * 4;
+    }
+};
+#ifndef DG_BT8_ROWS
+#define DG_BT8_ROWS 16
+#endif
+using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
+using Bt8 = BtCfg<DG_BT8_ROWS, 192, 320, 2, (DG_BT8_ROWS > 16 ? 2 : 4)>;  // mapping 8
+static_assert(Bt7::smem_bytes<kSpread>() <= 227 * 1024, "mapping 7 fits shared memory");
+static_assert(Bt8::smem_bytes<kSpread>() <= 227 * 1024, "mapping 8 fits shared memory");
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-template <int MODE, typename P>
-constexpr size_t bt_buf_bytes() {
-    return size_t(32) * kBtStride * 4 + size_t(kBtPCap) * (MODE == kSpread ? 32 : 16);
-}
-
-template <int MODE, typename P, int U2>
-__global__ void __launch_bounds__(kBtWarps * 32, 1)
+template <int MODE, typename P, class CFG>
+__global__ void __launch_bounds__(CFG::kThreads, 1)
     k_gather_bins(const int4 *__restrict__ items, const int32_t *__restrict__ meta,
                   const float4 *__restrict__ pair_a, const float4 *__restrict__ pair_b,
                   const int4 *__restrict__ org, const float4 *__restrict__ entry_std,
@@ -1010,34 +1028,38 @@ __global__ void __launch_bounds__(kBtWarps * 32, 1)
     using S = StagedPx<P>;
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
-    constexpr size_t BUF = bt_buf_bytes<MODE, P>();
+    constexpr int F2 = CFG::kF2, STRIDE = CFG::kStride, DCAP = CFG::kDCap, PCAP = CFG::kPCap;
+    constexpr int U2 = CFG::kU2, NT = CFG::kThreads;
+    constexpr int MH = CFG::kMetaHead, MW = CFG::kMetaWords;
+    constexpr size_t BUF = CFG::template buf_bytes<MODE>();
     extern __shared__ __align__(16) unsigned char smem[];
-    const int groups = (n_frames + 31) / 32;
+    const int groups = (n_frames + CFG::kFrames - 1) / CFG::kFrames;
     const int4 it = items[blockIdx.x / groups];
-    const int f0 = (blockIdx.x % groups) * 32, nv = min(32, n_frames - f0);
+    const int f0 = (blockIdx.x % groups) * CFG::kFrames;
+    const int nv = min(CFG::kFrames, n_frames - f0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int row0 = it.x, nrows = it.y, ch0 = it.z, nch = it.w;
 
     auto pxbuf = [&](int b) { return reinterpret_cast<S *>(smem + size_t(b) * BUF); };
     auto pabuf = [&](int b) {
-        return reinterpret_cast<float4 *>(smem + size_t(b) * BUF + size_t(32) * kBtStride * 4);
+        return reinterpret_cast<float4 *>(smem + size_t(b) * BUF +
+                                          size_t(CFG::kFrames) * STRIDE * 4);
     };
     auto mbuf = [&](int c) {
-        return reinterpret_cast<int32_t *>(smem + size_t(kBtBufs) * BUF) +
-               (c % kBtMetaBufs) * kBtMetaWords;
+        return reinterpret_cast<int32_t *>(smem + size_t(kBtBufs) * BUF) + (c % kBtMetaBufs) * MW;
     };
     // Copy chunk c's record into its record buffer (part of the open group).
     auto stage_meta = [&](int c) {
         if (c < nch) {
-            const int4 *src = reinterpret_cast<const int4 *>(meta + int64_t(ch0 + c) * kBtMetaWords);
+            const int4 *src = reinterpret_cast<const int4 *>(meta + int64_t(ch0 + c) * MW);
             int4 *dst = reinterpret_cast<int4 *>(mbuf(c));
-            for (int j = tid; j < kBtMetaWords / 4; j += kBtWarps * 32) cp_async16(dst + j, src + j);
+            for (int j = tid; j < MW / 4; j += NT) cp_async16(dst + j, src + j);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    // Column kBtDCap of every frame row is read by padding pairs and holds 0.
-    for (int j = tid; j < kBtBufs * 32; j += kBtWarps * 32)
-        pxbuf(j / 32)[(j % 32) * kBtStride + kBtDCap] = S(0);
+    // Column DCAP of every frame row is read by padding pairs and holds 0.
+    for (int j = tid; j < kBtBufs * CFG::kFrames; j += NT)
+        pxbuf(j / CFG::kFrames)[(j % CFG::kFrames) * STRIDE + DCAP] = S(0);
 
     // Stage chunk c (of this tile) into buffer b as one commit group; its
     // record is in shared memory already.
@@ -1047,35 +1069,40 @@ __global__ void __launch_bounds__(kBtWarps * 32, 1)
             const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
             S *dst = pxbuf(b);
             const P *base = frames + int64_t(f0) * n_pixels;
-            for (int k = tid; k < ch.y; k += kBtWarps * 32) {
-                const P *src = base + mb[kBtMetaHead + k];
+            for (int k = tid; k < ch.y; k += NT) {
+                const P *src = base + mb[MH + k];
                 if constexpr (sizeof(P) == 4) {
 #pragma unroll 8
                     for (int f = 0; f < nv; ++f)
-                        cp_async4(dst + f * kBtStride + k, src + int64_t(f) * n_pixels);
+                        cp_async4(dst + f * STRIDE + k, src + int64_t(f) * n_pixels);
                 } else {
 #pragma unroll 8
                     for (int f = 0; f < nv; ++f)
-                        dst[f * kBtStride + k] = load_px<P>(src + int64_t(f) * n_pixels, 0u);
+                        dst[f * STRIDE + k] = load_px<P>(src + int64_t(f) * n_pixels, 0u);
                 }
             }
             float4 *pa = pabuf(b);
-            for (int j = tid; j < ch.w; j += kBtWarps * 32) {
+            for (int j = tid; j < ch.w; j += NT) {
                 cp_async16(pa + j, pair_a + ch.z + j);
-                if (SPREAD) cp_async16(pa + kBtPCap + j, pair_b + ch.z + j);
+                if (SPREAD) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
             }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
 
-    // This warp's row: accumulators, fold counter, origin.
-    Acc2 acc0[NA];
+    // This warp's row: accumulators, fold counter and origin of each of the
+    // lane's frames.
+    Acc2 acc[F2][NA];
 #pragma unroll
-    for (int a = 0; a < NA; ++a) acc0[a].zero();
-    int since0 = 0;
-    float org0 = 0.f;
-    const int ra = warp;  // row of the tile
-    const int4 oa = ra < nrows ? org[row0 + ra] : make_int4(-1, 0, -1, 0);
+    for (int h = 0; h < F2; ++h)
+#pragma unroll
+        for (int a = 0; a < NA; ++a) acc[h][a].zero();
+    int since = 0;
+    float orgv[F2];
+#pragma unroll
+    for (int h = 0; h < F2; ++h) orgv[h] = 0.f;
+    const int r = warp;  // row of the tile
+    const int4 o = r < nrows ? org[row0 + r] : make_int4(-1, 0, -1, 0);
 
     // Pipeline: records two chunks ahead of their pixels, pixels two chunks
     // ahead of their sums; commit order M0 M1 | P0 M2 P1 M3 | P2 M4 | P3 M5 ...
@@ -1093,42 +1120,49 @@ __global__ void __launch_bounds__(kBtWarps * 32, 1)
         __syncthreads();
         stage(c + 2, (c + 2) % kBtBufs);
         stage_meta(c + 4);
+        if (r >= nrows) continue;
         const int b = c % kBtBufs;
-        const S *px = pxbuf(b) + lane * kBtStride;
+        const S *px[F2];
+#pragma unroll
+        for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + (lane + 32 * h) * STRIDE;
         const float4 *s_pa = pabuf(b);
-        const float4 *s_pb = s_pa + kBtPCap;
+        const float4 *s_pb = s_pa + PCAP;
         const int32_t *cp = mbuf(c) + 4;
-
-        auto run_row = [&](int r, const int4 &o, Acc2 *acc, int &since, float &orgv) {
-            if (r >= nrows) return;
-            if constexpr (SPREAD) {
-                if (o.x == c) {
-                    // Origin o = s/n of the row's first valid entry (row_origin):
-                    // its pixel is in this chunk; a non-finite float pixel there
-                    // sends the lane to the row's next entries in global memory.
-                    const float so = float(px[o.y]);
-                    orgv = __fdiv_rn(so, entry_std[o.z].z);
+        if constexpr (SPREAD) {
+            if (o.x == c) {
+                // Origin o = s/n of the row's first valid entry (row_origin):
+                // its pixel is in this chunk; a non-finite float pixel there
+                // sends the lane to the row's next entries in global memory.
+#pragma unroll
+                for (int h = 0; h < F2; ++h) {
+                    const float so = float(px[h][o.y]);
+                    orgv[h] = __fdiv_rn(so, entry_std[o.z].z);
                     if (is_float_px<P>() && !isfinite(so)) {
-                        const int fi = min(f0 + lane, n_frames - 1);
-                        orgv = row_origin<P>(entry_std, o.z, o.w, frames + int64_t(fi) * n_pixels);
+                        const int fi = min(f0 + lane + 32 * h, n_frames - 1);
+                        orgv[h] = row_origin<P>(entry_std, o.z, o.w, frames + int64_t(fi) * n_pixels);
                     }
                 }
             }
-            const f2 norg = pk(-orgv, -orgv);
-            const int p0 = cp[r], p1 = cp[r + 1];
-            auto body = [&](int p, auto unroll) {
-                constexpr int UU = decltype(unroll)::value;
-                float4 ea[UU], eb[UU];
+        }
+        f2 norg[F2];
 #pragma unroll
-                for (int u = 0; u < UU; ++u) {
-                    ea[u] = s_pa[p + u];
-                    if constexpr (SPREAD) eb[u] = s_pb[p + u];
-                }
+        for (int h = 0; h < F2; ++h) norg[h] = pk(-orgv[h], -orgv[h]);
+        const int p0 = cp[r], p1 = cp[r + 1];
+        auto body = [&](int p, auto unroll) {
+            constexpr int UU = decltype(unroll)::value;
+            float4 ea[UU], eb[UU];
+#pragma unroll
+            for (int u = 0; u < UU; ++u) {
+                ea[u] = s_pa[p + u];
+                if constexpr (SPREAD) eb[u] = s_pb[p + u];
+            }
+#pragma unroll
+            for (int h = 0; h < F2; ++h) {
                 float v0[UU], v1[UU];
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
-                    v0[u] = float(px[__float_as_int(ea[u].x)]);
-                    v1[u] = float(px[__float_as_int(ea[u].y)]);
+                    v0[u] = float(px[h][__float_as_int(ea[u].x)]);
+                    v1[u] = float(px[h][__float_as_int(ea[u].y)]);
                 }
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
@@ -1140,105 +1174,110 @@ __global__ void __launch_bounds__(kBtWarps * 32, 1)
                             const f2 ce = pk(ok0 ? ea[u].z : 0.f, ok1 ? ea[u].w : 0.f);
                             const f2 x = pk(x0, x1), n = pk(eb[u].x, eb[u].y);
                             const f2 cre = pk(ok0 ? eb[u].z : 0.f, ok1 ? eb[u].w : 0.f);
-                            acc[0].p = fma2(ce, x, acc[0].p);
-                            acc[1].p = fma2(mul2(ce, ce), pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f)),
-                                            acc[1].p);
-                            const f2 t = fma2(norg, n, x);
-                            acc[2].p = fma2(mul2(cre, t), t, acc[2].p);
-                            acc[NA - 2].p = add2(acc[NA - 2].p,
-                                                 pk(ok0 ? 0.f : __fmul_rn(ea[u].z, eb[u].x),
-                                                    ok1 ? 0.f : __fmul_rn(ea[u].w, eb[u].y)));
-                            acc[NA - 1].p = add2(acc[NA - 1].p,
-                                                 pk(!ok0 && ea[u].z > 0.f ? 1.f : 0.f,
-                                                    !ok1 && ea[u].w > 0.f ? 1.f : 0.f));
+                            acc[h][0].p = fma2(ce, x, acc[h][0].p);
+                            acc[h][1].p = fma2(mul2(ce, ce), pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f)),
+                                               acc[h][1].p);
+                            const f2 t = fma2(norg[h], n, x);
+                            acc[h][2].p = fma2(mul2(cre, t), t, acc[h][2].p);
+                            acc[h][NA - 2].p = add2(acc[h][NA - 2].p,
+                                                    pk(ok0 ? 0.f : __fmul_rn(ea[u].z, eb[u].x),
+                                                       ok1 ? 0.f : __fmul_rn(ea[u].w, eb[u].y)));
+                            acc[h][NA - 1].p = add2(acc[h][NA - 1].p,
+                                                    pk(!ok0 && ea[u].z > 0.f ? 1.f : 0.f,
+                                                       !ok1 && ea[u].w > 0.f ? 1.f : 0.f));
                             continue;
                         }
                     }
                     const f2 x = pk(v0[u], v1[u]);
-                    acc[0].p = fma2(cc, x, acc[0].p);
+                    acc[h][0].p = fma2(cc, x, acc[h][0].p);
                     if constexpr (MODE != kIntensity) {
                         const f2 xp = is_unsigned_px<P>()
                                           ? x
                                           : pk(fmaxf(v0[u], 0.f), fmaxf(v1[u], 0.f));
-                        acc[1].p = fma2(mul2(cc, cc), xp, acc[1].p);
+                        acc[h][1].p = fma2(mul2(cc, cc), xp, acc[h][1].p);
                     }
                     if constexpr (SPREAD) {
                         const f2 n = pk(eb[u].x, eb[u].y), cr = pk(eb[u].z, eb[u].w);
-                        const f2 t = fma2(norg, n, x);
-                        acc[2].p = fma2(mul2(cr, t), t, acc[2].p);
+                        const f2 t = fma2(norg[h], n, x);
+                        acc[h][2].p = fma2(mul2(cr, t), t, acc[h][2].p);
                     }
-                }
-            };
-            int p = p0;
-            for (; p + U2 <= p1; p += U2) {
-                body(p, std::integral_constant<int, U2>{});
-                since += U2;
-                if (since >= kFlFlushPairs) {
-                    since = 0;
-#pragma unroll
-                    for (int a = 0; a < NA; ++a) acc[a].flush();
-                }
-            }
-            for (; p < p1; ++p) {
-                body(p, std::integral_constant<int, 1>{});
-                if (++since >= kFlFlushPairs) {
-                    since = 0;
-#pragma unroll
-                    for (int a = 0; a < NA; ++a) acc[a].flush();
                 }
             }
         };
-        run_row(ra, oa, acc0, since0, org0);
+        auto fold = [&]() {
+#pragma unroll
+            for (int h = 0; h < F2; ++h)
+#pragma unroll
+                for (int a = 0; a < NA; ++a) acc[h][a].flush();
+        };
+        int p = p0;
+        for (; p + U2 <= p1; p += U2) {
+            body(p, std::integral_constant<int, U2>{});
+            since += U2;
+            if (since >= kFlFlushPairs) {
+                since = 0;
+                fold();
+            }
+        }
+        for (; p < p1; ++p) {
+            body(p, std::integral_constant<int, 1>{});
+            if (++since >= kFlFlushPairs) {
+                since = 0;
+                fold();
+            }
+        }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (r >= nrows) return;
 
     // Normalise (normalize_bin, prepared.rs:985-996; the spread's closing
     // formulas, azimuthal.rs:96-104), as k_finalize does from partial sums.
-    auto finish = [&](int rl, Acc2 *acc, float orgv) {
-        if (rl >= nrows || lane >= nv) return;
-        const int r = row0 + rl;
+#pragma unroll
+    for (int h = 0; h < F2; ++h) {
+        const int fl = lane + 32 * h;
+        if (fl >= nv) continue;
+        const int row = row0 + r;
         double v[NA];
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
-            acc[a].flush();
-            v[a] = acc[a].value();
+            acc[h][a].flush();
+            v[a] = acc[h][a].value();
         }
-        const int64_t o = int64_t(f0 + lane) * n_rows + r;
+        const int64_t oo = int64_t(f0 + fl) * n_rows + row;
         if constexpr (!SPREAD) {
-            const double n = den[r];
-            out_i[o] = n == 0.0 ? 0.0 : v[0] / n;
+            const double n = den[row];
+            out_i[oo] = n == 0.0 ? 0.0 : v[0] / n;
             if (MODE == kErrors) {
                 const double q = n == 0.0 ? 0.0 : v[1] / (n * n);
-                out_s[o] = sqrt(q > 0.0 ? q : 0.0);
+                out_s[oo] = sqrt(q > 0.0 ? q : 0.0);
             }
         } else {
-            int valid = valid_std[r];
-            double sw = den_std[r], wf = den_f32[r];
+            int valid = valid_std[row];
+            double sw = den_std[row], wf = den_f32[row];
             if (NA == 5) {
                 valid -= int(v[NA - 1] + 0.5);
                 sw -= v[NA - 2];
                 wf -= v[NA - 2];
             }
             if (valid <= 0 || !(sw > 0.0)) {
-                out_i[o] = 0.0;
-                if (out_s) out_s[o] = 0.0;
-                out_d[o] = __longlong_as_double(0x7ff8000000000000ll);
-                return;
+                out_i[oo] = 0.0;
+                if (out_s) out_s[oo] = 0.0;
+                out_d[oo] = __longlong_as_double(0x7ff8000000000000ll);
+                continue;
             }
-            const double a1 = v[0] - double(orgv) * wf;
-            out_i[o] = v[0] / sw;
-            if (out_s) out_s[o] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
+            const double a1 = v[0] - double(orgv[h]) * wf;
+            out_i[oo] = v[0] / sw;
+            if (out_s) out_s[oo] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
             const double mean = a1 / sw;
             const double m2 = v[2] - mean * a1;
             const double q = m2 / sw;
-            out_d[o] = sqrt(q > 0.0 ? q : 0.0);
+            out_d[oo] = sqrt(q > 0.0 ? q : 0.0);
         }
-    };
-    finish(ra, acc0, org0);
+    }
 }
 
 // Bin-tile entry pairs from the plan-time layout: per pair {slot 0, slot 1,
-// entry 0, entry 1} (entry -1: padding, slot kBtDCap) to A {slot 0, slot 1,
+// entry 0, entry 1} (entry -1: padding, slot = the zero column) to A {slot 0, slot 1,
 // c0, c1} with the table's FP32 weights, AS the same with the spread's
 // weights, B {n0, n1, c0/n0, c1/n1}.
 __global__ void k_bt_fill(const int4 *__restrict__ desc, int64_t n_pairs,
@@ -1458,26 +1497,24 @@ void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, doub
 
 // Launches lane-mapping variant `variant` of the gather (kVariantCount) with
 // its partial sums in `partial`.
-template <int MODE, typename P>
-void launch_bins(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, double *oi,
-                 double *os, double *od, cudaStream_t s) {
-    constexpr size_t smem =
-        size_t(kBtBufs) * bt_buf_bytes<MODE, P>() + size_t(kBtMetaBufs) * kBtMetaWords * 4;
-    auto kern = k_gather_bins<MODE, P, (kBtRows > 24 ? 2 : 4)>;
+template <int MODE, typename P, class CFG>
+void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t n_pixels, int nf,
+                 double *oi, double *os, double *od, cudaStream_t s) {
+    constexpr size_t smem = CFG::template smem_bytes<MODE>();
+    auto kern = k_gather_bins<MODE, P, CFG>;
     DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    const int groups = (nf + 31) / 32;
-    const int64_t grid = int64_t(t.bt_n_items) * groups;
+    const int groups = (nf + CFG::kFrames - 1) / CFG::kFrames;
+    const int64_t grid = int64_t(bt.n_items) * groups;
     if (grid > INT32_MAX) fail(DG_UNSUPPORTED, "too many bin tiles for one launch");
-    kern<<<unsigned(grid), kBtWarps * 32, smem, s>>>(
-        t.bt_item.ptr, t.bt_meta.ptr,
-        MODE == kSpread ? t.bt_pair_as.ptr : t.bt_pair_a.ptr, t.bt_pair_b.ptr, t.bt_org.ptr,
-        t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr, t.valid_std.ptr, fp, n_pixels,
-        nf, t.n_rows, oi, os, od);
+    kern<<<unsigned(grid), CFG::kThreads, smem, s>>>(
+        bt.item.ptr, bt.meta.ptr, MODE == kSpread ? bt.pair_as.ptr : bt.pair_a.ptr,
+        bt.pair_b.ptr, bt.org.ptr, t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr,
+        t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od);
 }
 
 // Launches lane mapping `variant`; returns true when the kernel wrote the
-// normalised results to oi/os/od itself (mapping 7), false when it left
-// partial sums for k_finalize. Mapping 7 needs the outputs; callers without
+// normalised results to oi/os/od itself (mappings 7, 8), false when it left
+// partial sums for k_finalize. Those mappings need the outputs; callers without
 // them (raw sums) get the frame-lane or an entry-lane mapping instead.
 template <int MODE, typename P>
 bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pixels, int nf,
@@ -1487,9 +1524,11 @@ bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pix
     if constexpr (MODE == kRaw) {
         if (variant >= 5) variant = 2;  // entry-lane mappings only
     } else {
-        if (variant == 7) {
-            if (oi && t.bt_n_items > 0) {
-                launch_bins<MODE, P>(t, fp, n_pixels, nf, oi, os, od, s);
+        if (variant == 7 || variant == 8) {
+            const BinTiles &bt = t.bt[variant - 7];
+            if (oi && bt.n_items > 0) {
+                if (variant == 7) launch_bins<MODE, P, Bt7>(t, bt, fp, n_pixels, nf, oi, os, od, s);
+                else launch_bins<MODE, P, Bt8>(t, bt, fp, n_pixels, nf, oi, os, od, s);
                 DG_CUDA(cudaGetLastError());
                 return true;
             }
@@ -1665,21 +1704,24 @@ void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<
 }
 
 // Bin tiles (k_gather_bins) at plan time, on the host: for every run of
-// kBtRows rows, the rows' entries merged in pixel order and cut into chunks of
+// CFG::kRows rows, the rows' entries merged in pixel order and cut into chunks of
 // at most kBtDCap distinct pixels and kBtPCap pairs (a new pixel that would
 // exceed either opens the next chunk, so a chunk is a pixel-index interval
 // and each row's entries in it are a contiguous run of its CSR row). Tiles
 // are ordered largest first. Each row's origin (its first entry valid for the
 // spread) is located as {chunk within the tile, slot}.
-void build_bin_tiles(GatherTable &out, const DeviceCsr &table, cudaStream_t s) {
+template <class CFG>
+void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cudaStream_t s) {
+    constexpr int kBtDCap = CFG::kDCap, kBtPCap = CFG::kPCap, kBtRows = CFG::kRows;
+    constexpr int kBtMetaHead = CFG::kMetaHead, kBtMetaWords = CFG::kMetaWords;
     const int64_t nb = table.n_rows;
-    out.bt_n_items = 0;
+    out.n_items = 0;
     if (nb == 0 || table.nnz == 0) return;
     std::vector<int64_t> rp(static_cast<size_t>(nb) + 1);
     DG_CUDA(cudaMemcpyAsync(rp.data(), table.row_ptr.ptr, rp.size() * 8, cudaMemcpyDeviceToHost, s));
     std::vector<int32_t> col(static_cast<size_t>(table.nnz)), fv(static_cast<size_t>(nb));
     DG_CUDA(cudaMemcpyAsync(col.data(), table.col.ptr, col.size() * 4, cudaMemcpyDeviceToHost, s));
-    DG_CUDA(cudaMemcpyAsync(fv.data(), out.first_valid.ptr, fv.size() * 4, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaMemcpyAsync(fv.data(), gt.first_valid.ptr, fv.size() * 4, cudaMemcpyDeviceToHost, s));
     DG_CUDA(cudaStreamSynchronize(s));
     const int64_t n_items = (nb + kBtRows - 1) / kBtRows;
     struct Tile {
@@ -1841,50 +1883,62 @@ void build_bin_tiles(GatherTable &out, const DeviceCsr &table, cudaStream_t s) {
         T = Tile();
     };
     parallel(flatten);
-    out.bt_n_items = int32_t(items.size());
-    out.bt_item.alloc(items.size());
-    out.bt_meta.alloc(std::max<size_t>(n_chunks * kBtMetaWords, 1));
-    out.bt_org.alloc(org.size());
-    out.bt_pair_a.alloc(std::max<size_t>(n_pairs, 1));
-    out.bt_pair_as.alloc(std::max<size_t>(n_pairs, 1));
-    out.bt_pair_b.alloc(std::max<size_t>(n_pairs, 1));
+    out.n_items = int32_t(items.size());
+    out.item.alloc(items.size());
+    out.meta.alloc(std::max<size_t>(n_chunks * kBtMetaWords, 1));
+    out.org.alloc(org.size());
+    out.pair_a.alloc(std::max<size_t>(n_pairs, 1));
+    out.pair_as.alloc(std::max<size_t>(n_pairs, 1));
+    out.pair_b.alloc(std::max<size_t>(n_pairs, 1));
     DeviceArray<int4> desc;
     desc.alloc(std::max<size_t>(n_pairs, 1));
-    DG_CUDA(cudaMemcpyAsync(out.bt_item.ptr, items.data(), items.size() * sizeof(int4),
+    DG_CUDA(cudaMemcpyAsync(out.item.ptr, items.data(), items.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, s));
     if (n_chunks)
-        DG_CUDA(cudaMemcpyAsync(out.bt_meta.ptr, meta.get(), n_chunks * kBtMetaWords * 4,
+        DG_CUDA(cudaMemcpyAsync(out.meta.ptr, meta.get(), n_chunks * kBtMetaWords * 4,
                                 cudaMemcpyHostToDevice, s));
-    DG_CUDA(cudaMemcpyAsync(out.bt_org.ptr, org.data(), org.size() * sizeof(int4),
+    DG_CUDA(cudaMemcpyAsync(out.org.ptr, org.data(), org.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, s));
     if (n_pairs) {
         DG_CUDA(cudaMemcpyAsync(desc.ptr, pairs.get(), n_pairs * sizeof(int4),
                                 cudaMemcpyHostToDevice, s));
-        k_bt_fill<<<148 * 8, 256, 0, s>>>(desc.ptr, int64_t(n_pairs), out.entry.ptr,
-                                         out.entry_std.ptr, out.bt_pair_a.ptr, out.bt_pair_as.ptr,
-                                         out.bt_pair_b.ptr);
+        k_bt_fill<<<148 * 8, 256, 0, s>>>(desc.ptr, int64_t(n_pairs), gt.entry.ptr,
+                                         gt.entry_std.ptr, out.pair_a.ptr, out.pair_as.ptr,
+                                         out.pair_b.ptr);
         DG_CUDA(cudaGetLastError());
     }
     DG_CUDA(cudaStreamSynchronize(s));
 }
 
 namespace {
-__global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int rows, int cols);
+__global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int words, int head,
+                            int rows, int cols);
 }  // namespace
 
-void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, cudaStream_t s) {
-    if (t.bt_built) return;
-    build_bin_tiles(t, table, s);
-    if (t.flip_rows && t.bt_n_items > 0) {
-        k_flip_meta<<<148 * 4, 256, 0, s>>>(t.bt_meta.ptr, int64_t(t.bt_meta.count) / kBtMetaWords,
-                                            t.flip_rows, t.flip_cols);
+void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, int variant, cudaStream_t s) {
+    if (variant != 7 && variant != 8) return;
+    BinTiles &bt = t.bt[variant - 7];
+    if (bt.built) return;
+    int words = 0, head = 0;
+    if (variant == 7) {
+        build_bin_tiles<Bt7>(t, bt, table, s);
+        words = Bt7::kMetaWords;
+        head = Bt7::kMetaHead;
+    } else {
+        build_bin_tiles<Bt8>(t, bt, table, s);
+        words = Bt8::kMetaWords;
+        head = Bt8::kMetaHead;
+    }
+    if (t.flip_rows && bt.n_items > 0) {
+        k_flip_meta<<<148 * 4, 256, 0, s>>>(bt.meta.ptr, int64_t(bt.meta.count) / words, words,
+                                            head, t.flip_rows, t.flip_cols);
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaStreamSynchronize(s));
     }
-    t.bt_built = true;
+    bt.built = true;
 }
 
-bool gather_variant_needs_tiles(int variant) { return variant == 7; }
+bool gather_variant_needs_tiles(int variant) { return variant == 7 || variant == 8; }
 
 void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1, int32_t dim2,
                        int32_t strip_rows, cudaStream_t s, GatherTable &out) {
@@ -2070,12 +2124,13 @@ __global__ void k_flip_rows(int2 *__restrict__ entry, float4 *__restrict__ entry
 }
 
 // The same for the pixel indices of bin-tile chunk records (D of them each).
-__global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int rows, int cols) {
+__global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int words, int head,
+                            int rows, int cols) {
     for (int64_t r = blockIdx.x; r < n_rec; r += gridDim.x) {
-        int32_t *rec = meta + r * kBtMetaWords;
+        int32_t *rec = meta + r * words;
         const int d = rec[0];
         for (int k = threadIdx.x; k < d; k += blockDim.x)
-            rec[kBtMetaHead + k] = flip_px(rec[kBtMetaHead + k], rows, cols);
+            rec[head + k] = flip_px(rec[head + k], rows, cols);
     }
 }
 
@@ -2205,7 +2260,7 @@ int gather_variant_count() { return kVariantCount; }
 bool gather_variant_available(const GatherTable &t, int variant) {
     if (variant < 0 || variant >= kVariantCount) return false;
     if (variant == 5 || variant == 6) return t.fl_n_units > 0;
-    if (variant == 7) return t.bt_n_items > 0;
+    if (variant == 7 || variant == 8) return t.bt[variant - 7].n_items > 0;
     return true;
 }
 

@@ -148,6 +148,21 @@ struct EventPool {
     }
 };
 
+// One bin-tile layout (dg_gather.cu): runs of rows whose entries are cut
+// into pixel-interval chunks, built on first use.
+struct BinTiles {
+    bool built = false;
+    int32_t n_items = 0;
+    DeviceArray<int4> item;        // {first row, rows, first chunk, chunks}, largest first
+    DeviceArray<int32_t> meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
+    DeviceArray<int4> org;         // per row {chunk in tile (-1: none), slot, entry, row end}
+    DeviceArray<float4> pair_a, pair_as, pair_b;
+    int64_t bytes() const {
+        return int64_t(item.bytes() + meta.bytes() + org.bytes() + pair_a.bytes() +
+                       pair_as.bytes() + pair_b.bytes());
+    }
+};
+
 // Gather-side table (dg_gather.cu). The masked table is cut into segments,
 // each a run of one row's entries whose pixels lie in one strip of detector
 // rows; segments of the same strip and neighbouring rows are grouped into
@@ -186,14 +201,8 @@ struct GatherTable {
     // {pixel bits, w, w*norm, 0} per entry and the FP64 weight sum per row.
     DeviceArray<float4> entry_raw;
     DeviceArray<double> cnt;
-    // Bin tiles (k_gather_bins): runs of 16 rows, their entries cut into
-    // pixel-interval chunks; see dg_gather.cu.
-    bool bt_built = false;            // built on first use (ensure_bin_tiles)
-    int32_t bt_n_items = 0;
-    DeviceArray<int4> bt_item;        // {first row, rows, first chunk, chunks}, largest first
-    DeviceArray<int32_t> bt_meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
-    DeviceArray<int4> bt_org;         // per row {chunk in tile (-1: none), slot, entry, row end}
-    DeviceArray<float4> bt_pair_a, bt_pair_as, bt_pair_b;
+    // Bin tiles (k_gather_bins), mappings 7 and 8; see dg_gather.cu.
+    BinTiles bt[2];
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     int32_t flip_rows = 0, flip_cols = 0;  // frames stored bottom row first (0: detector order)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
@@ -223,9 +232,9 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
 // InputOrder::FlipVertical: remaps the pixel indices of a built gather table
 // to frames whose rows come in reverse order (entry order unchanged).
 void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s);
-// Bin tiles for lane mapping 7, built from the plan's masked table on first
-// use (the autotuner, or selecting the mapping); idempotent.
-void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, cudaStream_t s);
+// Bin tiles of lane mapping `variant` (7 or 8), built from the plan's masked
+// table on first use (the autotuner, or selecting the mapping); idempotent.
+void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, int variant, cudaStream_t s);
 bool gather_variant_needs_tiles(int variant);
 // The autotuner times the bin-tile mapping only for batches of more frames
 // than this (one tile per CTA: smaller batches leave SMs idle).

@@ -1,5 +1,12 @@
 // Per-frame gather: CSR (bins x pixels) times a stack of frames.
 //
+// Three families of lane mappings, chosen per plan by timing (the
+// autotuner): entry-lane units (k_gather, mappings 0-4, described first
+// below), frame-lane units (k_gather_fl, 5-6) and bin tiles (k_gather_bins,
+// 7-8). The first two leave per-segment partial sums that k_finalize folds;
+// the bin tiles keep each bin's sums in registers for the whole batch and
+// write the results themselves.
+//
 // Layout. The masked table is cut into segments: a segment is a run of one
 // row's entries whose pixels lie in one strip of `strip_rows` detector rows
 // (rows list pixels in ascending order, so this is a contiguous range), split
@@ -1006,7 +1013,7 @@ struct BtCfg {
 #define DG_BT8_ROWS 16
 #endif
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
-using Bt8 = BtCfg<DG_BT8_ROWS, 192, 320, 2, (DG_BT8_ROWS > 16 ? 2 : 4)>;  // mapping 8
+using Bt8 = BtCfg<DG_BT8_ROWS, 160, 256, 2, (DG_BT8_ROWS > 16 ? 2 : 4)>;  // mapping 8
 static_assert(Bt7::smem_bytes<kSpread>() <= 227 * 1024, "mapping 7 fits shared memory");
 static_assert(Bt8::smem_bytes<kSpread>() <= 227 * 1024, "mapping 8 fits shared memory");
 

@@ -608,7 +608,9 @@ def main():
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": MEASURED_TRAFFIC.get((w.name, variant, n_frames)),
-                     "peak_kind": peak_kind, "kernel": "k_gather",
+                     "peak_kind": peak_kind,
+                     "kernel": ("k_gather_bins" if variant in (7, 8) else
+                                "k_gather_fl" if variant in (5, 6) else "k_gather"),
                      "alg_bytes_per_launch": alg,
                      "kernel_ms_per_launch": round(per_launch_s * 1000, 4)},
         "clocks": clk,

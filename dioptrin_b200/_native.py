@@ -26,7 +26,8 @@ DG_PLAN_FLIP_VERTICAL = 2
 EXPORTS = [
     "dg_plan_create", "dg_plan_destroy", "dg_plan_query", "dg_plan_radial",
     "dg_plan_azimuthal", "dg_plan_export_table", "dg_integrate", "dg_integrate_device",
-    "dg_integrate_device_plain", "dg_integrate_device_noalloc", "dg_plan_profile",
+    "dg_integrate_device_plain", "dg_integrate_device_noalloc", "dg_plan_test_wait_timeout",
+    "dg_plan_profile",
     "dg_plan_kernel_time", "dg_plan_autotune", "dg_plan_variant", "dg_eval_math",
     "dg_integrate_bslz4", "dg_bslz4_bound", "dg_bslz4_compress", "dg_plan_decode_time",
     "dg_integrate_dynamic", "dg_integrate_dynamic_device", "dg_integrate_raw",
@@ -118,6 +119,8 @@ def lib():
                      "dg_integrate_device_noalloc"):
             getattr(L, name).argtypes = [vp, vp, C.c_int32, C.c_int64, C.c_uint32, vp, vp, vp,
                                          vp]
+        L.dg_plan_test_wait_timeout.argtypes = [vp, vp, C.c_int32, C.c_int64, C.c_uint32, vp, vp,
+                                                vp]
         L.dg_plan_profile.argtypes = [vp, C.c_int32]
         L.dg_plan_kernel_time.argtypes = [vp, C.c_int32, pd, P(C.c_int64), P(C.c_int64)]
         L.dg_plan_autotune.argtypes = [vp, vp, C.c_int32, C.c_int64, C.c_uint32, vp,

@@ -407,6 +407,36 @@ dg_status dg_integrate_device_plain(dg_plan *plan, const void *d_frames, int32_t
     });
 }
 
+dg_status dg_plan_test_wait_timeout(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                    int64_t n_frames, uint32_t flags, double *d_i, double *d_s,
+                                    double *d_d) {
+    return guarded([&] {
+        check_frames(plan, d_frames, dtype, n_frames, flags, d_i, d_s, d_d);
+        if (n_frames == 0) dg::fail(DG_INVALID_INPUT, "the check needs at least one frame");
+        check_device_alignment(d_frames, dtype, d_i, d_s, d_d);
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        if (!dg::gather_variant_needs_tiles(plan->gather.variant))
+            dg::fail(DG_UNSUPPORTED, "the plan's gather lane mapping has no chunk pipeline "
+                                     "(select mapping 7 or 8)");
+        cudaStream_t s = plan->stream;
+        dg::check_bin_tile_waits(plan->gather);  // report an earlier failure as itself
+        plan->gather.withhold_test = 1;
+        try {
+            dg::run_gather(plan->gather, d_frames, dtype, int64_t(plan->dim1) * plan->dim2,
+                           n_frames, flags, plan->method.precision, d_i,
+                           (flags & DG_ERRORS) ? d_s : nullptr,
+                           (flags & DG_AZIMUTHAL_STD) ? d_d : nullptr, s);
+        } catch (...) {
+            plan->gather.withhold_test = 0;
+            throw;
+        }
+        plan->gather.withhold_test = 0;
+        DG_CUDA(cudaStreamSynchronize(s));
+        dg::check_bin_tile_waits(plan->gather);
+    });
+}
+
 namespace {
 
 // Arguments of the per-frame-mask and raw-sum calls.
@@ -632,6 +662,7 @@ dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t
                                         cudaMemcpyDeviceToHost, s));
         }
         DG_CUDA(cudaStreamSynchronize(s));
+        dg::check_bin_tile_waits(plan->gather);
     });
 }
 

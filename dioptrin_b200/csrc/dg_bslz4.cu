@@ -768,6 +768,7 @@ dg_status dg_integrate_bslz4(dg_plan *plan, const void *const *chunks, const int
         DG_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
         DG_CUDA(cudaStreamSynchronize(s));
         if (herr) fail(DG_INVALID_INPUT, "corrupt or truncated Bitshuffle/LZ4 compressed block");
+        check_bin_tile_waits(plan->gather);
     });
     if (st != DG_OK && plan) {
         // leave nothing of this call in flight (queued copies read the

@@ -967,29 +967,47 @@ __global__ void __launch_bounds__(256)
 // 32 apart). The tile's entries, merged over its rows in pixel order, are cut
 // into chunks of at most DCap distinct pixels and PCap entry pairs; a row's
 // entries inside a chunk are a contiguous run of its CSR row. The CTA walks
-// the tile's chunks in order with three buffers: while chunk k is summed,
-// chunk k+2's pixels (4-byte cp.async into frame rows Stride words apart) and
-// entry pairs (16-byte cp.async) are in flight; one barrier per chunk. Warp
-// w owns row w of the tile and keeps its sums in registers for the whole tile
-// (double-word FP32, folded every kFlFlushPairs pairs of the row), then
-// normalises and writes the results itself: no partial sums, no finalize
-// launch. Every row is summed in the same order for every frame and batch.
+// the tile's chunks in order through a ring of buffers: while chunk k is
+// summed, the next chunk's pixels (4-byte cp.async into frame rows Stride
+// words apart, every warp staging an equal share) and entry pairs (16-byte
+// cp.async) are in flight. There is no CTA-wide barrier per chunk: each
+// buffer has mbarriers for "landed" (every thread's copies) and "summed"
+// (every warp), so a warp whose row has many entries in one chunk can finish
+// it while the others start the next one; a row's load evens out over the
+// tile (rows of a tile hold nearly equal entry counts; their shares of one
+// chunk do not). Every wait is bounded (kBtWaitNs); a warp that gives up
+// ends the tile and sets a flag in mapped host memory that the host reports
+// as DG_TIMEOUT. Warp w owns row w of the tile and keeps its sums in
+// registers for the whole tile (double-word FP32, folded every kFlFlushPairs
+// pairs of the row), then normalises and writes the results itself: no
+// partial sums, no finalize launch. Every row is summed in the same order for
+// every frame and batch.
 // With two frames per lane (mapping 8) every entry pair read from shared
 // memory serves 64 frames: half the broadcast reads per frame, at half the
 // chunk size.
 
-constexpr int kBtBufs = 3;
-constexpr int kBtMetaBufs = 5;
-
 // One bin-tile layout: rows per tile (= warps per CTA: warp w owns row w),
-// chunk capacities, frames per lane and pairs per unrolled step. Per-chunk
+// chunk capacities, frames per lane, pairs per unrolled step and the chunk
+// pipeline: BUFS pixel/pair buffers, pixels staged AHEAD chunks before they
+// are summed and records MAHEAD chunks before their pixels. Per-chunk
 // record, fixed size: {pixels D, pairs, first pair, 0}, the rows' pair
 // offsets (ROWS + 1, padded to a multiple of 4 words), then D pixel indices.
-template <int ROWS, int DCAP, int PCAP, int F2, int U2>
+template <int ROWS, int DCAP, int PCAP, int F2, int U2, int BUFS = 3, int AHEAD = 1,
+          int MAHEAD = 1>
 struct BtCfg {
     static constexpr int kRows = ROWS;
     static constexpr int kThreads = ROWS * 32;
     static constexpr int kU2 = U2;
+    static constexpr int kBufs = BUFS;
+    static constexpr int kAhead = AHEAD;
+    static constexpr int kMetaAhead = MAHEAD;
+    // A record slot is rewritten only after every warp has summed the chunk
+    // it held (the buffer waits guarantee that for BUFS + MAHEAD slots).
+    static constexpr int kMetaBufs = BUFS + MAHEAD;
+    // How many chunks a warp may fall behind the fastest one.
+    static constexpr int kLag = AHEAD < MAHEAD ? (AHEAD < BUFS - AHEAD - 1 ? AHEAD : BUFS - AHEAD - 1)
+                                               : (MAHEAD < BUFS - AHEAD - 1 ? MAHEAD : BUFS - AHEAD - 1);
+    static_assert(AHEAD >= 1 && MAHEAD >= 1 && kLag >= 0, "pipeline depths");
     static_assert(ROWS <= 32, "tile rows are packed in 5 bits at plan time");
     static constexpr int kDCap = DCAP;          // distinct pixels per chunk
     static constexpr int kStride = DCAP + 1;    // odd frame-row stride; column DCAP stays 0
@@ -998,28 +1016,99 @@ struct BtCfg {
     static constexpr int kFrames = 32 * F2;     // frames per CTA
     static constexpr int kMetaHead = (4 + ROWS + 1 + 3) / 4 * 4;
     static constexpr int kMetaWords = kMetaHead + DCAP;
+    // Staging shares: the chunk's pixels are cut into kSlices slices and warp
+    // w stages slice w % kSlices of kStageFrames frames (w / kSlices + j *
+    // ROWS / kSlices), so every warp issues the same number of copies and
+    // reads each pixel index once for all its frames.
+    static constexpr int kSlices = ROWS % 3 == 0 ? 3 : 1;
+    static constexpr int kStageFrames = kFrames * kSlices / ROWS;
+    static_assert(ROWS % kSlices == 0 && (kFrames * kSlices) % ROWS == 0,
+                  "staging shares must divide evenly");
     static_assert(kMetaWords % 4 == 0, "records are copied in 16-byte pieces");
     static_assert(kStride % 2 == 1, "frame rows must start in different banks");
     template <int MODE>
     static constexpr size_t buf_bytes() {
         return size_t(kFrames) * kStride * 4 + size_t(PCAP) * (MODE == kSpread ? 32 : 16);
     }
+    // Buffers, records, then the mbarriers: full[BUFS], empty[BUFS], record[kMetaBufs].
+    template <int MODE>
+    static constexpr size_t bar_offset() {
+        return size_t(BUFS) * buf_bytes<MODE>() + size_t(kMetaBufs) * kMetaWords * 4;
+    }
     template <int MODE>
     static constexpr size_t smem_bytes() {
-        return size_t(kBtBufs) * buf_bytes<MODE>() + size_t(kBtMetaBufs) * kMetaWords * 4;
+        return bar_offset<MODE>() + size_t(2 * BUFS + kMetaBufs) * 8;
     }
 };
+// Mapping 8's layout can be changed at build time for measurements
+// (-DDG_BT8_ROWS=24, -DDG_BT8_DCAP=128 -DDG_BT8_PCAP=200 -DDG_BT8_BUFS=4 -DDG_BT8_AHEAD=2).
 #ifndef DG_BT8_ROWS
 #define DG_BT8_ROWS 16
 #endif
+#ifndef DG_BT8_DCAP
+#define DG_BT8_DCAP 160
+#endif
+#ifndef DG_BT8_PCAP
+#define DG_BT8_PCAP 256
+#endif
+#ifndef DG_BT8_BUFS
+#define DG_BT8_BUFS 3
+#endif
+#ifndef DG_BT8_AHEAD
+#define DG_BT8_AHEAD 1
+#endif
+// Bin tiles run largest first (1) or in bin order (0).
+#ifndef DG_BT_LARGEST_FIRST
+#define DG_BT_LARGEST_FIRST 1
+#endif
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
-using Bt8 = BtCfg<DG_BT8_ROWS, 160, 256, 2, (DG_BT8_ROWS > 16 ? 2 : 4)>;  // mapping 8
+using Bt8 = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, 2, (DG_BT8_ROWS > 16 ? 2 : 4),
+                  DG_BT8_BUFS, DG_BT8_AHEAD>;  // mapping 8
 static_assert(Bt7::smem_bytes<kSpread>() <= 227 * 1024, "mapping 7 fits shared memory");
 static_assert(Bt8::smem_bytes<kSpread>() <= 227 * 1024, "mapping 8 fits shared memory");
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Shared-memory mbarriers of the bin-tile chunk pipeline.
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(b)) : "memory");
+}
+// Arrives (without raising the expected count) once all of this thread's
+// earlier cp.async copies have landed.
+__device__ __forceinline__ void mbar_arrive_copies(uint64_t *b) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(b))
+                 : "memory");
+}
+// Waits for the phase of the given parity to complete; gives up (false)
+// after kBtWaitNs of global time, so a lost arrival cannot hang the GPU.
+constexpr uint64_t kBtWaitNs = 1000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
+    const unsigned a = smem_addr(b);
+    uint64_t t0 = 0;
+    for (int n = 0;; ++n) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        uint64_t now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (n == 0) t0 = now;
+        else if (now - t0 > kBtWaitNs) return false;
+    }
 }
 
 template <int MODE, typename P, class CFG>
@@ -1031,12 +1120,13 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                   const double *__restrict__ den_f32, const int32_t *__restrict__ valid_std,
                   const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_rows,
                   double *__restrict__ out_i, double *__restrict__ out_s,
-                  double *__restrict__ out_d) {
+                  double *__restrict__ out_d, int *__restrict__ wait_err, int withhold) {
     using S = StagedPx<P>;
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
     constexpr int F2 = CFG::kF2, STRIDE = CFG::kStride, DCAP = CFG::kDCap, PCAP = CFG::kPCap;
-    constexpr int U2 = CFG::kU2, NT = CFG::kThreads;
+    constexpr int U2 = CFG::kU2, NT = CFG::kThreads, NW = CFG::kRows;
+    constexpr int NB = CFG::kBufs, NM = CFG::kMetaBufs, AH = CFG::kAhead, MA = CFG::kMetaAhead;
     constexpr int MH = CFG::kMetaHead, MW = CFG::kMetaWords;
     constexpr size_t BUF = CFG::template buf_bytes<MODE>();
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1046,6 +1136,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     const int nv = min(CFG::kFrames, n_frames - f0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int row0 = it.x, nrows = it.y, ch0 = it.z, nch = it.w;
+    // Failure-detection check (dg_plan_test_wait_timeout): warp 0 of the first
+    // CTA never reports a chunk summed, so the waits for its buffers run out.
+    const bool signal = !(withhold && blockIdx.x == 0 && warp == 0);
 
     auto pxbuf = [&](int b) { return reinterpret_cast<S *>(smem + size_t(b) * BUF); };
     auto pabuf = [&](int b) {
@@ -1053,48 +1146,65 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                                           size_t(CFG::kFrames) * STRIDE * 4);
     };
     auto mbuf = [&](int c) {
-        return reinterpret_cast<int32_t *>(smem + size_t(kBtBufs) * BUF) + (c % kBtMetaBufs) * MW;
+        return reinterpret_cast<int32_t *>(smem + size_t(NB) * BUF) + (c % NM) * MW;
     };
-    // Copy chunk c's record into its record buffer (part of the open group).
-    auto stage_meta = [&](int c) {
-        if (c < nch) {
-            const int4 *src = reinterpret_cast<const int4 *>(meta + int64_t(ch0 + c) * MW);
-            int4 *dst = reinterpret_cast<int4 *>(mbuf(c));
-            for (int j = tid; j < MW / 4; j += NT) cp_async16(dst + j, src + j);
+    // full[b]: chunk in buffer b landed (every thread's copies and stores);
+    // empty[b]: every warp has summed the chunk in buffer b; rec[m]: the
+    // record in slot m landed.
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + CFG::template bar_offset<MODE>());
+    uint64_t *empty = full + NB, *rec = full + 2 * NB;
+    if (tid == 0) {
+        for (int b = 0; b < NB; ++b) {
+            mbar_init(full + b, NT);
+            mbar_init(empty + b, NW);
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
+        for (int m = 0; m < NM; ++m) mbar_init(rec + m, NT);
+    }
     // Column DCAP of every frame row is read by padding pairs and holds 0.
-    for (int j = tid; j < kBtBufs * CFG::kFrames; j += NT)
+    for (int j = tid; j < NB * CFG::kFrames; j += NT)
         pxbuf(j / CFG::kFrames)[(j % CFG::kFrames) * STRIDE + DCAP] = S(0);
+    __syncthreads();
 
-    // Stage chunk c (of this tile) into buffer b as one commit group; its
-    // record is in shared memory already.
-    auto stage = [&](int c, int b) {
-        if (c < nch) {
-            const int32_t *mb = mbuf(c);
-            const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
-            S *dst = pxbuf(b);
-            const P *base = frames + int64_t(f0) * n_pixels;
-            for (int k = tid; k < ch.y; k += NT) {
-                const P *src = base + mb[MH + k];
-                if constexpr (sizeof(P) == 4) {
-#pragma unroll 8
-                    for (int f = 0; f < nv; ++f)
-                        cp_async4(dst + f * STRIDE + k, src + int64_t(f) * n_pixels);
-                } else {
-#pragma unroll 8
-                    for (int f = 0; f < nv; ++f)
-                        dst[f * STRIDE + k] = load_px<P>(src + int64_t(f) * n_pixels, 0u);
-                }
-            }
-            float4 *pa = pabuf(b);
-            for (int j = tid; j < ch.w; j += NT) {
-                cp_async16(pa + j, pair_a + ch.z + j);
-                if (SPREAD) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
+    // Copy chunk c's record into its slot; every thread arrives on the
+    // slot's barrier once its copies have landed (all threads arriving, not
+    // only the copying ones, measured faster: 2.03 against 2.67 ms).
+    auto stage_meta = [&](int c) {
+        const int4 *src = reinterpret_cast<const int4 *>(meta + int64_t(ch0 + c) * MW);
+        int4 *dst = reinterpret_cast<int4 *>(mbuf(c));
+        for (int j = tid; j < MW / 4; j += NT) cp_async16(dst + j, src + j);
+        mbar_arrive_copies(rec + c % NM);
+    };
+    // Stage chunk c into buffer c % NB (its record is in shared memory); every
+    // thread arrives on the buffer's full barrier, counted once its copies
+    // have landed and ordering its plain stores (2-byte pixels) before it.
+    auto stage = [&](int c) {
+        const int b = c % NB;
+        const int32_t *mb = mbuf(c);
+        const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
+        constexpr int KS = CFG::kSlices, FS = CFG::kStageFrames, FSTEP = CFG::kRows / KS;
+        const int per = (ch.y + KS - 1) / KS, s0 = (warp % KS) * per;
+        const int k1 = min(ch.y, s0 + per), fw = warp / KS;
+        S *dst = pxbuf(b) + fw * STRIDE;
+        const P *base = frames + int64_t(f0 + fw) * n_pixels;
+        for (int k = s0 + lane; k < k1; k += 32) {
+            const P *src = base + mb[MH + k];
+#pragma unroll
+            for (int j = 0; j < FS; ++j) {
+                if (fw + j * FSTEP >= nv) break;
+                if constexpr (sizeof(P) == 4)
+                    cp_async4(dst + j * FSTEP * STRIDE + k, src + int64_t(j * FSTEP) * n_pixels);
+                else
+                    dst[j * FSTEP * STRIDE + k] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
             }
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        float4 *pa = pabuf(b);
+        for (int j = tid; j < ch.w; j += NT) {
+            cp_async16(pa + j, pair_a + ch.z + j);
+            if (SPREAD) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
+        }
+        asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];\n" ::"r"(smem_addr(full + b))
+                     : "memory");
+        mbar_arrive(full + b);
     };
 
     // This warp's row: accumulators, fold counter and origin of each of the
@@ -1111,24 +1221,35 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     const int r = warp;  // row of the tile
     const int4 o = r < nrows ? org[row0 + r] : make_int4(-1, 0, -1, 0);
 
-    // Pipeline: records two chunks ahead of their pixels, pixels two chunks
-    // ahead of their sums; commit order M0 M1 | P0 M2 P1 M3 | P2 M4 | P3 M5 ...
-    stage_meta(0);
-    stage_meta(1);
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
-    stage(0, 0);
-    stage_meta(2);
-    stage(1, 1);
-    stage_meta(3);
+    // Pipeline without a CTA-wide barrier: in step c a warp stages its share
+    // of chunk c + AH (once every warp has summed the chunk that buffer held)
+    // and of record c + AH + MA, then sums chunk c once all its shares have
+    // landed. A warp may fall kLag chunks behind the fastest, so rows whose
+    // entries are unevenly spread over the chunks even out over the tile.
+    bool ok = true;
+    for (int j = 0; j < AH + MA && j < nch; ++j) stage_meta(j);
+    for (int j = 0; j < AH && j < nch; ++j) {
+        if (ok) ok = mbar_wait(rec + j % NM, unsigned(j / NM) & 1u);
+        if (ok) stage(j);
+    }
     for (int c = 0; c < nch; ++c) {
-        // complete: P(c) and M(c+2); pending: P(c+1), M(c+3)
-        asm volatile("cp.async.wait_group 2;\n" ::: "memory");
-        __syncthreads();
-        stage(c + 2, (c + 2) % kBtBufs);
-        stage_meta(c + 4);
-        if (r >= nrows) continue;
-        const int b = c % kBtBufs;
+        const int j = c + AH;
+        if (j < nch) {
+            if (ok && j >= NB) ok = mbar_wait(empty + j % NB, unsigned(j / NB - 1) & 1u);
+            if (ok && j + MA < nch) stage_meta(j + MA);
+            if (ok) ok = mbar_wait(rec + j % NM, unsigned(j / NM) & 1u);
+            if (ok) stage(j);
+        }
+        if (ok) ok = mbar_wait(full + c % NB, unsigned(c / NB) & 1u);
+        if (!__all_sync(0xffffffffu, ok)) {
+            ok = false;
+            break;
+        }
+        const int b = c % NB;
+        if (r >= nrows) {
+            if (lane == 0 && signal) mbar_arrive(empty + b);
+            continue;
+        }
         const S *px[F2];
 #pragma unroll
         for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + (lane + 32 * h) * STRIDE;
@@ -1233,8 +1354,19 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 fold();
             }
         }
+        __syncwarp();
+        if (lane == 0 && signal) mbar_arrive(empty + b);
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (!ok) {
+        // A wait gave up: this tile's sums are incomplete. The host finds the
+        // flag (mapped host memory) and reports the call as failed.
+        if (lane == 0) {
+            *reinterpret_cast<volatile int *>(wait_err) = 1;
+            __threadfence_system();
+        }
+        return;
+    }
     if (r >= nrows) return;
 
     // Normalise (normalize_bin, prepared.rs:985-996; the spread's closing
@@ -1513,10 +1645,12 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
     const int groups = (nf + CFG::kFrames - 1) / CFG::kFrames;
     const int64_t grid = int64_t(bt.n_items) * groups;
     if (grid > INT32_MAX) fail(DG_UNSUPPORTED, "too many bin tiles for one launch");
+    check_bin_tile_waits(t);
     kern<<<unsigned(grid), CFG::kThreads, smem, s>>>(
         bt.item.ptr, bt.meta.ptr, MODE == kSpread ? bt.pair_as.ptr : bt.pair_a.ptr,
         bt.pair_b.ptr, bt.org.ptr, t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr,
-        t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od);
+        t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od, bt.wait_err.dev,
+        t.withhold_test);
 }
 
 // Launches lane mapping `variant`; returns true when the kernel wrote the
@@ -1724,6 +1858,7 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     const int64_t nb = table.n_rows;
     out.n_items = 0;
     if (nb == 0 || table.nnz == 0) return;
+    out.wait_err.alloc();
     std::vector<int64_t> rp(static_cast<size_t>(nb) + 1);
     DG_CUDA(cudaMemcpyAsync(rp.data(), table.row_ptr.ptr, rp.size() * 8, cudaMemcpyDeviceToHost, s));
     std::vector<int32_t> col(static_cast<size_t>(table.nnz)), fv(static_cast<size_t>(nb));
@@ -1844,12 +1979,14 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         for (auto &th : pool) th.join();
     };
     parallel(build);
-    // Largest tiles first; then flatten.
+    // Tile order, then flatten.
     std::vector<int64_t> order(static_cast<size_t>(n_items));
     for (int64_t i = 0; i < n_items; ++i) order[size_t(i)] = i;
+#if DG_BT_LARGEST_FIRST
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
         return tiles[size_t(a)].entries > tiles[size_t(b)].entries;
     });
+#endif
     // Output offsets of every tile, then the tiles copied in parallel.
     std::vector<int64_t> o_ch(size_t(n_items) + 1, 0), o_px(size_t(n_items) + 1, 0),
         o_pr(size_t(n_items) + 1, 0);
@@ -1921,6 +2058,22 @@ namespace {
 __global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int words, int head,
                             int rows, int cols);
 }  // namespace
+
+bool bin_tile_wait_failed(const GatherTable &t) {
+    bool failed = false;
+    for (const BinTiles &bt : t.bt)
+        if (bt.wait_err.host && *static_cast<volatile int *>(bt.wait_err.host)) {
+            *bt.wait_err.host = 0;
+            failed = true;
+        }
+    return failed;
+}
+
+void check_bin_tile_waits(const GatherTable &t) {
+    if (bin_tile_wait_failed(t))
+        fail(DG_TIMEOUT, "bin-tile gather: a chunk-pipeline wait gave up after 1 s; the "
+                          "results of a launch on this plan since the last check are invalid");
+}
 
 void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, int variant, cudaStream_t s) {
     if (variant != 7 && variant != 8) return;

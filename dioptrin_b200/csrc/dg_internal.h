@@ -68,6 +68,52 @@ struct DeviceArray {
     size_t bytes() const { return count * sizeof(T); }
 };
 
+// One int in mapped page-locked host memory: a kernel sets it to report a
+// failure without the host synchronising; the host reads it at any time.
+struct PinnedFlag {
+    int *host = nullptr;
+    int *dev = nullptr;
+    PinnedFlag() = default;
+    PinnedFlag(const PinnedFlag &) = delete;
+    PinnedFlag &operator=(const PinnedFlag &) = delete;
+    PinnedFlag(PinnedFlag &&o) noexcept : host(o.host), dev(o.dev) {
+        o.host = nullptr;
+        o.dev = nullptr;
+    }
+    PinnedFlag &operator=(PinnedFlag &&o) noexcept {
+        if (this != &o) {
+            release();
+            host = o.host;
+            dev = o.dev;
+            o.host = nullptr;
+            o.dev = nullptr;
+        }
+        return *this;
+    }
+    ~PinnedFlag() { release(); }
+    void alloc() {
+        if (host) return;
+        void *p = nullptr;
+        cudaError_t e = cudaHostAlloc(&p, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable);
+        void *d = nullptr;
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer(&d, p, 0);
+        if (e != cudaSuccess) {
+            if (p) cudaFreeHost(p);
+            (void)cudaGetLastError();
+            fail(DG_DEVICE, std::string("mapped host flag allocation failed: ") +
+                                cudaGetErrorString(e));
+        }
+        host = static_cast<int *>(p);
+        dev = static_cast<int *>(d);
+        *host = 0;
+    }
+    void release() {
+        if (host) cudaFreeHost(host);
+        host = nullptr;
+        dev = nullptr;
+    }
+};
+
 // Geometry scalars the device kernels need. Trigonometric constants and the
 // q scale are computed on the host with the C library so that they are the
 // same bits the reference computes (geometry.rs:640-660, integration.rs:147-158).
@@ -157,6 +203,8 @@ struct BinTiles {
     DeviceArray<int32_t> meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
     DeviceArray<int4> org;         // per row {chunk in tile (-1: none), slot, entry, row end}
     DeviceArray<float4> pair_a, pair_as, pair_b;
+    // Set by k_gather_bins when a wait of its chunk pipeline gave up.
+    PinnedFlag wait_err;
     int64_t bytes() const {
         return int64_t(item.bytes() + meta.bytes() + org.bytes() + pair_a.bytes() +
                        pair_as.bytes() + pair_b.bytes());
@@ -204,6 +252,7 @@ struct GatherTable {
     // Bin tiles (k_gather_bins), mappings 7 and 8; see dg_gather.cu.
     BinTiles bt[2];
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
+    int withhold_test = 0;            // bin tiles: stall one warp (dg_plan_test_wait_timeout)
     int32_t flip_rows = 0, flip_cols = 0;  // frames stored bottom row first (0: detector order)
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
     bool profile = false;
@@ -236,6 +285,10 @@ void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s
 // table on first use (the autotuner, or selecting the mapping); idempotent.
 void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, int variant, cudaStream_t s);
 bool gather_variant_needs_tiles(int variant);
+// Throws DG_TIMEOUT (once) when a bin-tile launch of this table gave up a
+// pipeline wait; bin_tile_wait_failed only reports and clears it.
+bool bin_tile_wait_failed(const GatherTable &t);
+void check_bin_tile_waits(const GatherTable &t);
 // The autotuner times the bin-tile mapping only for batches of more frames
 // than this (one tile per CTA: smaller batches leave SMs idle).
 constexpr int64_t kBinTileMinFrames = 64;

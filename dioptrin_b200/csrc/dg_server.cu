@@ -371,6 +371,10 @@ struct dg_server {
                         st = DG_DEVICE;
                         err = cudaGetErrorString(cudaGetLastError());
                     }
+                    if (st == DG_OK && dg::bin_tile_wait_failed(plan->gather)) {
+                        st = DG_TIMEOUT;
+                        err = "bin-tile gather: a chunk-pipeline wait gave up after 1 s";
+                    }
                     if (st == DG_OK) {
                         for (size_t i = 0; i < nf; ++i) {
                             Request *r = batch[i];

@@ -185,6 +185,21 @@ DG_EXPORT dg_status dg_integrate_device_plain(dg_plan *plan, const void *d_frame
                                     int64_t n_frames, uint32_t flags, double *d_intensity,
                                     double *d_sigma, double *d_std, void *stream);
 
+/* Failure-detection check of the bin-tile gathers (lane mappings 7 and 8);
+ * it has no counterpart in the reference. Their warps pass chunks through
+ * shared-memory barriers whose every wait gives up after 1 s; the kernel then
+ * marks a flag in mapped host memory, and the plan's next call (host-memory
+ * calls: the same call) returns DG_TIMEOUT. This call runs one gather of the
+ * device frames with one warp of one CTA never reporting a chunk summed, so
+ * the other warps' waits run out. It waits for the GPU and returns DG_TIMEOUT
+ * when the kernel reported the expired wait (DG_OK when the tile had too few
+ * chunks to stall); the results are undefined, and the plan integrates
+ * normally afterwards. DG_UNSUPPORTED unless the plan uses mapping 7 or 8. */
+DG_EXPORT dg_status dg_plan_test_wait_timeout(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                              int64_t n_frames, uint32_t flags,
+                                              double *d_intensity, double *d_sigma,
+                                              double *d_std);
+
 /* Kernel timing for roofline reports; the reference times its CUDA phases
  * with events in src/integration/cuda/bench.rs:139-196. With enable != 0,
  * every gather-kernel launch of the plan is bracketed by CUDA events on the

@@ -41,11 +41,12 @@ sys.path.insert(0, ROOT)
 METRIC = "eiger4m_1d_frames_per_s"
 
 # DRAM bytes (read + write) of one gather launch from an ncu capture, keyed by
-# (workload, gather mapping, frames per launch): the bin-tile mapping captured
+# (workload, gather mapping, frames per launch): the bin-tile mappings captured
 # at full size (dram__bytes_read.sum + dram__bytes_write.sum, one pass:
 # profiles/k_gather_bins_eiger4m_b256.md); the frame-lane mapping from a
 # 32-frame capture with frame and partial-sum bytes scaled to 256 frames.
-MEASURED_TRAFFIC = {("eiger4m_ps2000_b256", 7, 256): 5_722_000_000,
+MEASURED_TRAFFIC = {("eiger4m_ps2000_b256", 8, 256): 6_872_000_000,
+                    ("eiger4m_ps2000_b256", 7, 256): 5_722_000_000,
                     ("eiger4m_ps2000_b256", 6, 256): 5_533_000_000}
 
 

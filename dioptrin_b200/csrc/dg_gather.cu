@@ -1091,6 +1091,7 @@ __device__ __forceinline__ void mbar_arrive_copies(uint64_t *b) {
 }
 // Waits for the phase of the given parity to complete; gives up (false)
 // after kBtWaitNs of global time, so a lost arrival cannot hang the GPU.
+// (A suspend-time hint on the try, 1 ms, measured 2% slower on mapping 8.)
 constexpr uint64_t kBtWaitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned parity) {
     const unsigned a = smem_addr(b);
@@ -1120,7 +1121,8 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                   const double *__restrict__ den_f32, const int32_t *__restrict__ valid_std,
                   const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_rows,
                   double *__restrict__ out_i, double *__restrict__ out_s,
-                  double *__restrict__ out_d, int *__restrict__ wait_err, int withhold) {
+                  double *__restrict__ out_d, int *__restrict__ wait_err, int withhold,
+                  const double *__restrict__ raw_cnt, double *__restrict__ out_c, int raw) {
     using S = StagedPx<P>;
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
@@ -1383,6 +1385,15 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             v[a] = acc[h][a].value();
         }
         const int64_t oo = int64_t(f0 + fl) * n_rows + row;
+        if (raw) {
+            // Raw sums (integrate1d_raw*, integrate.rs:682-797): signal and
+            // variance sums of the frame, the row's strict norm and weight sums.
+            out_i[oo] = v[0];
+            if (NA > 1 && out_s) out_s[oo] = v[NA > 1 ? 1 : 0];
+            out_d[oo] = den[row];
+            out_c[oo] = raw_cnt[row];
+            continue;
+        }
         if constexpr (!SPREAD) {
             const double n = den[row];
             out_i[oo] = n == 0.0 ? 0.0 : v[0] / n;
@@ -1638,7 +1649,8 @@ void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, doub
 // its partial sums in `partial`.
 template <int MODE, typename P, class CFG>
 void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t n_pixels, int nf,
-                 double *oi, double *os, double *od, cudaStream_t s) {
+                 double *oi, double *os, double *od, cudaStream_t s, double *oc = nullptr,
+                 int raw = 0) {
     constexpr size_t smem = CFG::template smem_bytes<MODE>();
     auto kern = k_gather_bins<MODE, P, CFG>;
     DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -1650,7 +1662,7 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
         bt.item.ptr, bt.meta.ptr, MODE == kSpread ? bt.pair_as.ptr : bt.pair_a.ptr,
         bt.pair_b.ptr, bt.org.ptr, t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr,
         t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od, bt.wait_err.dev,
-        t.withhold_test);
+        t.withhold_test, t.cnt.ptr, oc, raw);
 }
 
 // Launches lane mapping `variant`; returns true when the kernel wrote the
@@ -2211,6 +2223,7 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
     const int64_t chunk = 256;
     const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 5;
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+    t.scratch.wait(s);
     const size_t esize = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
     for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
         const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
@@ -2254,6 +2267,7 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
             }
         }
     }
+    t.scratch.mark(s);
 }
 
 namespace {
@@ -2321,15 +2335,31 @@ void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, c
 namespace {
 
 template <typename P>
-void launch_raw(GatherTable &t, const void *frames, int64_t n_pixels, int nf, int mode,
-                const uint8_t *masks, int64_t mask_stride, cudaStream_t s) {
+bool launch_raw(GatherTable &t, const void *frames, int64_t n_pixels, int nf, int mode,
+                const uint8_t *masks, int64_t mask_stride, cudaStream_t s, double *o0 = nullptr,
+                double *o1 = nullptr, double *o2 = nullptr, double *o3 = nullptr) {
     const P *fp = static_cast<const P *>(frames);
+    // Raw sums over the plan mask on a bin-tile plan: the tiles write them.
+    if (o0 && mode != kRaw && gather_variant_needs_tiles(t.variant) &&
+        t.bt[t.variant - 7].n_items > 0) {
+        const BinTiles &bt = t.bt[t.variant - 7];
+        if (mode == kErrors) {
+            if (t.variant == 7) launch_bins<kErrors, P, Bt7>(t, bt, fp, n_pixels, nf, o0, o2, o1, s, o3, 1);
+            else launch_bins<kErrors, P, Bt8>(t, bt, fp, n_pixels, nf, o0, o2, o1, s, o3, 1);
+        } else {
+            if (t.variant == 7) launch_bins<kIntensity, P, Bt7>(t, bt, fp, n_pixels, nf, o0, nullptr, o1, s, o3, 1);
+            else launch_bins<kIntensity, P, Bt8>(t, bt, fp, n_pixels, nf, o0, nullptr, o1, s, o3, 1);
+        }
+        DG_CUDA(cudaGetLastError());
+        return true;
+    }
     if (mode == kRaw)
         launch_gather<kRaw, P>(t, t.variant, fp, n_pixels, nf, t.partial.ptr, s, masks, mask_stride);
     else if (mode == kErrors)
         launch_gather<kErrors, P>(t, t.variant, fp, n_pixels, nf, t.partial.ptr, s);
     else
         launch_gather<kIntensity, P>(t, t.variant, fp, n_pixels, nf, t.partial.ptr, s);
+    return false;
 }
 
 }  // namespace
@@ -2345,11 +2375,15 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     const int64_t chunk = 256;
     const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 5;
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+    t.scratch.wait(s);
     const size_t esize = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
     for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
         const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
         const void *fp = static_cast<const unsigned char *>(d_frames) + f0 * n_pixels * esize;
         const uint8_t *mp = d_masks ? d_masks + f0 * mask_stride : nullptr;
+        const int64_t off = f0 * t.n_rows;
+        auto at = [&](double *o) { return o ? o + off : nullptr; };
+        bool done = false;  // raw sums written by the bin tiles themselves
         if (t.n_units > 0) {
             std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
             if (t.profile) {
@@ -2364,19 +2398,22 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
                 DG_CUDA(cudaEventRecord(ev->first, s));
             }
             ++t.launches;
+            double *r0 = raw ? at(o0) : nullptr, *r1 = at(o1), *r2 = errors ? at(o2) : nullptr,
+                   *r3 = at(o3);
+#define DG_RAW_CALL(T) \
+    done = launch_raw<T>(t, fp, n_pixels, nf, mode, mp, mask_stride, s, r0, r1, r2, r3)
             switch (dtype) {
-            case DG_U16: launch_raw<uint16_t>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
-            case DG_U32: launch_raw<uint32_t>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
-            case DG_I32: launch_raw<int32_t>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
-            case DG_F32: launch_raw<float>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
-            case DG_F64: launch_raw<double>(t, fp, n_pixels, nf, mode, mp, mask_stride, s); break;
+            case DG_U16: DG_RAW_CALL(uint16_t); break;
+            case DG_U32: DG_RAW_CALL(uint32_t); break;
+            case DG_I32: DG_RAW_CALL(int32_t); break;
+            case DG_F32: DG_RAW_CALL(float); break;
+            case DG_F64: DG_RAW_CALL(double); break;
             }
+#undef DG_RAW_CALL
             if (ev) DG_CUDA(cudaEventRecord(ev->second, s));
         }
-        if (t.n_rows == 0) continue;
+        if (t.n_rows == 0 || done) continue;
         ++t.launches;
-        const int64_t off = f0 * t.n_rows;
-        auto at = [&](double *o) { return o ? o + off : nullptr; };
         const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);
         if (raw) {
 #define DG_RAW_ARGS                                                                          \
@@ -2399,6 +2436,7 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
             }
         }
     }
+    t.scratch.mark(s);
 }
 
 namespace {
@@ -2434,6 +2472,7 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     const int nf = int(std::min<int64_t>(n_frames, 256));
     const int64_t need = std::max<int64_t>(1, t.n_segments) * 256 * 5;
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+    t.scratch.wait(s);
     if (each) each->assign(size_t(kVariantCount), 0.0);
     if (t.n_units == 0) return t.variant;
     DeviceArray<double> outs;
@@ -2482,6 +2521,7 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    t.scratch.mark(s);
     t.variant = best;
     return best;
 }

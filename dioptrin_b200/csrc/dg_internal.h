@@ -163,6 +163,46 @@ void eval_math(int which, const double *a, const double *b, int64_t n, double *o
                cudaStream_t stream);
 
 // Pairs of CUDA events, created on demand and destroyed with the pool.
+// Orders the uses of a plan's scratch by calls on different streams (a
+// caller may name any stream): each use records `done` on its stream, and a
+// use on another stream waits for it first. Calls on one stream are ordered
+// by the stream already.
+struct ScratchOrder {
+    cudaEvent_t done = nullptr;
+    cudaStream_t last = nullptr;
+    bool used = false;
+    ScratchOrder() = default;
+    ScratchOrder(const ScratchOrder &) = delete;
+    ScratchOrder &operator=(const ScratchOrder &) = delete;
+    ScratchOrder(ScratchOrder &&o) noexcept : done(o.done), last(o.last), used(o.used) {
+        o.done = nullptr;
+        o.used = false;
+    }
+    ScratchOrder &operator=(ScratchOrder &&o) noexcept {
+        if (this != &o) {
+            if (done) cudaEventDestroy(done);
+            done = o.done;
+            last = o.last;
+            used = o.used;
+            o.done = nullptr;
+            o.used = false;
+        }
+        return *this;
+    }
+    ~ScratchOrder() {
+        if (done) cudaEventDestroy(done);
+    }
+    void wait(cudaStream_t s) {
+        if (used && last != s) DG_CUDA(cudaStreamWaitEvent(s, done, 0));
+    }
+    void mark(cudaStream_t s) {
+        if (!done) DG_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        DG_CUDA(cudaEventRecord(done, s));
+        last = s;
+        used = true;
+    }
+};
+
 struct EventPool {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     size_t used = 0;
@@ -257,6 +297,7 @@ struct GatherTable {
     // Optional CUDA-event timing of the gather launches (dg_plan_profile).
     bool profile = false;
     EventPool events;
+    ScratchOrder scratch;  // orders uses of `partial` across streams
     int64_t launches = 0;  // every kernel launch of run_gather since the last reset
 };
 

@@ -146,12 +146,17 @@ def test_dynamic_device_form_equals_host_form(dg):
     dyn.close()
 
 
+@pytest.mark.parametrize("variant", [None, 5, 7, 8])
 @pytest.mark.parametrize("dtype", ["uint32", "float64"])
-def test_raw_sums_with_the_plan_mask(dg, oracle, ref, dtype):
+def test_raw_sums_with_the_plan_mask(dg, oracle, ref, dtype, variant):
+    # None: the tuned mapping; 7 and 8: the bin tiles write the raw sums
+    # themselves, from the accumulators their normalised results divide.
     it = _integrator(dg)
     mask = _masks(1, 9)[0]
     it.set_mask(mask)
     plan = it.prepare_cuda1d(SHAPE, NB)
+    if variant is not None:
+        plan.gather_variant = variant
     frames = np.random.default_rng(10).poisson(40.0, (3,) + SHAPE).astype(dtype)
     res = plan.integrate_raw_stack(frames, with_variance=True)
     _, _, _, den = plan.export_table(0)
@@ -166,6 +171,11 @@ def test_raw_sums_with_the_plan_mask(dg, oracle, ref, dtype):
         np.testing.assert_allclose(r.count, c, rtol=1e-9, atol=1e-15)
         i = np.where(r.sum_norm == 0, 0.0, r.sum_signal / np.where(r.sum_norm == 0, 1, r.sum_norm))
         _close(i, I[k], I[k].max())
+        if variant in (7, 8):
+            assert np.array_equal(i, I[k])
+            safe = np.where(r.sum_norm == 0, 1, r.sum_norm)
+            q = np.where(r.sum_norm == 0, 0.0, r.sum_variance / (safe * safe))
+            assert np.array_equal(np.sqrt(np.maximum(q, 0.0)), S[k])
         assert np.array_equal(r.bins, plan.radial_array)
     # without variance
     r0 = plan.integrate1d_raw(frames[0])

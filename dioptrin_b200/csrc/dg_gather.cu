@@ -1026,9 +1026,14 @@ struct BtCfg {
                   "staging shares must divide evenly");
     static_assert(kMetaWords % 4 == 0, "records are copied in 16-byte pieces");
     static_assert(kStride % 2 == 1, "frame rows must start in different banks");
+    // Per-frame masks (mode kRaw): a byte per slot, frame rows an odd number
+    // of words apart (32 lanes reading one slot of their frames hit 32 banks).
+    static constexpr int kMStride = 4 * (((DCAP + 4) / 4) | 1);
     template <int MODE>
     static constexpr size_t buf_bytes() {
-        return size_t(kFrames) * kStride * 4 + size_t(PCAP) * (MODE == kSpread ? 32 : 16);
+        return size_t(kFrames) * kStride * 4 +
+               size_t(PCAP) * (MODE == kSpread || MODE == kRaw ? 32 : 16) +
+               (MODE == kRaw ? size_t(kFrames) * kMStride : 0);
     }
     // Buffers, records, then the mbarriers: full[BUFS], empty[BUFS], record[kMetaBufs].
     template <int MODE>
@@ -1066,6 +1071,12 @@ using Bt8 = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, 2, (DG_BT8_ROWS > 16 ? 
                   DG_BT8_BUFS, DG_BT8_AHEAD>;  // mapping 8
 static_assert(Bt7::smem_bytes<kSpread>() <= 227 * 1024, "mapping 7 fits shared memory");
 static_assert(Bt8::smem_bytes<kSpread>() <= 227 * 1024, "mapping 8 fits shared memory");
+// Per-frame masks on mapping 8's tiles (same rows and chunks, so the same
+// records): one frame per lane leaves registers for the four sums.
+using BtR = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, 1, 4, DG_BT8_BUFS, DG_BT8_AHEAD>;
+static_assert(BtR::kMetaWords == Bt8::kMetaWords && BtR::kMetaHead == Bt8::kMetaHead,
+              "masked tiles read mapping 8's chunk records");
+static_assert(BtR::smem_bytes<kRaw>() <= 227 * 1024, "masked tiles fit shared memory");
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -1122,7 +1133,8 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                   const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_rows,
                   double *__restrict__ out_i, double *__restrict__ out_s,
                   double *__restrict__ out_d, int *__restrict__ wait_err, int withhold,
-                  const double *__restrict__ raw_cnt, double *__restrict__ out_c, int raw) {
+                  const double *__restrict__ raw_cnt, double *__restrict__ out_c, int raw,
+                  const uint8_t *__restrict__ masks, int64_t mask_stride) {
     using S = StagedPx<P>;
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
@@ -1131,6 +1143,8 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     constexpr int NB = CFG::kBufs, NM = CFG::kMetaBufs, AH = CFG::kAhead, MA = CFG::kMetaAhead;
     constexpr int MH = CFG::kMetaHead, MW = CFG::kMetaWords;
     constexpr size_t BUF = CFG::template buf_bytes<MODE>();
+    constexpr bool WIDE = SPREAD || MODE == kRaw;  // 32-byte entry pairs
+    constexpr int MS = CFG::kMStride;
     extern __shared__ __align__(16) unsigned char smem[];
     const int groups = (n_frames + CFG::kFrames - 1) / CFG::kFrames;
     const int4 it = items[blockIdx.x / groups];
@@ -1150,6 +1164,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     auto mbuf = [&](int c) {
         return reinterpret_cast<int32_t *>(smem + size_t(NB) * BUF) + (c % NM) * MW;
     };
+    auto mkbuf = [&](int b) {  // mask rows (mode kRaw)
+        return smem + size_t(b) * BUF + size_t(CFG::kFrames) * STRIDE * 4 + size_t(PCAP) * 32;
+    };
     // full[b]: chunk in buffer b landed (every thread's copies and stores);
     // empty[b]: every warp has summed the chunk in buffer b; rec[m]: the
     // record in slot m landed.
@@ -1163,8 +1180,10 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         for (int m = 0; m < NM; ++m) mbar_init(rec + m, NT);
     }
     // Column DCAP of every frame row is read by padding pairs and holds 0.
-    for (int j = tid; j < NB * CFG::kFrames; j += NT)
+    for (int j = tid; j < NB * CFG::kFrames; j += NT) {
         pxbuf(j / CFG::kFrames)[(j % CFG::kFrames) * STRIDE + DCAP] = S(0);
+        if constexpr (MODE == kRaw) mkbuf(j / CFG::kFrames)[(j % CFG::kFrames) * MS + DCAP] = 0;
+    }
     __syncthreads();
 
     // Copy chunk c's record into its slot; every thread arrives on the
@@ -1188,6 +1207,21 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         const int k1 = min(ch.y, s0 + per), fw = warp / KS;
         S *dst = pxbuf(b) + fw * STRIDE;
         const P *base = frames + int64_t(f0 + fw) * n_pixels;
+        constexpr int KSTEP = (DCAP + 31) / 32;
+        unsigned mv[MODE == kRaw ? KSTEP : 1][FS];
+        if constexpr (MODE == kRaw) {
+#pragma unroll
+            for (int i = 0; i < KSTEP; ++i) {
+                const int k = s0 + lane + 32 * i;
+#pragma unroll
+                for (int j = 0; j < FS; ++j) {
+                    const int f = fw + j * FSTEP;
+                    mv[i][j] = k < k1 && f < nv
+                                   ? unsigned(__ldg(masks + int64_t(f0 + f) * mask_stride + mb[MH + k]))
+                                   : 0u;
+                }
+            }
+        }
         for (int k = s0 + lane; k < k1; k += 32) {
             const P *src = base + mb[MH + k];
 #pragma unroll
@@ -1202,7 +1236,19 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         float4 *pa = pabuf(b);
         for (int j = tid; j < ch.w; j += NT) {
             cp_async16(pa + j, pair_a + ch.z + j);
-            if (SPREAD) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
+            if (WIDE) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
+        }
+        if constexpr (MODE == kRaw) {
+            unsigned char *md = mkbuf(b);
+#pragma unroll
+            for (int i = 0; i < KSTEP; ++i) {
+                const int k = s0 + lane + 32 * i;
+#pragma unroll
+                for (int j = 0; j < FS; ++j) {
+                    const int f = fw + j * FSTEP;
+                    if (k < k1 && f < nv) md[f * MS + k] = static_cast<unsigned char>(mv[i][j]);
+                }
+            }
         }
         asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];\n" ::"r"(smem_addr(full + b))
                      : "memory");
@@ -1257,6 +1303,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + (lane + 32 * h) * STRIDE;
         const float4 *s_pa = pabuf(b);
         const float4 *s_pb = s_pa + PCAP;
+        const unsigned char *mk[F2];  // this lane's mask rows (mode kRaw)
+#pragma unroll
+        for (int h = 0; h < F2; ++h) mk[h] = mkbuf(b) + (lane + 32 * h) * MS;
         const int32_t *cp = mbuf(c) + 4;
         if constexpr (SPREAD) {
             if (o.x == c) {
@@ -1284,7 +1333,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
 #pragma unroll
             for (int u = 0; u < UU; ++u) {
                 ea[u] = s_pa[p + u];
-                if constexpr (SPREAD) eb[u] = s_pb[p + u];
+                if constexpr (WIDE) eb[u] = s_pb[p + u];
             }
 #pragma unroll
             for (int h = 0; h < F2; ++h) {
@@ -1293,6 +1342,25 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 for (int u = 0; u < UU; ++u) {
                     v0[u] = float(px[h][__float_as_int(ea[u].x)]);
                     v1[u] = float(px[h][__float_as_int(ea[u].y)]);
+                }
+                if constexpr (MODE == kRaw) {
+                    // Per-frame masks: {slot, slot, w, w}, {w*norm, w*norm, 0, 0};
+                    // a masked entry adds nothing to S, V, N or C, whatever its
+                    // pixel holds.
+#pragma unroll
+                    for (int u = 0; u < UU; ++u) {
+                        const bool l0 = mk[h][__float_as_int(ea[u].x)] == 0;
+                        const bool l1 = mk[h][__float_as_int(ea[u].y)] == 0;
+                        const f2 cc = pk(l0 ? ea[u].z : 0.f, l1 ? ea[u].w : 0.f);
+                        const float x0 = l0 ? v0[u] : 0.f, x1 = l1 ? v1[u] : 0.f;
+                        const f2 x = pk(x0, x1);
+                        acc[h][0].p = fma2(cc, x, acc[h][0].p);
+                        const f2 xp = is_unsigned_px<P>() ? x : pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f));
+                        acc[h][1].p = fma2(mul2(cc, cc), xp, acc[h][1].p);
+                        acc[h][2].p = add2(acc[h][2].p, pk(l0 ? eb[u].x : 0.f, l1 ? eb[u].y : 0.f));
+                        acc[h][3].p = add2(acc[h][3].p, cc);
+                    }
+                    continue;
                 }
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
@@ -1385,6 +1453,25 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             v[a] = acc[h][a].value();
         }
         const int64_t oo = int64_t(f0 + fl) * n_rows + row;
+        if constexpr (MODE == kRaw) {
+            // Sums of this frame's mask: raw (integrate1d_raw*) or normalised
+            // by the frame's own N (normalize_bin), as k_finalize_raw and
+            // k_finalize<kRaw> do from partial sums.
+            if (raw) {
+                out_i[oo] = v[0];
+                out_d[oo] = v[2];
+                if (out_s) out_s[oo] = v[1];
+                out_c[oo] = v[3];
+            } else {
+                const double n = v[2];
+                out_i[oo] = n == 0.0 ? 0.0 : v[0] / n;
+                if (out_s) {
+                    const double q = n == 0.0 ? 0.0 : v[1] / (n * n);
+                    out_s[oo] = sqrt(q > 0.0 ? q : 0.0);
+                }
+            }
+            continue;
+        }
         if (raw) {
             // Raw sums (integrate1d_raw*, integrate.rs:682-797): signal and
             // variance sums of the frame, the row's strict norm and weight sums.
@@ -1451,6 +1538,29 @@ __global__ void k_bt_fill(const int4 *__restrict__ desc, int64_t n_pairs,
         pair_a[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), c[0], c[1]);
         pair_as[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), cs[0], cs[1]);
         pair_b[i] = make_float4(n[0], n[1], cr[0], cr[1]);
+    }
+}
+
+// Pairs of the per-frame-mask bin tiles from the same layout: A {slot 0,
+// slot 1, w0, w1} and B {w0*norm, w1*norm, 0, 0} with the raw entries'
+// FP32 weights (k_pack_raw); padding entries are zero.
+__global__ void k_bt_fill_raw(const int4 *__restrict__ desc, int64_t n_pairs,
+                              const float4 *__restrict__ entry_raw, float4 *__restrict__ pair_a,
+                              float4 *__restrict__ pair_b) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pairs;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int4 d = desc[i];
+        float w[2] = {0.f, 0.f}, wn[2] = {0.f, 0.f};
+        const int k[2] = {d.z, d.w};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (k[h] < 0) continue;
+            const float4 e = entry_raw[k[h]];
+            w[h] = e.y;
+            wn[h] = e.z;
+        }
+        pair_a[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), w[0], w[1]);
+        pair_b[i] = make_float4(wn[0], wn[1], 0.f, 0.f);
     }
 }
 
@@ -1650,7 +1760,7 @@ void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, doub
 template <int MODE, typename P, class CFG>
 void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t n_pixels, int nf,
                  double *oi, double *os, double *od, cudaStream_t s, double *oc = nullptr,
-                 int raw = 0) {
+                 int raw = 0, const uint8_t *masks = nullptr, int64_t mask_stride = 0) {
     constexpr size_t smem = CFG::template smem_bytes<MODE>();
     auto kern = k_gather_bins<MODE, P, CFG>;
     DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -1658,11 +1768,12 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
     const int64_t grid = int64_t(bt.n_items) * groups;
     if (grid > INT32_MAX) fail(DG_UNSUPPORTED, "too many bin tiles for one launch");
     check_bin_tile_waits(t);
+    const float4 *pa = MODE == kSpread ? bt.pair_as.ptr : MODE == kRaw ? bt.pair_ra.ptr : bt.pair_a.ptr;
+    const float4 *pb = MODE == kRaw ? bt.pair_rb.ptr : bt.pair_b.ptr;
     kern<<<unsigned(grid), CFG::kThreads, smem, s>>>(
-        bt.item.ptr, bt.meta.ptr, MODE == kSpread ? bt.pair_as.ptr : bt.pair_a.ptr,
-        bt.pair_b.ptr, bt.org.ptr, t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr,
+        bt.item.ptr, bt.meta.ptr, pa, pb, bt.org.ptr, t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr,
         t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od, bt.wait_err.dev,
-        t.withhold_test, t.cnt.ptr, oc, raw);
+        t.withhold_test, t.cnt.ptr, oc, raw, masks, mask_stride);
 }
 
 // Launches lane mapping `variant`; returns true when the kernel wrote the
@@ -2046,8 +2157,11 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     out.pair_a.alloc(std::max<size_t>(n_pairs, 1));
     out.pair_as.alloc(std::max<size_t>(n_pairs, 1));
     out.pair_b.alloc(std::max<size_t>(n_pairs, 1));
-    DeviceArray<int4> desc;
+    DeviceArray<int4> &desc = out.desc;  // kept for the per-frame-mask pairs
     desc.alloc(std::max<size_t>(n_pairs, 1));
+    out.pair_ra.release();
+    out.pair_rb.release();
+    out.raw_built = false;
     DG_CUDA(cudaMemcpyAsync(out.item.ptr, items.data(), items.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, s));
     if (n_chunks)
@@ -2336,11 +2450,28 @@ namespace {
 
 template <typename P>
 bool launch_raw(GatherTable &t, const void *frames, int64_t n_pixels, int nf, int mode,
-                const uint8_t *masks, int64_t mask_stride, cudaStream_t s, double *o0 = nullptr,
-                double *o1 = nullptr, double *o2 = nullptr, double *o3 = nullptr) {
+                const uint8_t *masks, int64_t mask_stride, cudaStream_t s, bool raw, double *o0,
+                double *o1, double *o2, double *o3) {
     const P *fp = static_cast<const P *>(frames);
+    // Per-frame masks on a mapping-8 plan: the masked tiles write the raw
+    // sums (S, N, V, C in o0..o3) or the normalised results (o0, o1).
+    if (mode == kRaw && t.variant == 8 && t.bt[1].n_items > 0 && t.entry_raw.ptr) {
+        BinTiles &bt = t.bt[1];
+        if (!bt.raw_built) {
+            bt.pair_ra.alloc(bt.desc.count);
+            bt.pair_rb.alloc(bt.desc.count);
+            k_bt_fill_raw<<<148 * 8, 256, 0, s>>>(bt.desc.ptr, int64_t(bt.desc.count),
+                                                 t.entry_raw.ptr, bt.pair_ra.ptr, bt.pair_rb.ptr);
+            DG_CUDA(cudaGetLastError());
+            bt.raw_built = true;
+        }
+        if (raw) launch_bins<kRaw, P, BtR>(t, bt, fp, n_pixels, nf, o0, o2, o1, s, o3, 1, masks, mask_stride);
+        else launch_bins<kRaw, P, BtR>(t, bt, fp, n_pixels, nf, o0, o1, nullptr, s, nullptr, 0, masks, mask_stride);
+        DG_CUDA(cudaGetLastError());
+        return true;
+    }
     // Raw sums over the plan mask on a bin-tile plan: the tiles write them.
-    if (o0 && mode != kRaw && gather_variant_needs_tiles(t.variant) &&
+    if (raw && mode != kRaw && gather_variant_needs_tiles(t.variant) &&
         t.bt[t.variant - 7].n_items > 0) {
         const BinTiles &bt = t.bt[t.variant - 7];
         if (mode == kErrors) {
@@ -2398,10 +2529,12 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
                 DG_CUDA(cudaEventRecord(ev->first, s));
             }
             ++t.launches;
-            double *r0 = raw ? at(o0) : nullptr, *r1 = at(o1), *r2 = errors ? at(o2) : nullptr,
-                   *r3 = at(o3);
+            // raw: S, N, V, C; normalised (per-frame masks only): I, sigma
+            double *r0 = at(o0), *r1 = at(o1), *r2 = raw && errors ? at(o2) : nullptr,
+                   *r3 = raw ? at(o3) : nullptr;
+            if (!raw && !errors) r1 = nullptr;
 #define DG_RAW_CALL(T) \
-    done = launch_raw<T>(t, fp, n_pixels, nf, mode, mp, mask_stride, s, r0, r1, r2, r3)
+    done = launch_raw<T>(t, fp, n_pixels, nf, mode, mp, mask_stride, s, raw, r0, r1, r2, r3)
             switch (dtype) {
             case DG_U16: DG_RAW_CALL(uint16_t); break;
             case DG_U32: DG_RAW_CALL(uint32_t); break;

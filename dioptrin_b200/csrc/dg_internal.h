@@ -243,11 +243,17 @@ struct BinTiles {
     DeviceArray<int32_t> meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
     DeviceArray<int4> org;         // per row {chunk in tile (-1: none), slot, entry, row end}
     DeviceArray<float4> pair_a, pair_as, pair_b;
+    // Per pair {slot 0, slot 1, entry 0, entry 1}, kept to build the
+    // per-frame-mask pairs {slot, slot, w, w}, {w*norm, w*norm} on first use.
+    DeviceArray<int4> desc;
+    DeviceArray<float4> pair_ra, pair_rb;
+    bool raw_built = false;
     // Set by k_gather_bins when a wait of its chunk pipeline gave up.
     PinnedFlag wait_err;
     int64_t bytes() const {
         return int64_t(item.bytes() + meta.bytes() + org.bytes() + pair_a.bytes() +
-                       pair_as.bytes() + pair_b.bytes());
+                       pair_as.bytes() + pair_b.bytes() + desc.bytes() + pair_ra.bytes() +
+                       pair_rb.bytes());
     }
 };
 

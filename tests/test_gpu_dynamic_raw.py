@@ -62,9 +62,17 @@ def _oracle_dynamic(oracle, ref, frame, mask):
     return i, sg, (s, n, v, c)
 
 
+# None: the plan's tuned mapping (entry-lane gather with per-frame masks);
+# 8: the masked bin tiles on mapping 8's tiles.
+VARIANTS = [None, 8]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("dtype", ["uint16", "uint32", "int32", "float32", "float64"])
-def test_dynamic_masks_match_the_oracle(dg, oracle, ref, dtype):
+def test_dynamic_masks_match_the_oracle(dg, oracle, ref, dtype, variant):
     plan = _integrator(dg).prepare_dynamic1d(SHAPE, NB)
+    if variant is not None:
+        plan.cuda_plan.gather_variant = variant
     frames = np.random.default_rng(1).poisson(50.0, (5,) + SHAPE).astype(dtype)
     masks = _masks(5, 2)
     if dtype.startswith("float"):
@@ -80,8 +88,11 @@ def test_dynamic_masks_match_the_oracle(dg, oracle, ref, dtype):
     plan.close()
 
 
-def test_shared_mask_and_worker_api(dg, oracle, ref):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_shared_mask_and_worker_api(dg, oracle, ref, variant):
     dyn = _integrator(dg).prepare_dynamic1d(SHAPE, NB)
+    if variant is not None:
+        dyn.cuda_plan.gather_variant = variant
     assert dyn.shape == SHAPE and dyn.n_points == NB
     frames = np.random.default_rng(3).poisson(30.0, (4,) + SHAPE).astype(np.uint32)
     mask = _masks(1, 4)[0]
@@ -183,8 +194,11 @@ def test_raw_sums_with_the_plan_mask(dg, oracle, ref, dtype, variant):
     plan.close()
 
 
-def test_raw_sums_with_per_frame_masks(dg, oracle, ref):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_raw_sums_with_per_frame_masks(dg, oracle, ref, variant):
     plan = _integrator(dg).prepare_dynamic1d(SHAPE, NB).cuda_plan
+    if variant is not None:
+        plan.gather_variant = variant
     frames = np.random.default_rng(11).poisson(60.0, (4,) + SHAPE).astype(np.uint16)
     masks = _masks(4, 12)
     res = plan.integrate_raw_stack(frames, masks, with_variance=True)

@@ -1198,17 +1198,21 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     // Stage chunk c into buffer c % NB (its record is in shared memory); every
     // thread arrives on the buffer's full barrier, counted once its copies
     // have landed and ordering its plain stores (2-byte pixels) before it.
-    auto stage = [&](int c) {
+    // Mode kRaw: a chunk's mask bytes, loaded with its copies and stored into
+    // shared memory only after the warp has summed the chunk before it, so
+    // the loads' latency hides behind that work.
+    constexpr int KS = CFG::kSlices, FS = CFG::kStageFrames, FSTEP = CFG::kRows / KS;
+    constexpr int KSTEP = (DCAP + 31) / 32;
+    unsigned mv[MODE == kRaw ? KSTEP : 1][FS];
+    // The first of two halves of staging chunk c: mask loads and copies.
+    auto stage_issue = [&](int c) {
         const int b = c % NB;
         const int32_t *mb = mbuf(c);
         const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
-        constexpr int KS = CFG::kSlices, FS = CFG::kStageFrames, FSTEP = CFG::kRows / KS;
         const int per = (ch.y + KS - 1) / KS, s0 = (warp % KS) * per;
         const int k1 = min(ch.y, s0 + per), fw = warp / KS;
         S *dst = pxbuf(b) + fw * STRIDE;
         const P *base = frames + int64_t(f0 + fw) * n_pixels;
-        constexpr int KSTEP = (DCAP + 31) / 32;
-        unsigned mv[MODE == kRaw ? KSTEP : 1][FS];
         if constexpr (MODE == kRaw) {
 #pragma unroll
             for (int i = 0; i < KSTEP; ++i) {
@@ -1238,7 +1242,16 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             cp_async16(pa + j, pair_a + ch.z + j);
             if (WIDE) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
         }
+    };
+    // The second half: mask stores, then this thread's arrival on the
+    // buffer's full barrier.
+    auto stage_finish = [&](int c) {
+        const int b = c % NB;
         if constexpr (MODE == kRaw) {
+            const int32_t *mb = mbuf(c);
+            const int dn = mb[0];
+            const int per = (dn + KS - 1) / KS, s0 = (warp % KS) * per;
+            const int k1 = min(dn, s0 + per), fw = warp / KS;
             unsigned char *md = mkbuf(b);
 #pragma unroll
             for (int i = 0; i < KSTEP; ++i) {
@@ -1253,6 +1266,10 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];\n" ::"r"(smem_addr(full + b))
                      : "memory");
         mbar_arrive(full + b);
+    };
+    auto stage = [&](int c) {
+        stage_issue(c);
+        stage_finish(c);
     };
 
     // This warp's row: accumulators, fold counter and origin of each of the
@@ -1282,11 +1299,19 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     }
     for (int c = 0; c < nch; ++c) {
         const int j = c + AH;
+        bool pending = false;  // chunk j's second staging half, after chunk c
         if (j < nch) {
             if (ok && j >= NB) ok = mbar_wait(empty + j % NB, unsigned(j / NB - 1) & 1u);
             if (ok && j + MA < nch) stage_meta(j + MA);
             if (ok) ok = mbar_wait(rec + j % NM, unsigned(j / NM) & 1u);
-            if (ok) stage(j);
+            if (ok) {
+                if constexpr (MODE == kRaw) {
+                    stage_issue(j);
+                    pending = true;
+                } else {
+                    stage(j);
+                }
+            }
         }
         if (ok) ok = mbar_wait(full + c % NB, unsigned(c / NB) & 1u);
         if (!__all_sync(0xffffffffu, ok)) {
@@ -1295,6 +1320,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         }
         const int b = c % NB;
         if (r >= nrows) {
+            if (pending) stage_finish(j);
             if (lane == 0 && signal) mbar_arrive(empty + b);
             continue;
         }
@@ -1424,6 +1450,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 fold();
             }
         }
+        if (pending) stage_finish(j);
         __syncwarp();
         if (lane == 0 && signal) mbar_arrive(empty + b);
     }

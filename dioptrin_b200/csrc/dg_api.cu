@@ -698,9 +698,10 @@ dg_status dg_plan_autotune(dg_plan *plan, const void *d_frames, int32_t dtype, i
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
-        // bin tiles pay off only with enough frames to fill the GPU
-        if (n_frames > dg::kBinTileMinFrames)
-            for (int v : {7, 8}) dg::ensure_bin_tiles(plan->gather, plan->table, v, s);
+        // bin tiles pay off only when a launch fills the GPU
+        for (int v : {7, 8})
+            if (dg::bin_tiles_fill_gpu(plan->gather, v, n_frames))
+                dg::ensure_bin_tiles(plan->gather, plan->table, v, s);
         std::vector<double> each;
         const int v = dg::autotune_gather(plan->gather, d_frames, dtype,
                                           int64_t(plan->dim1) * plan->dim2, n_frames, flags, s,

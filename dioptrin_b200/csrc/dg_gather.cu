@@ -1062,6 +1062,11 @@ struct BtCfg {
 #ifndef DG_BT8_AHEAD
 #define DG_BT8_AHEAD 1
 #endif
+// 2-byte pixels of the bin tiles loaded with a chunk's copies and stored
+// after the chunk before it is summed (1), or stored as they arrive (0).
+#ifndef DG_BT_DEFER_PX
+#define DG_BT_DEFER_PX 1
+#endif
 // Bin tiles run largest first (1) or in bin order (0).
 #ifndef DG_BT_LARGEST_FIRST
 #define DG_BT_LARGEST_FIRST 1
@@ -1202,8 +1207,13 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     // shared memory only after the warp has summed the chunk before it, so
     // the loads' latency hides behind that work.
     constexpr int KS = CFG::kSlices, FS = CFG::kStageFrames, FSTEP = CFG::kRows / KS;
-    constexpr int KSTEP = (DCAP + 31) / 32;
+    constexpr int KSTEP = ((DCAP + KS - 1) / KS + 31) / 32;
     unsigned mv[MODE == kRaw ? KSTEP : 1][FS];
+    // 2-byte pixels are loaded, not copied: their loads are deferred the same
+    // way where the registers allow it (512 threads, no spread).
+    constexpr bool DEFER_PX = DG_BT_DEFER_PX && sizeof(P) != 4 && MODE != kSpread && NT <= 512;
+    constexpr bool DEFER = MODE == kRaw || DEFER_PX;
+    S pv[DEFER_PX ? KSTEP : 1][FS];
     // The first of two halves of staging chunk c: mask loads and copies.
     auto stage_issue = [&](int c) {
         const int b = c % NB;
@@ -1226,15 +1236,27 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 }
             }
         }
-        for (int k = s0 + lane; k < k1; k += 32) {
-            const P *src = base + mb[MH + k];
+        if constexpr (DEFER_PX) {
 #pragma unroll
-            for (int j = 0; j < FS; ++j) {
-                if (fw + j * FSTEP >= nv) break;
-                if constexpr (sizeof(P) == 4)
-                    cp_async4(dst + j * FSTEP * STRIDE + k, src + int64_t(j * FSTEP) * n_pixels);
-                else
-                    dst[j * FSTEP * STRIDE + k] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
+            for (int i = 0; i < KSTEP; ++i) {
+                const int k = s0 + lane + 32 * i;
+#pragma unroll
+                for (int j = 0; j < FS; ++j)
+                    pv[i][j] = k < k1 && fw + j * FSTEP < nv
+                                   ? load_px<P>(base + mb[MH + k] + int64_t(j * FSTEP) * n_pixels, 0u)
+                                   : S(0);
+            }
+        } else {
+            for (int k = s0 + lane; k < k1; k += 32) {
+                const P *src = base + mb[MH + k];
+#pragma unroll
+                for (int j = 0; j < FS; ++j) {
+                    if (fw + j * FSTEP >= nv) break;
+                    if constexpr (sizeof(P) == 4)
+                        cp_async4(dst + j * FSTEP * STRIDE + k, src + int64_t(j * FSTEP) * n_pixels);
+                    else
+                        dst[j * FSTEP * STRIDE + k] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
+                }
             }
         }
         float4 *pa = pabuf(b);
@@ -1247,6 +1269,19 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     // buffer's full barrier.
     auto stage_finish = [&](int c) {
         const int b = c % NB;
+        if constexpr (DEFER_PX) {
+            const int dn = mbuf(c)[0];
+            const int per = (dn + KS - 1) / KS, s0 = (warp % KS) * per;
+            const int k1 = min(dn, s0 + per), fw = warp / KS;
+            S *dst = pxbuf(b) + fw * STRIDE;
+#pragma unroll
+            for (int i = 0; i < KSTEP; ++i) {
+                const int k = s0 + lane + 32 * i;
+#pragma unroll
+                for (int j = 0; j < FS; ++j)
+                    if (k < k1 && fw + j * FSTEP < nv) dst[j * FSTEP * STRIDE + k] = pv[i][j];
+            }
+        }
         if constexpr (MODE == kRaw) {
             const int32_t *mb = mbuf(c);
             const int dn = mb[0];
@@ -1305,7 +1340,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             if (ok && j + MA < nch) stage_meta(j + MA);
             if (ok) ok = mbar_wait(rec + j % NM, unsigned(j / NM) & 1u);
             if (ok) {
-                if constexpr (MODE == kRaw) {
+                if constexpr (DEFER) {
                     stage_issue(j);
                     pending = true;
                 } else {
@@ -2253,6 +2288,15 @@ void ensure_bin_tiles(GatherTable &t, const DeviceCsr &table, int variant, cudaS
 
 bool gather_variant_needs_tiles(int variant) { return variant == 7 || variant == 8; }
 
+bool bin_tiles_fill_gpu(const GatherTable &t, int variant, int64_t n_frames) {
+    if (!gather_variant_needs_tiles(variant)) return false;
+    const int64_t rows = variant == 7 ? Bt7::kRows : Bt8::kRows;
+    const int64_t per = variant == 7 ? Bt7::kFrames : Bt8::kFrames;
+    const int64_t nf = std::min<int64_t>(n_frames, 256);
+    const int64_t ctas = (int64_t(t.n_rows) + rows - 1) / rows * ((nf + per - 1) / per);
+    return 2 * nf >= per && ctas >= 2 * 148;
+}
+
 void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1, int32_t dim2,
                        int32_t strip_rows, cudaStream_t s, GatherTable &out) {
     out.n_rows = int32_t(table.n_rows);
@@ -2648,7 +2692,7 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     try {
         for (int v = 0; v < kVariantCount; ++v) {
             if (!gather_variant_available(t, v) ||
-                (gather_variant_needs_tiles(v) && n_frames <= kBinTileMinFrames)) {
+                (gather_variant_needs_tiles(v) && !bin_tiles_fill_gpu(t, v, n_frames))) {
                 if (each) (*each)[size_t(v)] = -1.0;
                 continue;
             }

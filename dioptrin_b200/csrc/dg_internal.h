@@ -336,9 +336,10 @@ bool gather_variant_needs_tiles(int variant);
 // pipeline wait; bin_tile_wait_failed only reports and clears it.
 bool bin_tile_wait_failed(const GatherTable &t);
 void check_bin_tile_waits(const GatherTable &t);
-// The autotuner times the bin-tile mapping only for batches of more frames
-// than this (one tile per CTA: smaller batches leave SMs idle).
-constexpr int64_t kBinTileMinFrames = 64;
+// Whether the autotuner times bin-tile mapping `variant` (7 or 8) for a
+// batch of n_frames: a launch must give every SM at least two CTAs (tiles
+// times frame groups) and fill at least half of each CTA's frames.
+bool bin_tiles_fill_gpu(const GatherTable &t, int variant, int64_t n_frames);
 void prepare_raw(GatherTable &t, const DeviceCsr &table, const double *d_norm, cudaStream_t s);
 void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                     int64_t n_frames, const uint8_t *d_masks, int64_t mask_stride, uint32_t flags,

@@ -122,8 +122,9 @@ def test_autotune_keeps_a_valid_mapping(dg, oracle, case):
     dev = torch.from_numpy(frames).cuda()
     v, ms = plan.autotune(dev, errors=True, azimuthal_std=True)
     assert 0 <= v < _variant_count(dg, plan) == len(ms)
-    # every mapping runs on this table; the bin tiles are timed only for
-    # batches of more than 64 frames (-1: not timed)
+    # every mapping runs on this table; the bin tiles are timed only when a
+    # launch fills the GPU (4 frames fill less than half of a tile's frames;
+    # -1: not timed)
     assert all(t > 0 for t in ms[:7]) and all(t == -1 for t in ms[7:])
     assert ms[v] == min(t for t in ms if t > 0)
     assert plan.gather_variant == v

@@ -116,3 +116,25 @@ def test_pinned_batches(dg, dtype):
         plan.alloc_pinned_batch(2, "int8")
     del buf
     plan.close()
+
+
+def test_flip_vertical_per_frame_masks_on_bin_tiles(dg):
+    # The masked bin tiles read each frame's mask at the pixel indices the
+    # flip remapped; flipped frames with flipped masks must give the detector
+    # order's results bit for bit, normalised and raw.
+    det = _integrator(dg, mask=False).prepare_dynamic1d(SHAPE, 70)
+    flip = _integrator(dg, mask=False).prepare_dynamic1d(SHAPE, 70, input_order="flip_vertical")
+    for p in (det, flip):
+        p.cuda_plan.gather_variant = 8
+    frames = np.random.default_rng(6).poisson(35.0, (5,) + SHAPE).astype(np.uint32)
+    masks = (np.random.default_rng(7).random((5,) + SHAPE) < 0.15).astype(np.uint8)
+    ff = np.ascontiguousarray(frames[:, ::-1, :])
+    fm = np.ascontiguousarray(masks[:, ::-1, :])
+    _eq(flip.cuda_plan.integrate_dynamic_stack(ff, fm, True),
+        det.cuda_plan.integrate_dynamic_stack(frames, masks, True))
+    for a, b in zip(flip.cuda_plan.integrate_raw_stack(ff, fm, with_variance=True),
+                    det.cuda_plan.integrate_raw_stack(frames, masks, with_variance=True)):
+        _eq((a.sum_signal, a.sum_norm, a.sum_variance, a.count),
+            (b.sum_signal, b.sum_norm, b.sum_variance, b.count))
+    det.close()
+    flip.close()

@@ -2240,6 +2240,9 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         DG_CUDA(cudaGetLastError());
     }
     DG_CUDA(cudaStreamSynchronize(s));
+    // Only mapping 8's tiles carry per-frame masks (BtR); the others drop the
+    // descriptor once their pairs are filled.
+    if (!std::is_same<CFG, Bt8>::value) desc.release();
 }
 
 namespace {

@@ -1629,70 +1629,82 @@ __global__ void k_bt_fill_raw(const int4 *__restrict__ desc, int64_t n_pairs,
 // One thread per (frame, row): fold the row's segment partials in strip
 // order in FP64 and normalise (normalize_bin, prepared.rs:985-996; the
 // spread's closing formulas, azimuthal.rs:96-104).
+constexpr int kFinRows = 8;  // rows per k_finalize CTA (x 32 frames)
 template <int MODE, typename P>
-__global__ void k_finalize(const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
-                           const int32_t *__restrict__ seg_ids, const int4 *__restrict__ segs,
-                           const double *__restrict__ den, const double *__restrict__ den_std,
-                           const double *__restrict__ den_f32,
-                           const int32_t *__restrict__ valid_std,
-                           const int32_t *__restrict__ first_valid,
-                           const float4 *__restrict__ entry_std, const P *__restrict__ frames,
-                           int64_t n_pixels, int n_rows, int n_segments, int n_frames,
-                           double *__restrict__ out_i, double *__restrict__ out_s,
-                           double *__restrict__ out_d) {
+__global__ void __launch_bounds__(256)
+    k_finalize(const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
+               const int32_t *__restrict__ seg_ids, const int4 *__restrict__ segs,
+               const double *__restrict__ den, const double *__restrict__ den_std,
+               const double *__restrict__ den_f32, const int32_t *__restrict__ valid_std,
+               const int32_t *__restrict__ first_valid, const float4 *__restrict__ entry_std,
+               const P *__restrict__ frames, int64_t n_pixels, int n_rows, int n_segments,
+               int n_frames, double *__restrict__ out_i, double *__restrict__ out_s,
+               double *__restrict__ out_d) {
+    // A CTA takes kFinRows rows x 32 frames: lanes run over frames while the
+    // partial sums are read (frame-contiguous), the results go through
+    // shared memory and are written row-contiguous for each frame.
     constexpr int NA = NAcc<MODE, P>::value;
-    int64_t id = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (id >= int64_t(n_rows) * n_frames) return;
-    int f = int(id % n_frames), r = int(id / n_frames);
-    double v[NA];
-    for (int a = 0; a < NA; ++a) v[a] = 0.0;
-    const int k0 = row_seg[r], k1 = row_seg[r + 1];
-    for (int k = k0; k < k1; ++k) {
-        const double *p = partial + int64_t(seg_ids[k]) * NA * n_frames + f;
-        for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
-    }
-    int64_t o = int64_t(f) * n_rows + r;
-    if (MODE == kRaw) {  // denominators of this frame's mask
-        const double n = v[2];
-        out_i[o] = n == 0.0 ? 0.0 : v[0] / n;
-        if (out_s) {
+    __shared__ double s_o[3][kFinRows][33];
+    const int fl = threadIdx.x & 31, rl = threadIdx.x >> 5;
+    const int r0 = blockIdx.x * kFinRows, fb = blockIdx.y * 32;
+    const int r = r0 + rl, f = fb + fl;
+    double ri = 0.0, rs = 0.0, rd = 0.0;
+    if (r < n_rows && f < n_frames) {
+        double v[NA];
+        for (int a = 0; a < NA; ++a) v[a] = 0.0;
+        const int k0 = row_seg[r], k1 = row_seg[r + 1];
+        for (int k = k0; k < k1; ++k) {
+            const double *p = partial + int64_t(seg_ids[k]) * NA * n_frames + f;
+            for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
+        }
+        if (MODE == kRaw) {  // denominators of this frame's mask
+            const double n = v[2];
+            ri = n == 0.0 ? 0.0 : v[0] / n;
             const double q = n == 0.0 ? 0.0 : v[1] / (n * n);
-            out_s[o] = sqrt(q > 0.0 ? q : 0.0);
+            rs = sqrt(q > 0.0 ? q : 0.0);
+        } else if (MODE != kSpread) {
+            const double n = den[r];
+            ri = n == 0.0 ? 0.0 : v[0] / n;
+            if (MODE == kErrors) {
+                const double q = n == 0.0 ? 0.0 : v[1] / (n * n);
+                rs = sqrt(q > 0.0 ? q : 0.0);
+            }
+        } else {
+            int valid = valid_std[r];
+            double sw = den_std[r], wf = den_f32[r];
+            if (NA == 5) {
+                valid -= int(v[NA - 1] + 0.5);
+                sw -= v[NA - 2];
+                wf -= v[NA - 2];
+            }
+            if (valid <= 0 || !(sw > 0.0)) {
+                rd = __longlong_as_double(0x7ff8000000000000ll);
+            } else {
+                // A = sum c*(s - o*n) = S - o * sum c*n over the same FP32 weights.
+                const int row_end = k0 < k1 ? segs[seg_ids[k0]].w : 0;
+                const float org = row_origin<P>(entry_std, first_valid[r], row_end,
+                                                frames + int64_t(f) * n_pixels);
+                const double a1 = v[0] - double(org) * wf;
+                ri = v[0] / sw;
+                rs = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
+                const double mean = a1 / sw;
+                const double m2 = v[2] - mean * a1;
+                const double q = m2 / sw;
+                rd = sqrt(q > 0.0 ? q : 0.0);
+            }
         }
-        return;
     }
-    if (MODE != kSpread) {
-        double n = den[r];
-        out_i[o] = n == 0.0 ? 0.0 : v[0] / n;
-        if (MODE == kErrors) {
-            double q = n == 0.0 ? 0.0 : v[1] / (n * n);
-            out_s[o] = sqrt(q > 0.0 ? q : 0.0);
-        }
-        return;
-    }
-    int valid = valid_std[r];
-    double sw = den_std[r], wf = den_f32[r];
-    if (NA == 5) {
-        valid -= int(v[4] + 0.5);
-        sw -= v[3];
-        wf -= v[3];
-    }
-    if (valid <= 0 || !(sw > 0.0)) {
-        out_i[o] = 0.0;
-        if (out_s) out_s[o] = 0.0;
-        out_d[o] = __longlong_as_double(0x7ff8000000000000ll);
-        return;
-    }
-    // A = sum c*(s - o*n) = S - o * sum c*n over the same FP32 weights.
-    const int row_end = k0 < k1 ? segs[seg_ids[k0]].w : 0;
-    const float org = row_origin<P>(entry_std, first_valid[r], row_end, frames + int64_t(f) * n_pixels);
-    const double a1 = v[0] - double(org) * wf;
-    out_i[o] = v[0] / sw;
-    if (out_s) out_s[o] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
-    const double mean = a1 / sw;
-    const double m2 = v[2] - mean * a1;
-    const double q = m2 / sw;
-    out_d[o] = sqrt(q > 0.0 ? q : 0.0);
+    s_o[0][rl][fl] = ri;
+    s_o[1][rl][fl] = rs;
+    s_o[2][rl][fl] = rd;
+    __syncthreads();
+    const int wr = threadIdx.x % kFinRows, wf = threadIdx.x / kFinRows;
+    const int rr = r0 + wr, ff = fb + wf;
+    if (rr >= n_rows || ff >= n_frames) return;
+    const int64_t o = int64_t(ff) * n_rows + rr;
+    out_i[o] = s_o[0][wr][wf];
+    if (MODE != kIntensity && out_s) out_s[o] = s_o[1][wr][wf];
+    if (MODE == kSpread) out_d[o] = s_o[2][wr][wf];
 }
 
 // Raw sums per (frame, row) (IntermediateResult1d, lut/integrate.rs:372-379):
@@ -1902,9 +1914,8 @@ bool launch_typed(const GatherTable &t, int variant, const void *frames, int64_t
 template <int MODE, typename P>
 void launch_finalize(GatherTable &t, const void *frames, int64_t n_pixels, int nf, double *oi,
                      double *os, double *od, cudaStream_t s) {
-    const int64_t total = int64_t(t.n_rows) * nf;
-    const unsigned blocks = unsigned((total + 255) / 256);
-    k_finalize<MODE, P><<<blocks, 256, 0, s>>>(
+    const dim3 grid(unsigned((t.n_rows + kFinRows - 1) / kFinRows), unsigned((nf + 31) / 32));
+    k_finalize<MODE, P><<<grid, 32 * kFinRows, 0, s>>>(
         t.partial.ptr, t.row_seg.ptr, t.seg_ids.ptr, t.seg.ptr, t.den.ptr, t.den_std.ptr,
         t.den_f32.ptr, t.valid_std.ptr, t.first_valid.ptr, t.entry_std.ptr,
         static_cast<const P *>(frames), n_pixels, t.n_rows, t.n_segments, nf, oi, os, od);
@@ -2792,9 +2803,9 @@ void noalloc_launch(const GatherTable &t, double *partial, const void *frames, i
     if (t.n_units > 0) done = launch_typed<P>(t, t.variant, frames, n_pixels, nf, mode, partial,
                                               oi, os, od, s);
     if (t.n_rows > 0 && !done) {
-        const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);
+        const dim3 grid(unsigned((t.n_rows + kFinRows - 1) / kFinRows), unsigned((nf + 31) / 32));
 #define DG_NOALLOC_FINALIZE(M)                                                                 \
-    k_finalize<M, P><<<blocks, 256, 0, s>>>(                                                   \
+    k_finalize<M, P><<<grid, 32 * kFinRows, 0, s>>>(                                           \
         partial, t.row_seg.ptr, t.seg_ids.ptr, t.seg.ptr, t.den.ptr, t.den_std.ptr,           \
         t.den_f32.ptr, t.valid_std.ptr, t.first_valid.ptr, t.entry_std.ptr, fp, n_pixels,      \
         t.n_rows, t.n_segments, nf, oi, os, od)

@@ -100,12 +100,14 @@ def test_every_mapping_keeps_a_nan_in_its_own_bins(dg, oracle, case):
 
 def test_every_mapping_gives_batch_equal_to_single(dg, case):
     plan = case["plan"]
-    frames = np.random.default_rng(8).poisson(40.0, (11,) + case["shape"]).astype(np.uint16)
+    # 70 frames: the finalize and the bin tiles take frames in groups of 32
+    # and 64, so frames 35 and 69 sit in later groups than frame 0
+    frames = np.random.default_rng(8).poisson(40.0, (70,) + case["shape"]).astype(np.uint16)
     for v in range(_variant_count(dg, plan)):
         plan.gather_variant = v
         for flags in [(False, False), (True, False), (True, True)]:
             I, S, D = plan.integrate_stack(frames, *flags)
-            for k in (0, 5, 10):
+            for k in (0, 35, 69):
                 i1, s1, d1 = plan.integrate_stack(frames[k], *flags)
                 assert np.array_equal(I[k], i1[0]), (v, flags, k)
                 if flags[0]:

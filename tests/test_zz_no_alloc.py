@@ -65,7 +65,8 @@ def test_noalloc_entry_matches_the_regular_entry_twice_in_a_row():
     for flags in (N.DG_ERRORS | N.DG_AZIMUTHAL_STD, N.DG_ERRORS, 0):
         frames_a = torch.from_numpy(gen.poisson(300.0, (5,) + shape).astype(np.uint32)).cuda()
         frames_b = torch.from_numpy(gen.poisson(80.0, (3,) + shape).astype(np.uint32)).cuda()
-        for frames in (frames_a, frames_b):  # two calls in a row, different contents
+        frames_c = torch.from_numpy(gen.poisson(50.0, (40,) + shape).astype(np.uint32)).cuda()
+        for frames in (frames_a, frames_b, frames_c):  # calls in a row, different contents
             ref = _run(L.dg_integrate_device, plan, frames, flags, nb)
             got = _run(L.dg_integrate_device_noalloc, plan, frames, flags, nb)
             _close(got[0], ref[0])

@@ -1711,27 +1711,40 @@ __global__ void __launch_bounds__(256)
 // S and V from the partial sums; N and C from them too for the per-frame-mask
 // gather, else the plan's strict FP64 denominator and weight sum.
 template <int MODE>
-__global__ void k_finalize_raw(const double *__restrict__ partial,
-                               const int32_t *__restrict__ row_seg,
-                               const int32_t *__restrict__ seg_ids, const double *__restrict__ den,
-                               const double *__restrict__ cnt, int n_rows, int n_frames,
-                               double *__restrict__ out_sig, double *__restrict__ out_norm,
-                               double *__restrict__ out_var, double *__restrict__ out_cnt) {
+__global__ void __launch_bounds__(256)
+    k_finalize_raw(const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
+                   const int32_t *__restrict__ seg_ids, const double *__restrict__ den,
+                   const double *__restrict__ cnt, int n_rows, int n_frames,
+                   double *__restrict__ out_sig, double *__restrict__ out_norm,
+                   double *__restrict__ out_var, double *__restrict__ out_cnt) {
+    // Tiles of kFinRows rows x 32 frames, written row-contiguous per frame
+    // through shared memory (as k_finalize).
     constexpr int NA = NAcc<MODE, float>::value;
-    int64_t id = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (id >= int64_t(n_rows) * n_frames) return;
-    int f = int(id % n_frames), r = int(id / n_frames);
+    __shared__ double s_o[4][kFinRows][33];
+    const int fl = threadIdx.x & 31, rl = threadIdx.x >> 5;
+    const int r0 = blockIdx.x * kFinRows, fb = blockIdx.y * 32;
+    const int r = r0 + rl, f = fb + fl;
     double v[NA];
     for (int a = 0; a < NA; ++a) v[a] = 0.0;
-    for (int k = row_seg[r]; k < row_seg[r + 1]; ++k) {
-        const double *p = partial + int64_t(seg_ids[k]) * NA * n_frames + f;
-        for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
+    if (r < n_rows && f < n_frames) {
+        for (int k = row_seg[r]; k < row_seg[r + 1]; ++k) {
+            const double *p = partial + int64_t(seg_ids[k]) * NA * n_frames + f;
+            for (int a = 0; a < NA; ++a) v[a] = __dadd_rn(v[a], p[int64_t(a) * n_frames]);
+        }
+        s_o[0][rl][fl] = v[0];
+        s_o[1][rl][fl] = NA > 1 ? v[1] : 0.0;
+        s_o[2][rl][fl] = MODE == kRaw ? v[NA > 2 ? 2 : 0] : den[r];
+        s_o[3][rl][fl] = MODE == kRaw ? v[NA > 3 ? 3 : 0] : cnt[r];
     }
-    const int64_t o = int64_t(f) * n_rows + r;
-    out_sig[o] = v[0];
-    if (out_var) out_var[o] = NA > 1 ? v[1] : 0.0;
-    out_norm[o] = MODE == kRaw ? v[NA > 2 ? 2 : 0] : den[r];
-    out_cnt[o] = MODE == kRaw ? v[NA > 3 ? 3 : 0] : cnt[r];
+    __syncthreads();
+    const int wr = threadIdx.x % kFinRows, wf = threadIdx.x / kFinRows;
+    const int rr = r0 + wr, ff = fb + wf;
+    if (rr >= n_rows || ff >= n_frames) return;
+    const int64_t o = int64_t(ff) * n_rows + rr;
+    out_sig[o] = s_o[0][wr][wf];
+    if (out_var) out_var[o] = s_o[1][wr][wf];
+    out_norm[o] = s_o[2][wr][wf];
+    out_cnt[o] = s_o[3][wr][wf];
 }
 
 // Entries for the per-frame-mask gather, {pixel, w, w*norm} in FP32 (the
@@ -2632,14 +2645,14 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
         }
         if (t.n_rows == 0 || done) continue;
         ++t.launches;
-        const unsigned blocks = unsigned((int64_t(t.n_rows) * nf + 255) / 256);
+        const dim3 grid(unsigned((t.n_rows + kFinRows - 1) / kFinRows), unsigned((nf + 31) / 32));
         if (raw) {
 #define DG_RAW_ARGS                                                                          \
     t.partial.ptr, t.row_seg.ptr, t.seg_ids.ptr, t.den.ptr, t.cnt.ptr, t.n_rows, nf, at(o0), \
         at(o1), errors ? at(o2) : nullptr, at(o3)
-            if (mode == kRaw) k_finalize_raw<kRaw><<<blocks, 256, 0, s>>>(DG_RAW_ARGS);
-            else if (mode == kErrors) k_finalize_raw<kErrors><<<blocks, 256, 0, s>>>(DG_RAW_ARGS);
-            else k_finalize_raw<kIntensity><<<blocks, 256, 0, s>>>(DG_RAW_ARGS);
+            if (mode == kRaw) k_finalize_raw<kRaw><<<grid, 32 * kFinRows, 0, s>>>(DG_RAW_ARGS);
+            else if (mode == kErrors) k_finalize_raw<kErrors><<<grid, 32 * kFinRows, 0, s>>>(DG_RAW_ARGS);
+            else k_finalize_raw<kIntensity><<<grid, 32 * kFinRows, 0, s>>>(DG_RAW_ARGS);
 #undef DG_RAW_ARGS
             DG_CUDA(cudaGetLastError());
         } else {

@@ -232,3 +232,21 @@ def test_integrator_raw_methods_and_2d(dg, oracle, ref):
                  raw2.sum_signal / np.where(raw2.sum_norm == 0, 1, raw2.sum_norm))
     _close(i, i2[0], i2.max())
     p2.close()
+
+
+@pytest.mark.parametrize("with_masks", [False, True])
+def test_raw_sums_batch_equals_single_frames(dg, with_masks):
+    # 40 frames: the raw finalize takes frames in groups of 32, so frames 33
+    # and 39 sit in a later group than frame 0; each must equal its own call.
+    plan = _integrator(dg).prepare_dynamic1d(SHAPE, NB).cuda_plan
+    plan.gather_variant = 5
+    frames = np.random.default_rng(21).poisson(45.0, (40,) + SHAPE).astype(np.uint32)
+    masks = _masks(40, 22) if with_masks else None
+    res = plan.integrate_raw_stack(frames, masks, with_variance=True)
+    for k in (0, 33, 39):
+        one = plan.integrate_raw_stack(frames[k:k + 1], None if masks is None else masks[k:k + 1],
+                                       with_variance=True)[0]
+        for a, b in ((res[k].sum_signal, one.sum_signal), (res[k].sum_norm, one.sum_norm),
+                     (res[k].sum_variance, one.sum_variance), (res[k].count, one.count)):
+            assert np.array_equal(a, b)
+    plan.close()

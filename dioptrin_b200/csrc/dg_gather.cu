@@ -1144,7 +1144,15 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
     constexpr int F2 = CFG::kF2, STRIDE = CFG::kStride, DCAP = CFG::kDCap, PCAP = CFG::kPCap;
-    constexpr int U2 = CFG::kU2, NT = CFG::kThreads, NW = CFG::kRows;
+    // Float pixels with the spread keep five sums per frame (the excluded
+    // non-finite weights): half the unroll keeps them in registers.
+#ifndef DG_BT_FLOAT_SPREAD_U2
+#define DG_BT_FLOAT_SPREAD_U2 2
+#endif
+    constexpr int U2 = (SPREAD && is_float_px<P>() && CFG::kU2 > DG_BT_FLOAT_SPREAD_U2)
+                           ? DG_BT_FLOAT_SPREAD_U2
+                           : CFG::kU2;
+    constexpr int NT = CFG::kThreads, NW = CFG::kRows;
     constexpr int NB = CFG::kBufs, NM = CFG::kMetaBufs, AH = CFG::kAhead, MA = CFG::kMetaAhead;
     constexpr int MH = CFG::kMetaHead, MW = CFG::kMetaWords;
     constexpr size_t BUF = CFG::template buf_bytes<MODE>();

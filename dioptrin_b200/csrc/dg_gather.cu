@@ -985,6 +985,12 @@ __global__ void __launch_bounds__(256)
 // With two frames per lane (mapping 8) every entry pair read from shared
 // memory serves 64 frames: half the broadcast reads per frame, at half the
 // chunk size.
+// The same kernel writes raw sums instead (flag `raw`: S and V, with the
+// row's strict N and C), and in mode kRaw applies per-frame masks on mapping
+// 8's tiles with one frame per lane (BtR): a chunk's mask bytes are staged
+// next to its pixels, and a masked entry adds nothing to S, V, N or C. Bytes
+// the kernel loads rather than copies (masks, 2-byte pixels) are loaded with
+// a chunk's copies and stored after the warp has summed the chunk before it.
 
 // One bin-tile layout: rows per tile (= warps per CTA: warp w owns row w),
 // chunk capacities, frames per lane, pairs per unrolled step and the chunk

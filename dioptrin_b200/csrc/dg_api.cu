@@ -179,9 +179,10 @@ int64_t dg_plan::device_bytes() const {
     b += gather.seg.bytes() + gather.unit.bytes() + gather.row_seg.bytes() +
          gather.seg_ids.bytes() + gather.first_valid.bytes() + gather.entry.bytes() +
          gather.entry_std.bytes() + gather.den.bytes() + gather.den_std.bytes() +
-         gather.den_f32.bytes() +
+         gather.entry_nlo.bytes() + gather.origin.bytes() +
          gather.valid_std.bytes() + gather.partial.bytes() + gather.fl_unit.bytes() +
          gather.fl_px.bytes() + gather.fl_pair_a.bytes() + gather.fl_pair_b.bytes() +
+         gather.fl_pair_c.bytes() +
          gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes() + gather.entry_raw.bytes() +
          gather.cnt.bytes() + gather.bt[0].bytes() + gather.bt[1].bytes();
     b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes() +
@@ -382,6 +383,30 @@ dg_status dg_integrate_device(dg_plan *plan, const void *d_frames, int32_t dtype
         dg::run_gather(plan->gather, d_frames, dtype, int64_t(plan->dim1) * plan->dim2, n_frames,
                        flags, plan->method.precision, d_i, (flags & DG_ERRORS) ? d_s : nullptr,
                        (flags & DG_AZIMUTHAL_STD) ? d_d : nullptr, s);
+    });
+}
+
+// Allocation-free integration: the partial sums go to the library's fixed
+// device array (dg::noalloc_scratch) instead of the plan's own, so nothing is
+// allocated once the plan exists. Every call on a device shares that array
+// and leaves its contents behind; calls that overlap on the GPU race on it.
+// Each launch's partial sums are written by its gather before its finalize
+// reads them, so nothing needs clearing between calls.
+dg_status dg_integrate_device_noalloc(dg_plan *plan, const void *d_frames, int32_t dtype,
+                                      int64_t n_frames, uint32_t flags, double *d_i, double *d_s,
+                                      double *d_d, void *stream) {
+    return guarded([&] {
+        check_frames(plan, d_frames, dtype, n_frames, flags, d_i, d_s, d_d);
+        if (n_frames == 0) return;
+        check_device_alignment(d_frames, dtype, d_i, d_s, d_d);
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceScope scope(plan->device);
+        size_t cap = 0;
+        double *scratch = dg::noalloc_scratch(&cap);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+        dg::run_gather(plan->gather, d_frames, dtype, int64_t(plan->dim1) * plan->dim2, n_frames,
+                       flags, plan->method.precision, d_i, (flags & DG_ERRORS) ? d_s : nullptr,
+                       (flags & DG_AZIMUTHAL_STD) ? d_d : nullptr, s, scratch, cap);
     });
 }
 

@@ -35,11 +35,18 @@
 // bit-identical results.
 //
 // Azimuthal spread (azimuthal.rs:48-118): with x = s/n, w = c*n and origin
-// o = x of the row's first valid entry, t = s - o*n (one FMA) gives
-// w*(x - o) = c*t and w*(x - o)^2 = (c/n)*t*t, so the shifted moments
-// B = sum (c/n)*t*t needs no division per pixel, A = sum c*t equals
-// S - o*sum(c*n) and is formed once per row in the finalize, and
-// m2 = B - A^2 / sum(w).
+// o = x of one valid entry of the row, t = s - o*n gives w*(x - o) = c*t
+// and w*(x - o)^2 = (c/n)*t*t, so the shifted moments A = sum c*t and
+// B = sum (c/n)*t*t need no division per pixel, and the reference's second
+// pass sum w*((x - o) - A/W)^2 equals m2 = B - A^2/W with W = sum w. The
+// shift is exact to the last bit of t: n is kept as an FP32 pair
+// (n_hi, n_lo) with n_hi + n_lo = n to 2^-48, t = (s - o*n_hi) - o*n_lo by
+// two FMAs, and A is accumulated from the same t (forming it as S - o*W
+// instead loses the products' rounding of S to the cancellation). Any
+// constant origin gives the same m2 and o only has to be the same for every
+// entry of a row, so its FP32 rounding is harmless; its distance from the
+// mean sets the cancellation in m2, so o is the row's heaviest valid entry
+// (row_origin) rather than the reference's first one.
 #include <algorithm>
 #include <climits>
 #include <type_traits>
@@ -79,16 +86,24 @@ constexpr bool is_float_px() {
 }
 
 // Accumulators per (segment, frame): S = sum c*s, then V = sum c^2*max(s,0),
-// then for the spread B = sum (c/n)*t^2, then for float pixels the weight
-// c*n and the count of non-finite pixels. The spread's first moment
-// A = sum c*t = S - o*sum c*n is formed in the finalize.
+// then for the spread B = sum (c/n)*t^2 and A = sum c*t, then for float
+// pixels the weight c*n and the count of non-finite pixels.
 template <int MODE, typename P>
 struct NAcc {
     static constexpr int value = MODE == kIntensity ? 1
                                  : MODE == kErrors  ? 2
                                  : MODE == kRaw     ? 4
-                                                    : (is_float_px<P>() ? 5 : 3);
+                                                    : (is_float_px<P>() ? 6 : 4);
 };
+constexpr int kSpreadA = 3;  // index of A among the spread's accumulators
+constexpr int kMaxAcc = 6;   // accumulators per (segment, frame), at most
+static_assert(NAcc<kSpread, float>::value <= kMaxAcc && NAcc<kRaw, float>::value <= kMaxAcc,
+              "partial sums are sized for kMaxAcc accumulators");
+
+// Accumulators per frame of a mode, for sizing partial sums at run time.
+inline int n_accumulators(int mode, bool float_px) {
+    return mode == kIntensity ? 1 : mode == kErrors ? 2 : mode == kRaw ? 4 : (float_px ? 6 : 4);
+}
 
 template <typename P>
 constexpr bool is_unsigned_px() {
@@ -134,20 +149,28 @@ __device__ __forceinline__ float load_px<double>(const double *__restrict__ f, u
     return __double2float_rn(__ldg(f + i));
 }
 
-// Origin o = s/n of the row's first valid entry in this frame
-// (azimuthal.rs:80-82): entries that are statically invalid carry c = 0, and
-// for float pixels a non-finite value moves on to the next entry.
+// Origin o = s/n of the spread's shift in this frame. The reference shifts
+// by the row's first valid entry (azimuthal.rs:80-82); the spread does not
+// depend on the shift, only its rounding does: the moments lose to
+// cancellation about (mean - o)^2 / variance, so this build shifts by the
+// row's heaviest valid entry (largest c*n, chosen at plan time), which sits
+// at the mean of a bin dominated by one pixel. A float pixel that is not
+// finite there hands the origin to the row's first valid finite entry
+// (entries that are statically invalid carry c = 0).
 template <typename P>
-__device__ __forceinline__ float row_origin(const float4 *__restrict__ entry_std, int first,
-                                            int row_end, const P *__restrict__ frame) {
-    if (first < 0) return 0.f;
-    int k = first;
-    float4 e = entry_std[k];
+__device__ __forceinline__ float row_origin(const float4 *__restrict__ entry_std, int origin,
+                                            int first, int row_end,
+                                            const P *__restrict__ frame) {
+    if (origin < 0) return 0.f;
+    float4 e = entry_std[origin];
     float s = load_px<P>(frame, uint32_t(__float_as_int(e.x)));
-    if (is_float_px<P>()) {
-        while (!isfinite(s) && ++k < row_end) {
-            e = entry_std[k];
-            if (e.y > 0.f) s = load_px<P>(frame, uint32_t(__float_as_int(e.x)));
+    if (is_float_px<P>() && !isfinite(s)) {
+        for (int k = first; k < row_end; ++k) {
+            const float4 ek = entry_std[k];
+            if (!(ek.y > 0.f)) continue;
+            e = ek;
+            s = load_px<P>(frame, uint32_t(__float_as_int(e.x)));
+            if (isfinite(s)) break;
         }
     }
     return __fdiv_rn(s, e.z);
@@ -187,13 +210,18 @@ __device__ __forceinline__ double reduce_scatter(double (&v)[V], int lane) {
 // sl, sl + SLICES, ...), 32 / SLICES lane groups take different frames, and
 // each lane carries FPL frames, so a task is (segment, 32 / SLICES * FPL
 // frames). U entries per lane per step have all their loads in flight.
+// One unit of the entry-lane gather, run by the whole CTA (k_gather runs unit
+// blockIdx.x; the work-queue gather runs the units it claims, several per
+// CTA). It ends with a CTA barrier, so the next unit may restage the shared
+// memory at once.
 template <int MODE, typename P, int SLICES, int FPL, int U>
-__global__ void __launch_bounds__(kThreads)
-    k_gather(const int2 *__restrict__ units, const int4 *__restrict__ segs,
-             const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
-             const int32_t *__restrict__ first_valid, const P *__restrict__ frames,
-             int64_t n_pixels, int n_frames, int n_segments, double *__restrict__ partial,
-             const uint8_t *__restrict__ masks, int64_t mask_stride) {
+__device__ __forceinline__ void gather_unit(
+    int unit, const int2 *__restrict__ units, const int4 *__restrict__ segs,
+    const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
+    const float *__restrict__ entry_nlo, const int32_t *__restrict__ first_valid,
+    const int32_t *__restrict__ origin_entry, const P *__restrict__ frames, int64_t n_pixels,
+    int n_frames, int n_segments, double *__restrict__ partial,
+    const uint8_t *__restrict__ masks, int64_t mask_stride) {
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool WIDE = MODE == kSpread || MODE == kRaw;  // 16-byte entries
     constexpr int GROUPS = 32 / SLICES;         // frame lane groups per warp
@@ -201,7 +229,7 @@ __global__ void __launch_bounds__(kThreads)
     static_assert(kFlush % U == 0, "flush cadence must be a multiple of the unroll");
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_off[kWarps + 1];
-    const int2 un = units[blockIdx.x];
+    const int2 un = units[unit];
     const int seg0 = un.x, nseg = un.y;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
@@ -253,7 +281,8 @@ __global__ void __launch_bounds__(kThreads)
         float origin[FPL];
 #pragma unroll
         for (int q = 0; q < FPL; ++q)
-            origin[q] = MODE == kSpread ? row_origin<P>(entry_std, first_valid[row], sg.w, fr[q])
+            origin[q] = MODE == kSpread ? row_origin<P>(entry_std, origin_entry[row],
+                                                        first_valid[row], sg.w, fr[q])
                                         : 0.f;
         AccDW acc[FPL][NA];
 #pragma unroll
@@ -313,14 +342,15 @@ __global__ void __launch_bounds__(kThreads)
                     else
                         e[u] = reinterpret_cast<const float4 *>(smem)[off + j];
                 }
-                float sv[U][FPL];
+                float sv[U][FPL], nlo[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < U; ++u) {
+                    const bool in = !CHECK || j0 + SLICES * u < len;
+                    nlo[u] = in ? __ldg(entry_nlo + sg.y + j0 + SLICES * u) : 0.f;
 #pragma unroll
                     for (int q = 0; q < FPL; ++q)
-                        sv[u][q] = !CHECK || j0 + SLICES * u < len
-                                       ? load_px<P>(fr[q], uint32_t(__float_as_int(e[u].x)))
-                                       : 0.f;
+                        sv[u][q] = in ? load_px<P>(fr[q], uint32_t(__float_as_int(e[u].x))) : 0.f;
+                }
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const float c = e[u].y, n = e[u].z, cr = e[u].w;
@@ -335,8 +365,9 @@ __global__ void __launch_bounds__(kThreads)
                         }
                         acc[q][0].fma(c, v);
                         acc[q][1].fma(c2, is_unsigned_px<P>() ? v : fmaxf(v, 0.f));
-                        const float t = __fmaf_rn(-origin[q], n, v);
+                        const float t = __fmaf_rn(-origin[q], nlo[u], __fmaf_rn(-origin[q], n, v));
                         acc[q][2].fma(__fmul_rn(cr, t), t);
+                        acc[q][kSpreadA].fma(c, t);
                     }
                 }
             } else {
@@ -434,6 +465,21 @@ __global__ void __launch_bounds__(kThreads)
             }
         }
     }
+    __syncthreads();
+}
+
+template <int MODE, typename P, int SLICES, int FPL, int U>
+__global__ void __launch_bounds__(kThreads)
+    k_gather(const int2 *__restrict__ units, const int4 *__restrict__ segs,
+             const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
+             const float *__restrict__ entry_nlo,
+             const int32_t *__restrict__ first_valid, const int32_t *__restrict__ origin_entry,
+             const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_segments,
+             double *__restrict__ partial, const uint8_t *__restrict__ masks,
+             int64_t mask_stride) {
+    gather_unit<MODE, P, SLICES, FPL, U>(blockIdx.x, units, segs, entry, entry_std, entry_nlo,
+                                         first_valid, origin_entry, frames, n_pixels, n_frames,
+                                         n_segments, partial, masks, mask_stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -537,9 +583,13 @@ struct Acc2 {
 
 // Dynamic shared memory of k_gather_fl: entry pairs, pixel list, one or
 // (double-buffered) two sets of 32 frame rows, piece-boundary slots.
+template <int MODE>
+constexpr size_t fl_pair_bytes() {
+    return MODE == kSpread ? 40 : 16;  // pair A, and B and C for the spread
+}
 template <int MODE, typename P, bool DB>
 constexpr size_t fl_smem_bytes() {
-    return size_t(kFlPairCap) * (MODE == kSpread ? 32 : 16) + size_t(kFlDCap) * 4 +
+    return size_t(kFlPairCap) * fl_pair_bytes<MODE>() + size_t(kFlDCap) * 4 +
            size_t(DB ? 64 : 32) * kFlStride * 4 + size_t(kFlSlots) * NAcc<MODE, P>::value * 32 * 8;
 }
 
@@ -554,21 +604,25 @@ template <int MODE, typename P, int U2, bool DB>
 __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
     k_gather_fl(const int4 *__restrict__ units, const int4 *__restrict__ segs,
                 const int32_t *__restrict__ unit_px, const float4 *__restrict__ pair_a,
-                const float4 *__restrict__ pair_b, const float4 *__restrict__ entry_std,
-                const int32_t *__restrict__ first_valid, const int32_t *__restrict__ seg_org,
+                const float4 *__restrict__ pair_b, const float2 *__restrict__ pair_c,
+                const float4 *__restrict__ entry_std,
+                const int32_t *__restrict__ first_valid, const int32_t *__restrict__ origin_entry,
+                const int32_t *__restrict__ seg_org,
                 const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_segments,
                 double *__restrict__ partial) {
     using S = StagedPx<P>;
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_off[kFlSegs + 1], s_first[kFlSegs], s_rend[kFlSegs], s_oidx[kFlSegs];
+    __shared__ int s_off[kFlSegs + 1], s_first[kFlSegs], s_rend[kFlSegs], s_oidx[kFlSegs],
+        s_oent[kFlSegs];
     __shared__ float s_on[kFlSegs];
     __shared__ int s_sa[kWarps], s_sb[kWarps];
     __shared__ int s_nb, s_bseg[kFlSlots], s_bwlo[kFlSlots], s_bwhi[kFlSlots];
     float4 *s_pa = reinterpret_cast<float4 *>(smem);
     float4 *s_pb = s_pa + kFlPairCap;
-    int32_t *s_px = reinterpret_cast<int32_t *>(smem + size_t(kFlPairCap) * (SPREAD ? 32 : 16));
+    float2 *s_pc = reinterpret_cast<float2 *>(s_pb + kFlPairCap);
+    int32_t *s_px = reinterpret_cast<int32_t *>(smem + size_t(kFlPairCap) * fl_pair_bytes<MODE>());
     S *s_buf = reinterpret_cast<S *>(s_px + kFlDCap);
     double *s_red = reinterpret_cast<double *>(s_buf + (DB ? 64 : 32) * kFlStride);
 
@@ -581,12 +635,13 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
         if (lane < nseg) {
             const int4 sg = segs[seg0 + lane];
             plen = (sg.z - sg.y + 1) & ~1;
-            const int first = first_valid[sg.x];
+            const int first = first_valid[sg.x], oe = origin_entry[sg.x];
             s_first[lane] = first;
             s_rend[lane] = sg.w;
+            s_oent[lane] = oe;
             if (SPREAD) {
                 s_oidx[lane] = seg_org[seg0 + lane];
-                s_on[lane] = first >= 0 ? entry_std[first].z : 1.f;
+                s_on[lane] = oe >= 0 ? entry_std[oe].z : 1.f;
             }
         }
         int inc = plen;
@@ -602,7 +657,10 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
     const int np = s_off[nseg] >> 1;
     for (int j = tid; j < np; j += kThreads) {
         s_pa[j] = pair_a[poff + j];
-        if (SPREAD) s_pb[j] = pair_b[poff + j];
+        if (SPREAD) {
+            s_pb[j] = pair_b[poff + j];
+            s_pc[j] = pair_c[poff + j];
+        }
     }
     for (int j = tid; j < D; j += kThreads) s_px[j] = unit_px[int64_t(blockIdx.x) * kFlDCap + j];
     // Column kFlDCap of every frame row is read by padding entries and must
@@ -686,16 +744,16 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
 
         for (int i = sa; i <= sb; ++i) {
             const int p0 = max(lo, s_off[i]) >> 1, p1 = min(hi, s_off[i + 1]) >> 1;
-            // Origin o = s/n of the row's first valid entry (row_origin): its
-            // pixel is staged with the unit's; a non-finite float pixel there
-            // sends the lane to the row's next entries in global memory.
+            // Origin o = s/n of the row's origin entry (row_origin): its pixel
+            // is staged with the unit's; a non-finite float pixel there sends
+            // the lane to the row's entries in global memory.
             float org = 0.f;
             if constexpr (SPREAD) {
                 const float so = float(px[s_oidx[i]]);
                 org = __fdiv_rn(so, s_on[i]);
                 if (is_float_px<P>() && !isfinite(so)) {
                     const int fi = min(f0 + lane, n_frames - 1);
-                    org = row_origin<P>(entry_std, s_first[i], s_rend[i],
+                    org = row_origin<P>(entry_std, s_oent[i], s_first[i], s_rend[i],
                                         frames + int64_t(fi) * n_pixels);
                 }
             }
@@ -708,10 +766,14 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
             auto body = [&](int p, auto unroll) {
                 constexpr int UU = decltype(unroll)::value;
                 float4 ea[UU], eb[UU];
+                f2 ec[UU];
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
                     ea[u] = s_pa[p + u];
-                    if constexpr (SPREAD) eb[u] = s_pb[p + u];
+                    if constexpr (SPREAD) {
+                        eb[u] = s_pb[p + u];
+                        ec[u] = reinterpret_cast<const f2 *>(s_pc)[p + u];
+                    }
                 }
                 float v0[UU], v1[UU];
 #pragma unroll
@@ -733,8 +795,9 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
                         const f2 cre = pk(ok0 ? eb[u].z : 0.f, ok1 ? eb[u].w : 0.f);
                         acc[0].p = fma2(ce, x, acc[0].p);
                         acc[1].p = fma2(mul2(ce, ce), pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f)), acc[1].p);
-                        const f2 t = fma2(norg, n, x);
+                        const f2 t = fma2(norg, ec[u], fma2(norg, n, x));
                         acc[2].p = fma2(mul2(cre, t), t, acc[2].p);
+                        acc[kSpreadA].p = fma2(ce, t, acc[kSpreadA].p);
                         acc[NA - 2].p = add2(acc[NA - 2].p,
                                              pk(ok0 ? 0.f : __fmul_rn(ea[u].z, eb[u].x),
                                                 ok1 ? 0.f : __fmul_rn(ea[u].w, eb[u].y)));
@@ -753,8 +816,9 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
                     }
                     if constexpr (SPREAD) {
                         const f2 n = pk(eb[u].x, eb[u].y), cr = pk(eb[u].z, eb[u].w);
-                        const f2 t = fma2(norg, n, x);
+                        const f2 t = fma2(norg, ec[u], fma2(norg, n, x));
                         acc[2].p = fma2(mul2(cr, t), t, acc[2].p);
+                        acc[kSpreadA].p = fma2(c, t, acc[kSpreadA].p);
                     }
                 }
             };
@@ -812,14 +876,16 @@ __global__ void __launch_bounds__(kThreads, (fl_ctas_per_sm<MODE, P, DB>()))
 // for a row without valid entries), counts the distinct ones into out_d
 // and, with fill (and D <= kFlDCap), writes the distinct list and the
 // unit's entry pairs: A {index 0, index 1, c0, c1} with the table's FP32
-// weights, B {n0, n1, c0/n0, c1/n1} and, when pair_as is given, A with the
-// spread's weights (0 for entries the spread excludes).
+// weights, B {n0, n1, c0/n0, c1/n1}, C {n_lo 0, n_lo 1} and, when pair_as is
+// given, A with the spread's weights (0 for entries the spread excludes).
+// Each segment's origin pixel is its row's origin entry's.
 __global__ void __launch_bounds__(256)
     k_fl_units(const int4 *__restrict__ units, const int4 *__restrict__ segs,
-               const int32_t *__restrict__ col, const int32_t *__restrict__ first_valid,
+               const int32_t *__restrict__ col, const int32_t *__restrict__ origin_entry,
                int fill, int32_t *__restrict__ out_d, int32_t *__restrict__ unit_px,
                const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
-               float4 *__restrict__ pair_a, float4 *__restrict__ pair_b,
+               const float *__restrict__ entry_nlo, float4 *__restrict__ pair_a,
+               float4 *__restrict__ pair_b, float2 *__restrict__ pair_c,
                float4 *__restrict__ pair_as, int32_t *__restrict__ seg_org) {
     constexpr int N = kFlSortMax, T = 256, PER = N / T;
     __shared__ int s_key[N];
@@ -849,7 +915,7 @@ __global__ void __launch_bounds__(256)
         for (int j = tid; j < sg.z - sg.y; j += T) s_key[s_off[i] + j] = col[sg.y + j];
     }
     if (tid < un.y) {
-        const int fv = first_valid[segs[un.x + tid].x];
+        const int fv = origin_entry[segs[un.x + tid].x];
         s_key[E + tid] = fv >= 0 ? col[fv] : INT_MAX;
     }
     for (int j = E + un.y + tid; j < N; j += T) s_key[j] = INT_MAX;
@@ -910,7 +976,7 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
     if (tid < un.y) {
-        const int fv = first_valid[segs[un.x + tid].x];
+        const int fv = origin_entry[segs[un.x + tid].x];
         int a = kFlDCap;
         if (fv >= 0) {
             const int cc = col[fv];
@@ -926,6 +992,7 @@ __global__ void __launch_bounds__(256)
     }
     float *pa = reinterpret_cast<float *>(pair_a + un.z);
     float *pb = reinterpret_cast<float *>(pair_b + un.z);
+    float *pc = reinterpret_cast<float *>(pair_c + un.z);
     float *ps = pair_as ? reinterpret_cast<float *>(pair_as + un.z) : nullptr;
     for (int i = 0; i < un.y; ++i) {
         const int4 sg = segs[un.x + i];
@@ -933,7 +1000,7 @@ __global__ void __launch_bounds__(256)
         for (int j = tid; j < padded; j += T) {
             const int p = s_poff[i] + j, rec = (p >> 1) * 4, h = p & 1;
             int idx = kFlDCap;
-            float c = 0.f, cs = 0.f, n = 1.f, cr = 0.f;
+            float c = 0.f, cs = 0.f, n = 1.f, cr = 0.f, nlo = 0.f;
             if (j < len) {
                 const int k = sg.y + j, cc = col[k];
                 int a = 0, b = D;
@@ -948,11 +1015,13 @@ __global__ void __launch_bounds__(256)
                 cs = es.y;
                 n = es.z;
                 cr = es.w;
+                nlo = entry_nlo[k];
             }
             pa[rec + h] = __int_as_float(idx);
             pa[rec + 2 + h] = c;
             pb[rec + h] = n;
             pb[rec + 2 + h] = cr;
+            pc[(p >> 1) * 2 + h] = nlo;
             if (ps) {
                 ps[rec + h] = __int_as_float(idx);
                 ps[rec + 2 + h] = cs;
@@ -1035,10 +1104,14 @@ struct BtCfg {
     // Per-frame masks (mode kRaw): a byte per slot, frame rows an odd number
     // of words apart (32 lanes reading one slot of their frames hit 32 banks).
     static constexpr int kMStride = 4 * (((DCAP + 4) / 4) | 1);
+    // Entry pairs: A, then B (spread, masks), then C (spread).
+    template <int MODE>
+    static constexpr size_t pair_bytes() {
+        return MODE == kSpread ? 40 : MODE == kRaw ? 32 : 16;
+    }
     template <int MODE>
     static constexpr size_t buf_bytes() {
-        return size_t(kFrames) * kStride * 4 +
-               size_t(PCAP) * (MODE == kSpread || MODE == kRaw ? 32 : 16) +
+        return size_t(kFrames) * kStride * 4 + size_t(PCAP) * pair_bytes<MODE>() +
                (MODE == kRaw ? size_t(kFrames) * kMStride : 0);
     }
     // Buffers, records, then the mbarriers: full[BUFS], empty[BUFS], record[kMetaBufs].
@@ -1093,6 +1166,10 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
 
 // Shared-memory mbarriers of the bin-tile chunk pipeline.
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
@@ -1138,9 +1215,10 @@ template <int MODE, typename P, class CFG>
 __global__ void __launch_bounds__(CFG::kThreads, 1)
     k_gather_bins(const int4 *__restrict__ items, const int32_t *__restrict__ meta,
                   const float4 *__restrict__ pair_a, const float4 *__restrict__ pair_b,
+                  const float2 *__restrict__ pair_c,
                   const int4 *__restrict__ org, const float4 *__restrict__ entry_std,
                   const double *__restrict__ den, const double *__restrict__ den_std,
-                  const double *__restrict__ den_f32, const int32_t *__restrict__ valid_std,
+                  const int32_t *__restrict__ valid_std,
                   const P *__restrict__ frames, int64_t n_pixels, int n_frames, int n_rows,
                   double *__restrict__ out_i, double *__restrict__ out_s,
                   double *__restrict__ out_d, int *__restrict__ wait_err, int withhold,
@@ -1185,6 +1263,10 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     };
     auto mkbuf = [&](int b) {  // mask rows (mode kRaw)
         return smem + size_t(b) * BUF + size_t(CFG::kFrames) * STRIDE * 4 + size_t(PCAP) * 32;
+    };
+    auto pcbuf = [&](int b) {  // pairs C (spread)
+        return reinterpret_cast<f2 *>(smem + size_t(b) * BUF + size_t(CFG::kFrames) * STRIDE * 4 +
+                                      size_t(PCAP) * 32);
     };
     // full[b]: chunk in buffer b landed (every thread's copies and stores);
     // empty[b]: every warp has summed the chunk in buffer b; rec[m]: the
@@ -1274,9 +1356,11 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             }
         }
         float4 *pa = pabuf(b);
+        f2 *pc = pcbuf(b);
         for (int j = tid; j < ch.w; j += NT) {
             cp_async16(pa + j, pair_a + ch.z + j);
             if (WIDE) cp_async16(pa + PCAP + j, pair_b + ch.z + j);
+            if (SPREAD) cp_async8(pc + j, pair_c + ch.z + j);
         }
     };
     // The second half: mask stores, then this thread's arrival on the
@@ -1329,11 +1413,26 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
 #pragma unroll
         for (int a = 0; a < NA; ++a) acc[h][a].zero();
     int since = 0;
+    const int r = warp;  // row of the tile
+    // Origin of the spread's shift, per frame of the lane: the row's origin
+    // entry {origin, first valid, row end} read from the frames before the
+    // first chunk (row_origin).
     float orgv[F2];
 #pragma unroll
     for (int h = 0; h < F2; ++h) orgv[h] = 0.f;
-    const int r = warp;  // row of the tile
-    const int4 o = r < nrows ? org[row0 + r] : make_int4(-1, 0, -1, 0);
+    if constexpr (SPREAD) {
+        if (r < nrows) {
+            const int4 o = org[row0 + r];
+#pragma unroll
+            for (int h = 0; h < F2; ++h) {
+                const int fi = min(f0 + lane + 32 * h, n_frames - 1);
+                orgv[h] = row_origin<P>(entry_std, o.x, o.y, o.z, frames + int64_t(fi) * n_pixels);
+            }
+        }
+    }
+    f2 norg[F2];
+#pragma unroll
+    for (int h = 0; h < F2; ++h) norg[h] = pk(-orgv[h], -orgv[h]);
 
     // Pipeline without a CTA-wide barrier: in step c a warp stages its share
     // of chunk c + AH (once every warp has summed the chunk that buffer held)
@@ -1378,37 +1477,21 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + (lane + 32 * h) * STRIDE;
         const float4 *s_pa = pabuf(b);
         const float4 *s_pb = s_pa + PCAP;
+        const f2 *s_pc = pcbuf(b);
         const unsigned char *mk[F2];  // this lane's mask rows (mode kRaw)
 #pragma unroll
         for (int h = 0; h < F2; ++h) mk[h] = mkbuf(b) + (lane + 32 * h) * MS;
         const int32_t *cp = mbuf(c) + 4;
-        if constexpr (SPREAD) {
-            if (o.x == c) {
-                // Origin o = s/n of the row's first valid entry (row_origin):
-                // its pixel is in this chunk; a non-finite float pixel there
-                // sends the lane to the row's next entries in global memory.
-#pragma unroll
-                for (int h = 0; h < F2; ++h) {
-                    const float so = float(px[h][o.y]);
-                    orgv[h] = __fdiv_rn(so, entry_std[o.z].z);
-                    if (is_float_px<P>() && !isfinite(so)) {
-                        const int fi = min(f0 + lane + 32 * h, n_frames - 1);
-                        orgv[h] = row_origin<P>(entry_std, o.z, o.w, frames + int64_t(fi) * n_pixels);
-                    }
-                }
-            }
-        }
-        f2 norg[F2];
-#pragma unroll
-        for (int h = 0; h < F2; ++h) norg[h] = pk(-orgv[h], -orgv[h]);
         const int p0 = cp[r], p1 = cp[r + 1];
         auto body = [&](int p, auto unroll) {
             constexpr int UU = decltype(unroll)::value;
             float4 ea[UU], eb[UU];
+            f2 ec[UU];
 #pragma unroll
             for (int u = 0; u < UU; ++u) {
                 ea[u] = s_pa[p + u];
                 if constexpr (WIDE) eb[u] = s_pb[p + u];
+                if constexpr (SPREAD) ec[u] = s_pc[p + u];
             }
 #pragma unroll
             for (int h = 0; h < F2; ++h) {
@@ -1450,8 +1533,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                             acc[h][0].p = fma2(ce, x, acc[h][0].p);
                             acc[h][1].p = fma2(mul2(ce, ce), pk(fmaxf(x0, 0.f), fmaxf(x1, 0.f)),
                                                acc[h][1].p);
-                            const f2 t = fma2(norg[h], n, x);
+                            const f2 t = fma2(norg[h], ec[u], fma2(norg[h], n, x));
                             acc[h][2].p = fma2(mul2(cre, t), t, acc[h][2].p);
+                            acc[h][kSpreadA].p = fma2(ce, t, acc[h][kSpreadA].p);
                             acc[h][NA - 2].p = add2(acc[h][NA - 2].p,
                                                     pk(ok0 ? 0.f : __fmul_rn(ea[u].z, eb[u].x),
                                                        ok1 ? 0.f : __fmul_rn(ea[u].w, eb[u].y)));
@@ -1471,8 +1555,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                     }
                     if constexpr (SPREAD) {
                         const f2 n = pk(eb[u].x, eb[u].y), cr = pk(eb[u].z, eb[u].w);
-                        const f2 t = fma2(norg[h], n, x);
+                        const f2 t = fma2(norg[h], ec[u], fma2(norg[h], n, x));
                         acc[h][2].p = fma2(mul2(cr, t), t, acc[h][2].p);
+                        acc[h][kSpreadA].p = fma2(cc, t, acc[h][kSpreadA].p);
                     }
                 }
             }
@@ -1566,11 +1651,10 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             }
         } else {
             int valid = valid_std[row];
-            double sw = den_std[row], wf = den_f32[row];
-            if (NA == 5) {
+            double sw = den_std[row];
+            if (NA == 6) {
                 valid -= int(v[NA - 1] + 0.5);
                 sw -= v[NA - 2];
-                wf -= v[NA - 2];
             }
             if (valid <= 0 || !(sw > 0.0)) {
                 out_i[oo] = 0.0;
@@ -1578,7 +1662,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 out_d[oo] = __longlong_as_double(0x7ff8000000000000ll);
                 continue;
             }
-            const double a1 = v[0] - double(orgv[h]) * wf;
+            const double a1 = v[kSpreadA];
             out_i[oo] = v[0] / sw;
             if (out_s) out_s[oo] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
             const double mean = a1 / sw;
@@ -1595,12 +1679,14 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
 // weights, B {n0, n1, c0/n0, c1/n1}.
 __global__ void k_bt_fill(const int4 *__restrict__ desc, int64_t n_pairs,
                           const int2 *__restrict__ entry, const float4 *__restrict__ entry_std,
-                          float4 *__restrict__ pair_a, float4 *__restrict__ pair_as,
-                          float4 *__restrict__ pair_b) {
+                          const float *__restrict__ entry_nlo, float4 *__restrict__ pair_a,
+                          float4 *__restrict__ pair_as, float4 *__restrict__ pair_b,
+                          float2 *__restrict__ pair_c) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pairs;
          i += int64_t(gridDim.x) * blockDim.x) {
         const int4 d = desc[i];
-        float c[2] = {0.f, 0.f}, cs[2] = {0.f, 0.f}, n[2] = {1.f, 1.f}, cr[2] = {0.f, 0.f};
+        float c[2] = {0.f, 0.f}, cs[2] = {0.f, 0.f}, n[2] = {1.f, 1.f}, cr[2] = {0.f, 0.f},
+              nlo[2] = {0.f, 0.f};
         const int k[2] = {d.z, d.w};
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -1610,10 +1696,12 @@ __global__ void k_bt_fill(const int4 *__restrict__ desc, int64_t n_pairs,
             cs[h] = es.y;
             n[h] = es.z;
             cr[h] = es.w;
+            nlo[h] = entry_nlo[k[h]];
         }
         pair_a[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), c[0], c[1]);
         pair_as[i] = make_float4(__int_as_float(d.x), __int_as_float(d.y), cs[0], cs[1]);
         pair_b[i] = make_float4(n[0], n[1], cr[0], cr[1]);
+        pair_c[i] = make_float2(nlo[0], nlo[1]);
     }
 }
 
@@ -1644,23 +1732,21 @@ __global__ void k_bt_fill_raw(const int4 *__restrict__ desc, int64_t n_pairs,
 // order in FP64 and normalise (normalize_bin, prepared.rs:985-996; the
 // spread's closing formulas, azimuthal.rs:96-104).
 constexpr int kFinRows = 8;  // rows per k_finalize CTA (x 32 frames)
+// One tile of kFinRows rows from r0 and 32 frames from fb, by a CTA of 256
+// threads: lanes run over frames while the partial sums are read
+// (frame-contiguous), the results go through shared memory and are written
+// row-contiguous for each frame. Ends with a CTA barrier, so the next tile
+// may reuse the shared memory at once.
 template <int MODE, typename P>
-__global__ void __launch_bounds__(256)
-    k_finalize(const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
-               const int32_t *__restrict__ seg_ids, const int4 *__restrict__ segs,
-               const double *__restrict__ den, const double *__restrict__ den_std,
-               const double *__restrict__ den_f32, const int32_t *__restrict__ valid_std,
-               const int32_t *__restrict__ first_valid, const float4 *__restrict__ entry_std,
-               const P *__restrict__ frames, int64_t n_pixels, int n_rows, int n_segments,
-               int n_frames, double *__restrict__ out_i, double *__restrict__ out_s,
-               double *__restrict__ out_d) {
-    // A CTA takes kFinRows rows x 32 frames: lanes run over frames while the
-    // partial sums are read (frame-contiguous), the results go through
-    // shared memory and are written row-contiguous for each frame.
+__device__ __forceinline__ void finalize_tile(
+    int r0, int fb, const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
+    const int32_t *__restrict__ seg_ids, const double *__restrict__ den,
+    const double *__restrict__ den_std, const int32_t *__restrict__ valid_std, int n_rows,
+    int n_frames, double *__restrict__ out_i, double *__restrict__ out_s,
+    double *__restrict__ out_d) {
     constexpr int NA = NAcc<MODE, P>::value;
     __shared__ double s_o[3][kFinRows][33];
     const int fl = threadIdx.x & 31, rl = threadIdx.x >> 5;
-    const int r0 = blockIdx.x * kFinRows, fb = blockIdx.y * 32;
     const int r = r0 + rl, f = fb + fl;
     double ri = 0.0, rs = 0.0, rd = 0.0;
     if (r < n_rows && f < n_frames) {
@@ -1685,20 +1771,15 @@ __global__ void __launch_bounds__(256)
             }
         } else {
             int valid = valid_std[r];
-            double sw = den_std[r], wf = den_f32[r];
-            if (NA == 5) {
+            double sw = den_std[r];
+            if (NA == 6) {
                 valid -= int(v[NA - 1] + 0.5);
                 sw -= v[NA - 2];
-                wf -= v[NA - 2];
             }
             if (valid <= 0 || !(sw > 0.0)) {
                 rd = __longlong_as_double(0x7ff8000000000000ll);
             } else {
-                // A = sum c*(s - o*n) = S - o * sum c*n over the same FP32 weights.
-                const int row_end = k0 < k1 ? segs[seg_ids[k0]].w : 0;
-                const float org = row_origin<P>(entry_std, first_valid[r], row_end,
-                                                frames + int64_t(f) * n_pixels);
-                const double a1 = v[0] - double(org) * wf;
+                const double a1 = v[kSpreadA];
                 ri = v[0] / sw;
                 rs = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
                 const double mean = a1 / sw;
@@ -1714,11 +1795,24 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     const int wr = threadIdx.x % kFinRows, wf = threadIdx.x / kFinRows;
     const int rr = r0 + wr, ff = fb + wf;
-    if (rr >= n_rows || ff >= n_frames) return;
-    const int64_t o = int64_t(ff) * n_rows + rr;
-    out_i[o] = s_o[0][wr][wf];
-    if (MODE != kIntensity && out_s) out_s[o] = s_o[1][wr][wf];
-    if (MODE == kSpread) out_d[o] = s_o[2][wr][wf];
+    if (rr < n_rows && ff < n_frames) {
+        const int64_t o = int64_t(ff) * n_rows + rr;
+        out_i[o] = s_o[0][wr][wf];
+        if (MODE != kIntensity && out_s) out_s[o] = s_o[1][wr][wf];
+        if (MODE == kSpread) out_d[o] = s_o[2][wr][wf];
+    }
+    __syncthreads();
+}
+
+template <int MODE, typename P>
+__global__ void __launch_bounds__(256)
+    k_finalize(const double *__restrict__ partial, const int32_t *__restrict__ row_seg,
+               const int32_t *__restrict__ seg_ids, const double *__restrict__ den,
+               const double *__restrict__ den_std, const int32_t *__restrict__ valid_std,
+               int n_rows, int n_frames, double *__restrict__ out_i, double *__restrict__ out_s,
+               double *__restrict__ out_d) {
+    finalize_tile<MODE, P>(blockIdx.x * kFinRows, blockIdx.y * 32, partial, row_seg, seg_ids, den,
+                           den_std, valid_std, n_rows, n_frames, out_i, out_s, out_d);
 }
 
 // Raw sums per (frame, row) (IntermediateResult1d, lut/integrate.rs:372-379):
@@ -1787,17 +1881,20 @@ __global__ void k_pack_raw(const int64_t *__restrict__ row_ptr, int n_rows,
 }
 
 // Packs the masked f64 table into the gather's entry formats and computes
-// the spread's denominators over its valid entries (c > 0, n > 0, finite).
+// the spread's denominators over its valid entries (c > 0, n > 0, finite),
+// its first valid entry and its origin entry (the heaviest valid, row_origin).
+// The spread's n is stored as the pair (n_hi, n_lo): n_hi = FP32(n) in
+// entry_std, n_lo = FP32(n - n_hi) in entry_nlo.
 __global__ void k_pack(const int64_t *__restrict__ row_ptr, int n_rows,
                        const int32_t *__restrict__ col, const double *__restrict__ w,
                        const double *__restrict__ norm, int2 *__restrict__ entry,
-                       float4 *__restrict__ entry_std, double *__restrict__ den_std,
-                       double *__restrict__ den_f32, int32_t *__restrict__ valid_std,
-                       int32_t *__restrict__ first_valid) {
+                       float4 *__restrict__ entry_std, float *__restrict__ entry_nlo,
+                       double *__restrict__ den_std, int32_t *__restrict__ valid_std,
+                       int32_t *__restrict__ first_valid, int32_t *__restrict__ origin) {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
-    double sw = 0.0, swf = 0.0;
-    int valid = 0, first = -1;
+    double sw = 0.0, heaviest = 0.0;
+    int valid = 0, first = -1, org = -1;
     for (int64_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
         int32_t j = col[k];
         double c = w[k], n = norm[j];
@@ -1808,17 +1905,21 @@ __global__ void k_pack(const int64_t *__restrict__ row_ptr, int n_rows,
         float nf = __double2float_rn(n);
         entry_std[k] = make_float4(__int_as_float(j), ok ? cf : 0.f, ok ? nf : 1.f,
                                    ok ? __double2float_rn(c / n) : 0.f);
+        entry_nlo[k] = ok ? __double2float_rn(n - double(nf)) : 0.f;
         if (ok) {
             sw += ww;
-            swf += double(cf) * double(nf);
             ++valid;
             if (first < 0) first = int(k);
+            if (ww > heaviest) {  // the first of equally heavy entries
+                heaviest = ww;
+                org = int(k);
+            }
         }
     }
     den_std[r] = sw;
-    den_f32[r] = swf;
     valid_std[r] = valid;
     first_valid[r] = first;
+    origin[r] = org;
 }
 
 // bounds[r * (n_strips + 1) + s]: first entry of row r whose pixel lies in
@@ -1851,9 +1952,9 @@ void launch_fl(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, doub
     DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const float4 *pa = MODE == kSpread ? t.fl_pair_as : t.fl_pair_a.ptr;
     kern<<<t.fl_n_units, kThreads, smem, s>>>(t.fl_unit.ptr, t.seg.ptr, t.fl_px.ptr, pa,
-                                              t.fl_pair_b.ptr, t.entry_std.ptr, t.first_valid.ptr,
-                                              t.fl_seg_org.ptr, fp, n_pixels, nf, t.n_segments,
-                                              partial);
+                                              t.fl_pair_b.ptr, t.fl_pair_c.ptr, t.entry_std.ptr,
+                                              t.first_valid.ptr, t.origin.ptr, t.fl_seg_org.ptr,
+                                              fp, n_pixels, nf, t.n_segments, partial);
 }
 
 // Launches lane-mapping variant `variant` of the gather (kVariantCount) with
@@ -1872,8 +1973,8 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
     const float4 *pa = MODE == kSpread ? bt.pair_as.ptr : MODE == kRaw ? bt.pair_ra.ptr : bt.pair_a.ptr;
     const float4 *pb = MODE == kRaw ? bt.pair_rb.ptr : bt.pair_b.ptr;
     kern<<<unsigned(grid), CFG::kThreads, smem, s>>>(
-        bt.item.ptr, bt.meta.ptr, pa, pb, bt.org.ptr, t.entry_std.ptr, t.den.ptr, t.den_std.ptr, t.den_f32.ptr,
-        t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od, bt.wait_err.dev,
+        bt.item.ptr, bt.meta.ptr, pa, pb, bt.pair_c.ptr, bt.org.ptr, t.entry_std.ptr, t.den.ptr,
+        t.den_std.ptr, t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od, bt.wait_err.dev,
         t.withhold_test, t.cnt.ptr, oc, raw, masks, mask_stride);
 }
 
@@ -1908,9 +2009,9 @@ bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pix
     }
     const size_t smem = size_t(t.unit_cap) * (MODE == kSpread || MODE == kRaw ? 16 : 8);
     const float4 *wide = MODE == kRaw ? t.entry_raw.ptr : t.entry_std.ptr;
-#define DG_GATHER_ARGS                                                                     \
-    t.unit.ptr, t.seg.ptr, t.entry.ptr, wide, t.first_valid.ptr, fp, n_pixels, nf, t.n_segments, \
-        partial, masks, mask_stride
+#define DG_GATHER_ARGS                                                                        \
+    t.unit.ptr, t.seg.ptr, t.entry.ptr, wide, t.entry_nlo.ptr, t.first_valid.ptr, t.origin.ptr, fp, \
+        n_pixels, nf, t.n_segments, partial, masks, mask_stride
     switch (variant) {
     case 0: k_gather<MODE, P, 32, 4, 4><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
     case 1: k_gather<MODE, P, 32, 2, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
@@ -1939,22 +2040,21 @@ bool launch_typed(const GatherTable &t, int variant, const void *frames, int64_t
 }
 
 template <int MODE, typename P>
-void launch_finalize(GatherTable &t, const void *frames, int64_t n_pixels, int nf, double *oi,
-                     double *os, double *od, cudaStream_t s) {
+void launch_finalize(const GatherTable &t, const double *partial, int nf, double *oi, double *os,
+                     double *od, cudaStream_t s) {
     const dim3 grid(unsigned((t.n_rows + kFinRows - 1) / kFinRows), unsigned((nf + 31) / 32));
-    k_finalize<MODE, P><<<grid, 32 * kFinRows, 0, s>>>(
-        t.partial.ptr, t.row_seg.ptr, t.seg_ids.ptr, t.seg.ptr, t.den.ptr, t.den_std.ptr,
-        t.den_f32.ptr, t.valid_std.ptr, t.first_valid.ptr, t.entry_std.ptr,
-        static_cast<const P *>(frames), n_pixels, t.n_rows, t.n_segments, nf, oi, os, od);
+    k_finalize<MODE, P><<<grid, 32 * kFinRows, 0, s>>>(partial, t.row_seg.ptr, t.seg_ids.ptr,
+                                                        t.den.ptr, t.den_std.ptr, t.valid_std.ptr,
+                                                        t.n_rows, nf, oi, os, od);
     DG_CUDA(cudaGetLastError());
 }
 
 template <typename P>
-void finalize_typed(GatherTable &t, int mode, const void *frames, int64_t n_pixels, int nf,
-                    double *oi, double *os, double *od, cudaStream_t s) {
-    if (mode == kSpread) launch_finalize<kSpread, P>(t, frames, n_pixels, nf, oi, os, od, s);
-    else if (mode == kErrors) launch_finalize<kErrors, P>(t, frames, n_pixels, nf, oi, os, od, s);
-    else launch_finalize<kIntensity, P>(t, frames, n_pixels, nf, oi, os, od, s);
+void finalize_typed(const GatherTable &t, int mode, const double *partial, int nf, double *oi,
+                    double *os, double *od, cudaStream_t s) {
+    if (mode == kSpread) launch_finalize<kSpread, P>(t, partial, nf, oi, os, od, s);
+    else if (mode == kErrors) launch_finalize<kErrors, P>(t, partial, nf, oi, os, od, s);
+    else launch_finalize<kIntensity, P>(t, partial, nf, oi, os, od, s);
 }
 
 }  // namespace
@@ -2001,8 +2101,8 @@ void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<
         DG_CUDA(cudaMemcpyAsync(d_units.ptr, fl.data(), fl.size() * sizeof(int4),
                                 cudaMemcpyHostToDevice, s));
         k_fl_units<<<unsigned(fl.size()), 256, 0, s>>>(
-            d_units.ptr, out.seg.ptr, table.col.ptr, out.first_valid.ptr, 0, d_count.ptr, nullptr,
-            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+            d_units.ptr, out.seg.ptr, table.col.ptr, out.origin.ptr, 0, d_count.ptr, nullptr,
+            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
         DG_CUDA(cudaGetLastError());
         count.resize(fl.size());
         DG_CUDA(cudaMemcpyAsync(count.data(), d_count.ptr, count.size() * 4,
@@ -2052,15 +2152,17 @@ void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<
     out.fl_px.alloc(fl.size() * size_t(kFlDCap));
     out.fl_pair_a.alloc(size_t(std::max<int64_t>(pairs, 1)));
     out.fl_pair_b.alloc(size_t(std::max<int64_t>(pairs, 1)));
+    out.fl_pair_c.alloc(size_t(std::max<int64_t>(pairs, 1)));
     if (own_spread) out.fl_pair_s.alloc(size_t(std::max<int64_t>(pairs, 1)));
     else out.fl_pair_s.release();
     DG_CUDA(cudaMemcpyAsync(out.fl_unit.ptr, fl.data(), fl.size() * sizeof(int4),
                             cudaMemcpyHostToDevice, s));
     out.fl_seg_org.alloc(segs.size());
     k_fl_units<<<unsigned(fl.size()), 256, 0, s>>>(
-        out.fl_unit.ptr, out.seg.ptr, table.col.ptr, out.first_valid.ptr, 1, d_count.ptr,
-        out.fl_px.ptr, out.entry.ptr, out.entry_std.ptr, out.fl_pair_a.ptr, out.fl_pair_b.ptr,
-        own_spread ? out.fl_pair_s.ptr : nullptr, out.fl_seg_org.ptr);
+        out.fl_unit.ptr, out.seg.ptr, table.col.ptr, out.origin.ptr, 1, d_count.ptr,
+        out.fl_px.ptr, out.entry.ptr, out.entry_std.ptr, out.entry_nlo.ptr, out.fl_pair_a.ptr,
+        out.fl_pair_b.ptr, out.fl_pair_c.ptr, own_spread ? out.fl_pair_s.ptr : nullptr,
+        out.fl_seg_org.ptr);
     DG_CUDA(cudaGetLastError());
     DG_CUDA(cudaStreamSynchronize(s));
     out.fl_pair_as = own_spread ? out.fl_pair_s.ptr : out.fl_pair_a.ptr;
@@ -2072,8 +2174,8 @@ void build_fl_units(GatherTable &out, const DeviceCsr &table, const std::vector<
 // at most kBtDCap distinct pixels and kBtPCap pairs (a new pixel that would
 // exceed either opens the next chunk, so a chunk is a pixel-index interval
 // and each row's entries in it are a contiguous run of its CSR row). Tiles
-// are ordered largest first. Each row's origin (its first entry valid for the
-// spread) is located as {chunk within the tile, slot}.
+// are ordered largest first. Each row keeps {origin entry, first valid entry,
+// row end} for the spread's origin (row_origin), read before the first chunk.
 template <class CFG>
 void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cudaStream_t s) {
     constexpr int kBtDCap = CFG::kDCap, kBtPCap = CFG::kPCap, kBtRows = CFG::kRows;
@@ -2084,9 +2186,11 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     out.wait_err.alloc();
     std::vector<int64_t> rp(static_cast<size_t>(nb) + 1);
     DG_CUDA(cudaMemcpyAsync(rp.data(), table.row_ptr.ptr, rp.size() * 8, cudaMemcpyDeviceToHost, s));
-    std::vector<int32_t> col(static_cast<size_t>(table.nnz)), fv(static_cast<size_t>(nb));
+    std::vector<int32_t> col(static_cast<size_t>(table.nnz)), fv(static_cast<size_t>(nb)),
+        oe(static_cast<size_t>(nb));
     DG_CUDA(cudaMemcpyAsync(col.data(), table.col.ptr, col.size() * 4, cudaMemcpyDeviceToHost, s));
     DG_CUDA(cudaMemcpyAsync(fv.data(), gt.first_valid.ptr, fv.size() * 4, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaMemcpyAsync(oe.data(), gt.origin.ptr, oe.size() * 4, cudaMemcpyDeviceToHost, s));
     DG_CUDA(cudaStreamSynchronize(s));
     const int64_t n_items = (nb + kBtRows - 1) / kBtRows;
     struct Tile {
@@ -2094,7 +2198,6 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         std::vector<int32_t> cpair;    // per chunk kBtRows + 1
         std::vector<int32_t> px;
         std::vector<int4> pairs;       // {slot0, slot1, entry0, entry1}
-        std::vector<int4> org;         // per row
         int64_t entries = 0;
     };
     std::vector<Tile> tiles(static_cast<size_t>(n_items));
@@ -2139,12 +2242,10 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         T.entries = n_e;
         T.pairs.reserve(size_t(n_e / 2 + 64));
         T.px.reserve(size_t(n_e / 2 + 64));
-        T.org.assign(size_t(nr), make_int4(-1, 0, -1, 0));
         std::vector<std::vector<std::pair<int32_t, int32_t>>> run(static_cast<size_t>(nr));  // (slot, entry)
         std::vector<int32_t> chunk_px;
         auto close = [&]() {
             if (chunk_px.empty()) return;
-            const int ci = int(T.chunks.size());
             int4 ch = make_int4(int(T.px.size()), int(chunk_px.size()), int(T.pairs.size()), 0);
             T.px.insert(T.px.end(), chunk_px.begin(), chunk_px.end());
             int po = 0;
@@ -2158,8 +2259,6 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
                                                 rv[e].second, two ? rv[e + 1].second : -1));
                     ++po;
                 }
-                for (const auto &se : rv)
-                    if (se.second == fv[size_t(r0 + j)]) T.org[size_t(j)] = make_int4(ci, se.first, se.second, 0);
             }
             T.cpair.push_back(po);
             ch.w = po;
@@ -2187,8 +2286,6 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
             i = e;
         }
         close();
-        for (int j = 0; j < nr; ++j)
-            if (T.org[size_t(j)].x >= 0) T.org[size_t(j)].w = int(rp[size_t(r0 + j) + 1]);
     };
     const int nt = int(std::min<int64_t>(
         n_items, std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
@@ -2224,6 +2321,9 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     // default-initialised (not zeroed): every element is written below
     const size_t n_chunks = size_t(o_ch[size_t(n_items)]), n_pairs = size_t(o_pr[size_t(n_items)]);
     std::vector<int4> items(static_cast<size_t>(n_items)), org(static_cast<size_t>(nb));
+    // per row {origin entry, first valid entry, row end, 0} (row_origin)
+    for (int64_t r = 0; r < nb; ++r)
+        org[size_t(r)] = make_int4(oe[size_t(r)], fv[size_t(r)], int(rp[size_t(r) + 1]), 0);
     std::unique_ptr<int32_t[]> meta(new int32_t[std::max<size_t>(n_chunks * kBtMetaWords, 1)]);
     std::unique_ptr<int4[]> pairs(new int4[std::max<size_t>(n_pairs, 1)]);
     auto flatten = [&](int64_t i) {
@@ -2245,7 +2345,6 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         std::copy(T.pairs.begin(), T.pairs.end(), pairs.get() + pr0);
         const int64_t r0 = ti * kBtRows;
         const int nr = int(std::min<int64_t>(nb, r0 + kBtRows) - r0);
-        for (int j = 0; j < nr; ++j) org[size_t(r0 + j)] = T.org[size_t(j)];
         items[size_t(i)] = make_int4(int(r0), nr, int(c0), int(T.chunks.size()));
         T = Tile();
     };
@@ -2257,6 +2356,7 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     out.pair_a.alloc(std::max<size_t>(n_pairs, 1));
     out.pair_as.alloc(std::max<size_t>(n_pairs, 1));
     out.pair_b.alloc(std::max<size_t>(n_pairs, 1));
+    out.pair_c.alloc(std::max<size_t>(n_pairs, 1));
     DeviceArray<int4> &desc = out.desc;  // kept for the per-frame-mask pairs
     desc.alloc(std::max<size_t>(n_pairs, 1));
     out.pair_ra.release();
@@ -2273,8 +2373,8 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         DG_CUDA(cudaMemcpyAsync(desc.ptr, pairs.get(), n_pairs * sizeof(int4),
                                 cudaMemcpyHostToDevice, s));
         k_bt_fill<<<148 * 8, 256, 0, s>>>(desc.ptr, int64_t(n_pairs), gt.entry.ptr,
-                                         gt.entry_std.ptr, out.pair_a.ptr, out.pair_as.ptr,
-                                         out.pair_b.ptr);
+                                         gt.entry_std.ptr, gt.entry_nlo.ptr, out.pair_a.ptr,
+                                         out.pair_as.ptr, out.pair_b.ptr, out.pair_c.ptr);
         DG_CUDA(cudaGetLastError());
     }
     DG_CUDA(cudaStreamSynchronize(s));
@@ -2348,15 +2448,17 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     out.entry_std.alloc(size_t(table.nnz));
     out.den.alloc(size_t(table.n_rows));
     out.den_std.alloc(size_t(table.n_rows));
-    out.den_f32.alloc(size_t(table.n_rows));
+    out.entry_nlo.alloc(size_t(table.nnz));
     out.valid_std.alloc(size_t(table.n_rows));
     out.first_valid.alloc(size_t(table.n_rows));
+    out.origin.alloc(size_t(table.n_rows));
     denominators(table, d_norm, s, out.den.ptr);
     const unsigned rb = unsigned((table.n_rows + 127) / 128);
     if (table.n_rows > 0)
         k_pack<<<rb, 128, 0, s>>>(table.row_ptr.ptr, int(table.n_rows), table.col.ptr, table.w.ptr,
-                                  d_norm, out.entry.ptr, out.entry_std.ptr, out.den_std.ptr,
-                                  out.den_f32.ptr, out.valid_std.ptr, out.first_valid.ptr);
+                                  d_norm, out.entry.ptr, out.entry_std.ptr, out.entry_nlo.ptr,
+                                  out.den_std.ptr, out.valid_std.ptr, out.first_valid.ptr,
+                                  out.origin.ptr);
     DG_CUDA(cudaGetLastError());
 
     // Segments: (row, strip) runs from per-row strip bounds found on the
@@ -2437,19 +2539,52 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     }, s);
 }
 
+bool gather_writes_results(const GatherTable &t) {
+    return (t.variant == 7 || t.variant == 8) && t.bt[t.variant - 7].n_items > 0;
+}
+
+void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtype,
+                      bool any_mapping) {
+    if ((!any_mapping && gather_writes_results(t)) || n_frames <= 0) return;
+    const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
+                                                                                : kIntensity;
+    const int64_t need = std::max<int64_t>(1, t.n_segments) *
+                         n_accumulators(mode, dtype == DG_F32 || dtype == DG_F64) *
+                         std::min<int64_t>(256, (n_frames + 31) / 32 * 32);
+    if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+}
+
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                 int64_t n_frames, uint32_t flags, int precision, double *d_i, double *d_sigma,
-                double *d_std, cudaStream_t s) {
+                double *d_std, cudaStream_t s, double *scratch, size_t scratch_doubles) {
     (void)precision;
     if (n_frames <= 0) return;
     if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
     const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
                                                                                 : kIntensity;
-    // Frames per launch bounded by the partial-sum scratch (256 frames).
-    const int64_t chunk = 256;
-    const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 5;
-    if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
-    t.scratch.wait(s);
+    // Frames per launch: 256, or fewer where the caller's fixed scratch holds
+    // the partial sums of fewer frames (the bin tiles write no partial sums).
+    int64_t chunk = 256;
+    double *partial = nullptr;
+    if (scratch) {
+        const bool fpx = dtype == DG_F32 || dtype == DG_F64;
+        const int64_t per_frame =
+            gather_writes_results(t) || t.n_units == 0
+                ? 0
+                : std::max<int64_t>(1, t.n_segments) * n_accumulators(mode, fpx);
+        if (per_frame > 0) chunk = std::min<int64_t>(chunk, int64_t(scratch_doubles) / per_frame);
+        if (chunk < 1)
+            fail(DG_UNSUPPORTED, "this plan needs " + std::to_string(per_frame * 8) +
+                                     " bytes of partial sums per frame; the fixed scratch holds " +
+                                     std::to_string(scratch_doubles * 8) + " bytes");
+        partial = scratch;
+    } else {
+        // [segment][accumulator][frame] for the largest launch of this call,
+        // frames rounded up to 32 so that growing batches reallocate rarely
+        reserve_partials(t, std::min<int64_t>(chunk, n_frames), flags, dtype, true);
+        t.scratch.wait(s);
+        partial = t.partial.ptr;
+    }
     const size_t esize = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
     for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
         const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
@@ -2472,28 +2607,27 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
                 DG_CUDA(cudaEventRecord(ev->first, s));
             }
             ++t.launches;
-            double *pp = t.partial.ptr;
             switch (dtype) {
-            case DG_U16: done = launch_typed<uint16_t>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
-            case DG_U32: done = launch_typed<uint32_t>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
-            case DG_I32: done = launch_typed<int32_t>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
-            case DG_F32: done = launch_typed<float>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
-            case DG_F64: done = launch_typed<double>(t, t.variant, fp, n_pixels, nf, mode, pp, oi, os, od, s); break;
+            case DG_U16: done = launch_typed<uint16_t>(t, t.variant, fp, n_pixels, nf, mode, partial, oi, os, od, s); break;
+            case DG_U32: done = launch_typed<uint32_t>(t, t.variant, fp, n_pixels, nf, mode, partial, oi, os, od, s); break;
+            case DG_I32: done = launch_typed<int32_t>(t, t.variant, fp, n_pixels, nf, mode, partial, oi, os, od, s); break;
+            case DG_F32: done = launch_typed<float>(t, t.variant, fp, n_pixels, nf, mode, partial, oi, os, od, s); break;
+            case DG_F64: done = launch_typed<double>(t, t.variant, fp, n_pixels, nf, mode, partial, oi, os, od, s); break;
             }
             if (ev) DG_CUDA(cudaEventRecord(ev->second, s));
         }
         if (t.n_rows > 0 && !done) {
             ++t.launches;
             switch (dtype) {
-            case DG_U16: finalize_typed<uint16_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
-            case DG_U32: finalize_typed<uint32_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
-            case DG_I32: finalize_typed<int32_t>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
-            case DG_F32: finalize_typed<float>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
-            case DG_F64: finalize_typed<double>(t, mode, fp, n_pixels, nf, oi, os, od, s); break;
+            case DG_U16: finalize_typed<uint16_t>(t, mode, partial, nf, oi, os, od, s); break;
+            case DG_U32: finalize_typed<uint32_t>(t, mode, partial, nf, oi, os, od, s); break;
+            case DG_I32: finalize_typed<int32_t>(t, mode, partial, nf, oi, os, od, s); break;
+            case DG_F32: finalize_typed<float>(t, mode, partial, nf, oi, os, od, s); break;
+            case DG_F64: finalize_typed<double>(t, mode, partial, nf, oi, os, od, s); break;
             }
         }
     }
-    t.scratch.mark(s);
+    if (!scratch) t.scratch.mark(s);
 }
 
 namespace {
@@ -2616,7 +2750,9 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     const bool errors = (flags & DG_ERRORS) != 0;
     const int mode = d_masks ? kRaw : errors ? kErrors : kIntensity;
     const int64_t chunk = 256;
-    const int64_t need = std::max<int64_t>(1, t.n_segments) * chunk * 5;
+    const int64_t need = std::max<int64_t>(1, t.n_segments) *
+                         n_accumulators(mode, dtype == DG_F32 || dtype == DG_F64) *
+                         std::min<int64_t>(chunk, (n_frames + 31) / 32 * 32);
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
     t.scratch.wait(s);
     const size_t esize = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
@@ -2672,13 +2808,7 @@ void run_gather_raw(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
         } else {
             if (mode != kRaw) fail(DG_INVALID_INPUT, "normalised results need per-frame masks");
             double *oi = at(o0), *os = errors ? at(o1) : nullptr;
-            switch (dtype) {
-            case DG_U16: launch_finalize<kRaw, uint16_t>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
-            case DG_U32: launch_finalize<kRaw, uint32_t>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
-            case DG_I32: launch_finalize<kRaw, int32_t>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
-            case DG_F32: launch_finalize<kRaw, float>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
-            case DG_F64: launch_finalize<kRaw, double>(t, fp, n_pixels, nf, oi, os, nullptr, s); break;
-            }
+            launch_finalize<kRaw, float>(t, t.partial.ptr, nf, oi, os, nullptr, s);
         }
     }
     t.scratch.mark(s);
@@ -2693,7 +2823,7 @@ void launch_mode(GatherTable &t, int variant, int mode, const void *frames, int6
                  int nf, double *oi, double *os, double *od, cudaStream_t s) {
     if (!launch_typed<P>(t, variant, frames, n_pixels, nf, mode, t.partial.ptr, oi, os, od, s) &&
         t.n_rows > 0)
-        finalize_typed<P>(t, mode, frames, n_pixels, nf, oi, os, od, s);
+        finalize_typed<P>(t, mode, t.partial.ptr, nf, oi, os, od, s);
 }
 
 }  // namespace
@@ -2715,8 +2845,7 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
     const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
                                                                                 : kIntensity;
     const int nf = int(std::min<int64_t>(n_frames, 256));
-    const int64_t need = std::max<int64_t>(1, t.n_segments) * 256 * 5;
-    if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+    reserve_partials(t, nf, flags, dtype, true);
     t.scratch.wait(s);
     if (each) each->assign(size_t(kVariantCount), 0.0);
     if (t.n_units == 0) return t.variant;
@@ -2774,152 +2903,38 @@ int autotune_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_p
 }  // namespace dg
 
 // ---------------------------------------------------------------------------
-// Allocation-free integration (dg_integrate_device_noalloc).
+// Fixed scratch of the allocation-free entry point (dg_integrate_device_noalloc
+// in dg_api.cu).
 //
-// For callers that must not allocate device memory while they integrate: a
+// Some callers may not allocate device memory while they integrate: a
 // real-time acquisition loop with a fixed memory budget, a host thread that
-// may not enter the CUDA allocator, or code running where cudaMalloc is not
+// must not enter the CUDA allocator, code running where cudaMalloc is not
 // permitted. dg_integrate_device allocates its per-segment partial sums on
-// first use; this variant keeps them in one fixed array in the library
-// instead, so after the plan exists nothing is allocated. The plan itself is
-// created beforehand with dg_plan_create, which does allocate.
-//
-// The array is a file-scope __device__ variable of kNoAllocScratchBytes. Host
-// code cannot use its name as a device address, so its address is obtained
-// with cudaGetSymbolAddress once per device, with that device current, on
-// the first call on that device; make that first call before any stream
-// capture. Every call on a device shares the one array: calls that overlap on
-// the GPU (from different streams or threads) race on it, so serialise them.
-// Every partial sum the finalize reads is written by the gather kernel of the
-// same call, so nothing needs clearing between calls.
+// first use; the allocation-free entry point keeps them in this one fixed
+// array instead. It is a file-scope __device__ variable of
+// kNoAllocScratchBytes, which every GPU that loads the library holds until
+// the process exits. Host code cannot use its name as a device address (a
+// kernel given the host-side name would fault or read the wrong memory), so
+// its address is looked up with cudaGetSymbolAddress, with the device
+// current, on every call: the lookup allocates nothing once the module is
+// loaded, the first call on a device loads it (make that call before any
+// stream capture), and an address never outlives a context that was reset.
 namespace dg {
 namespace {
-
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
-constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
-constexpr int kNoAllocMaxDevices = 64;
-
-static __device__ __align__(256) double g_noalloc_partial[kNoAllocScratchDoubles];
-
-std::mutex g_noalloc_mu;
-double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// The array's device address on `device` (current), resolved once.
-double *noalloc_scratch(int device) {
-    if (device < 0 || device >= kNoAllocMaxDevices)
-        fail(DG_UNSUPPORTED, "device ordinal beyond the allocation-free path's table");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partial);
-        if (e != cudaSuccess) {
-            (void)cudaGetLastError();
-            fail(DG_DEVICE, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
-                                cudaGetErrorString(e));
-        }
-        g_noalloc_ptr[device] = static_cast<double *>(p);
-    }
-    return g_noalloc_ptr[device];
-}
-
-template <typename P>
-void noalloc_launch(const GatherTable &t, double *partial, const void *frames, int64_t n_pixels,
-                    int nf, int mode, double *oi, double *os, double *od, cudaStream_t s) {
-    const P *fp = static_cast<const P *>(frames);
-    bool done = false;
-    if (t.n_units > 0) done = launch_typed<P>(t, t.variant, frames, n_pixels, nf, mode, partial,
-                                              oi, os, od, s);
-    if (t.n_rows > 0 && !done) {
-        const dim3 grid(unsigned((t.n_rows + kFinRows - 1) / kFinRows), unsigned((nf + 31) / 32));
-#define DG_NOALLOC_FINALIZE(M)                                                                 \
-    k_finalize<M, P><<<grid, 32 * kFinRows, 0, s>>>(                                           \
-        partial, t.row_seg.ptr, t.seg_ids.ptr, t.seg.ptr, t.den.ptr, t.den_std.ptr,           \
-        t.den_f32.ptr, t.valid_std.ptr, t.first_valid.ptr, t.entry_std.ptr, fp, n_pixels,      \
-        t.n_rows, t.n_segments, nf, oi, os, od)
-        if (mode == kSpread) DG_NOALLOC_FINALIZE(kSpread);
-        else if (mode == kErrors) DG_NOALLOC_FINALIZE(kErrors);
-        else DG_NOALLOC_FINALIZE(kIntensity);
-#undef DG_NOALLOC_FINALIZE
-        DG_CUDA(cudaGetLastError());
-    }
-}
-
+static __device__ __align__(256) double g_noalloc_partial[kNoAllocScratchBytes / sizeof(double)];
 }  // namespace
-}  // namespace dg
 
-extern "C" dg_status dg_integrate_device_noalloc(dg_plan *plan, const void *d_frames,
-                                                 int32_t dtype, int64_t n_frames, uint32_t flags,
-                                                 double *d_i, double *d_s, double *d_d,
-                                                 void *stream) {
-    using namespace dg;
-    try {
-        if (!plan) fail(DG_INVALID_INPUT, "plan must not be NULL");
-        if (dtype < DG_U16 || dtype > DG_F64) fail(DG_INVALID_INPUT, "unknown pixel dtype");
-        if (n_frames < 0) fail(DG_INVALID_INPUT, "frame count must not be negative");
-        if (flags & ~(DG_ERRORS | DG_AZIMUTHAL_STD)) fail(DG_INVALID_INPUT, "unknown flags");
-        if (n_frames == 0) return DG_OK;
-        if (!d_frames || !d_i) fail(DG_INVALID_INPUT, "frames and intensity must not be NULL");
-        if ((flags & DG_ERRORS) && !d_s) fail(DG_INVALID_INPUT, "errors requested without an output");
-        if ((flags & DG_AZIMUTHAL_STD) && !d_d)
-            fail(DG_INVALID_INPUT, "azimuthal_std requested without an output");
-        if ((flags & DG_AZIMUTHAL_STD) && plan->n_azimuthal != 0)
-            fail(DG_UNSUPPORTED, "azimuthal_std is defined for 1D tables only");
-        const uintptr_t pes = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
-        if (reinterpret_cast<uintptr_t>(d_frames) % pes)
-            fail(DG_INVALID_INPUT, "device frames must be aligned to the pixel size");
-        for (const void *o : {(const void *)d_i, (const void *)d_s, (const void *)d_d})
-            if (reinterpret_cast<uintptr_t>(o) % 8)
-                fail(DG_INVALID_INPUT, "device outputs must be 8-byte aligned");
-        std::lock_guard<std::mutex> lock(plan->mu);
-        int previous = -1;
-        DG_CUDA(cudaGetDevice(&previous));
-        if (previous != plan->device) DG_CUDA(cudaSetDevice(plan->device));
-        struct Restore {
-            int dev;
-            ~Restore() {
-                int now = -1;
-                if (dev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != dev) cudaSetDevice(dev);
-            }
-        } restore{previous};
-        double *scratch = noalloc_scratch(plan->device);
-        const GatherTable &t = plan->gather;
-        const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
-                                                                                    : kIntensity;
-        const bool fpx = dtype == DG_F32 || dtype == DG_F64;
-        const int na = mode == kIntensity ? 1 : mode == kErrors ? 2 : (fpx ? 5 : 3);
-        const int64_t per_frame = std::max<int64_t>(1, t.n_segments) * na;
-        const int64_t chunk = std::min<int64_t>(int64_t(kNoAllocScratchDoubles) / per_frame, 256);
-        if (chunk < 1)
-            fail(DG_UNSUPPORTED,
-                 "this plan needs " + std::to_string(per_frame * 8) +
-                     " bytes of partial sums per frame; the allocation-free path holds " +
-                     std::to_string(kNoAllocScratchBytes) + " bytes (use dg_integrate_device)");
-        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
-        const int64_t npix = int64_t(plan->dim1) * plan->dim2;
-        const size_t es = dtype == DG_U16 ? 2 : dtype == DG_F64 ? 8 : 4;
-        for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
-            const int nf = int(std::min<int64_t>(chunk, n_frames - f0));
-            const void *fp = static_cast<const unsigned char *>(d_frames) + f0 * npix * int64_t(es);
-            double *oi = d_i + f0 * t.n_rows;
-            double *os = (flags & DG_ERRORS) ? d_s + f0 * t.n_rows : nullptr;
-            double *od = (flags & DG_AZIMUTHAL_STD) ? d_d + f0 * t.n_rows : nullptr;
-            switch (dtype) {
-            case DG_U16: noalloc_launch<uint16_t>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
-            case DG_U32: noalloc_launch<uint32_t>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
-            case DG_I32: noalloc_launch<int32_t>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
-            case DG_F32: noalloc_launch<float>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
-            case DG_F64: noalloc_launch<double>(t, scratch, fp, npix, nf, mode, oi, os, od, s); break;
-            }
-        }
-        return DG_OK;
-    } catch (const Error &e) {
-        set_last_error(e.message);
-        return e.status;
-    } catch (const std::exception &e) {
-        set_last_error(e.what());
-        return DG_DEVICE;
-    } catch (...) {
-        set_last_error("unknown failure");
-        return DG_DEVICE;
+double *noalloc_scratch(size_t *n_doubles) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partial);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        fail(DG_DEVICE, std::string("cudaGetSymbolAddress of the fixed scratch array failed: ") +
+                            cudaGetErrorString(e));
     }
+    *n_doubles = kNoAllocScratchBytes / sizeof(double);
+    return static_cast<double *>(p);
 }
+
+}  // namespace dg

@@ -241,8 +241,9 @@ struct BinTiles {
     int32_t n_items = 0;
     DeviceArray<int4> item;        // {first row, rows, first chunk, chunks}, largest first
     DeviceArray<int32_t> meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
-    DeviceArray<int4> org;         // per row {chunk in tile (-1: none), slot, entry, row end}
+    DeviceArray<int4> org;         // per row {origin entry, first valid entry, row end, 0}
     DeviceArray<float4> pair_a, pair_as, pair_b;
+    DeviceArray<float2> pair_c;    // {n_lo 0, n_lo 1} (spread)
     // Per pair {slot 0, slot 1, entry 0, entry 1}, kept to build the
     // per-frame-mask pairs {slot, slot, w, w}, {w*norm, w*norm} on first use.
     DeviceArray<int4> desc;
@@ -252,7 +253,7 @@ struct BinTiles {
     PinnedFlag wait_err;
     int64_t bytes() const {
         return int64_t(item.bytes() + meta.bytes() + org.bytes() + pair_a.bytes() +
-                       pair_as.bytes() + pair_b.bytes() + desc.bytes() + pair_ra.bytes() +
+                       pair_as.bytes() + pair_b.bytes() + pair_c.bytes() + desc.bytes() + pair_ra.bytes() +
                        pair_rb.bytes());
     }
 };
@@ -273,11 +274,12 @@ struct GatherTable {
     DeviceArray<int32_t> row_seg;     // n_rows + 1: row r's segments are
     DeviceArray<int32_t> seg_ids;     //   seg_ids[row_seg[r] .. row_seg[r+1]) in strip order
     DeviceArray<int32_t> first_valid; // first entry valid for the spread, per row (-1: none)
+    DeviceArray<int32_t> origin;      // the spread's origin entry: the row's heaviest valid (-1: none)
     DeviceArray<int2> entry;          // {col, weight bits} for the I/sigma path
-    DeviceArray<float4> entry_std;    // {col bits, c, n, c/n} for the spread path
+    DeviceArray<float4> entry_std;    // {col bits, c, n, c/n} for the spread path (n in FP32)
+    DeviceArray<float> entry_nlo;     // n - FP32(n) per entry: the spread's n as an FP32 pair
     DeviceArray<double> den;          // strict f64 sum w*norm
     DeviceArray<double> den_std;      // sum c*n over entries valid for the spread
-    DeviceArray<double> den_f32;      // the same sum over the FP32-rounded c and n
     DeviceArray<int32_t> valid_std;   // entries valid for the spread, per row
     DeviceArray<double> partial;      // scratch: per (frame, segment) FP64 sums
     // Frame-lane layout (k_gather_fl): units of segments with a bounded
@@ -288,6 +290,7 @@ struct GatherTable {
     DeviceArray<int32_t> fl_px;
     DeviceArray<float4> fl_pair_a;    // {index 0 bits, index 1 bits, c0, c1}
     DeviceArray<float4> fl_pair_b;    // {n0, n1, c0/n0, c1/n1} (spread)
+    DeviceArray<float2> fl_pair_c;    // {n_lo 0, n_lo 1} (spread)
     DeviceArray<float4> fl_pair_s;    // pair_a with the spread's weights, when they differ
     const float4 *fl_pair_as = nullptr;  // the spread's pair_a (fl_pair_s or fl_pair_a)
     DeviceArray<int32_t> fl_seg_org;  // per segment: its origin pixel's index in the unit list
@@ -314,10 +317,25 @@ void gather_kernel_time(GatherTable &t, bool reset, double *ms, int64_t *gather_
 
 void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim1,
                        int32_t dim2, int32_t strip_rows, cudaStream_t stream, GatherTable &out);
-// Enqueues the batched gather for n_frames device-resident frames.
+// Enqueues the batched gather for n_frames device-resident frames. With
+// `scratch` (scratch_doubles long) the partial sums go there instead of the
+// plan's own array, which is then neither allocated nor ordered across
+// streams; frames per launch shrink to what the scratch holds.
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,
                 int64_t n_frames, uint32_t flags, int precision, double *d_i, double *d_sigma,
-                double *d_std, cudaStream_t stream);
+                double *d_std, cudaStream_t stream, double *scratch = nullptr,
+                size_t scratch_doubles = 0);
+// Whether the plan's gather writes the results itself (bin tiles: no partial
+// sums, no finalize).
+bool gather_writes_results(const GatherTable &t);
+// Allocates the plan's partial sums for launches of up to n_frames frames of
+// this dtype and these flags, ahead of the first call that needs them (not
+// for a plan whose bin tiles need none, unless `any_mapping`).
+void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtype,
+                      bool any_mapping = false);
+// The allocation-free path's fixed device array (dg_gather.cu): its address
+// on the current device, looked up on every call, and its size in doubles.
+double *noalloc_scratch(size_t *n_doubles);
 // Raw sums and per-frame masks. prepare_raw builds the entries once (from the
 // plan's masked f64 table and per-pixel norm). run_gather_raw: with d_masks
 // (n_frames masks mask_stride bytes apart, 0 = one mask for every frame;

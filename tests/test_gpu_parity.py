@@ -5,7 +5,7 @@ denominators within 1e-12 relative (the device's FP64 atan2/cos differ from
 glibc in the last bits). Integration: the reference's magnitude-scaled test
 (src/integration/cuda/tests.rs:206-227) with the tolerance of this build's
 compensated FP32 path, 1e-5 relative to sum(w*|s|)/den for intensity and
-sigma; the spread within 1e-4 relative of the FP64 oracle."""
+sigma; the spread within 1e-5 relative of the FP64 oracle."""
 import math
 
 import numpy as np
@@ -14,7 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL_I = 1e-5
-TOL_STD = 1e-4
+TOL_STD = 1e-5
 
 
 @pytest.fixture(scope="module")

@@ -13,7 +13,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL_I = 1e-5
-TOL_STD = 1e-4
+TOL_STD = 1e-5
 
 
 @pytest.fixture(scope="module")

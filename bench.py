@@ -91,7 +91,7 @@ class ClockSampler:
 
     def start(self):
         cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-               "-lms", "200"]
+               "-lms", "50"]
         if self.uuid:
             cmd += ["-i", self.uuid]
         try:
@@ -159,11 +159,11 @@ def oracle_tables(w):
     return full, table, mask, norm, den
 
 
-def cpu_reference(w, frames_np, threads: int, budget_s: float, n_steps: int):
+def cpu_reference(w, frames_np, threads: int, budget_s: float, n_steps: int, tables=None):
     """Times the oracle (restated reference CPU algorithm) frame-parallel on
     host cores; returns (frames/s, frames per sample, seconds)."""
     from oracle import oracle as o
-    full, table, mask, norm, den = oracle_tables(w)
+    full, table, mask, norm, den = tables or oracle_tables(w)
     # calibrate on a small sample, then size the per-step sample to the budget
     t = time.perf_counter()
     o.integrate_frames_mt(table, den, full, mask, norm, frames_np[:2], w.errors,
@@ -211,35 +211,30 @@ def metric_of(w) -> str:
     return METRIC if w.name == "eiger4m_ps2000_b256" else f"{w.name}_frames_per_s"
 
 
-def precision_report(w, frames, oi, os_, od, n: int = 4):
-    """Max and RMS relative error of intensity, sigma and the spread against
-    the FP64 oracle on the first n frames (bins with a nonzero finite
-    reference value)."""
+def precision_report(w, frames_np, gi, gs, gd, tables, threads: int):
+    """Max and RMS relative error of intensity, sigma and the spread of the
+    GPU results against the FP64 oracle on the same frames (bins with a
+    nonzero finite oracle value): the strict sums (normalize_bin) without
+    the spread, the reference's two-pass spread path with it."""
     import numpy as np
     from oracle import oracle as o
-    full, table, mask, norm, den = oracle_tables(w)
-    fr = frames[:n].cpu().numpy()
-    gi, gs, gd = oi[:n].cpu().numpy(), os_[:n].cpu().numpy(), od[:n].cpu().numpy()
-    errs = {"intensity": [], "sigma": [], "azimuthal_std": []}
-    for k in range(len(fr)):
-        sig = fr[k].astype(np.float64).ravel()
-        yi, ys = o.integrate_strict(table, den, sig, True)
-        errs["intensity"].append((gi[k], yi))
-        if w.errors:
-            errs["sigma"].append((gs[k], ys))
-        if w.azimuthal_std:
-            _, _, sd = o.azimuthal_std(full, mask, norm, sig, np.maximum(sig, 0))
-            errs["azimuthal_std"].append((gd[k], sd))
-    out = {"frames": int(len(fr)), "reference": "FP64 oracle (strict sums)"}
-    for name, pairs in errs.items():
-        if not pairs:
+    full, table, mask, norm, den = tables
+    yi, ys, yd = o.integrate_frames_mt(table, den, full, mask, norm, frames_np, w.errors,
+                                       w.azimuthal_std, threads)
+    out = {"frames": int(len(frames_np)),
+           "reference": "FP64 oracle: strict CSR sums, or the two-pass spread path when "
+                        "the spread is requested"}
+    for name, got, ref in (("intensity", gi, yi), ("sigma", gs, ys), ("azimuthal_std", gd, yd)):
+        if got is None or ref is None:
             continue
-        got = np.concatenate([a for a, _ in pairs])
-        ref = np.concatenate([b for _, b in pairs])
         ok = np.isfinite(ref) & (ref != 0)
         rel = np.abs(got[ok] - ref[ok]) / np.abs(ref[ok])
-        out[name] = {"max_rel": float(rel.max()), "rms_rel": float(np.sqrt(np.mean(rel ** 2))),
+        out[name] = {"max_rel": float(rel.max()) if rel.size else 0.0,
+                     "rms_rel": float(np.sqrt(np.mean(rel ** 2))) if rel.size else 0.0,
                      "bins": int(ok.sum())}
+        if name == "azimuthal_std":
+            out[name]["nan_pattern_equal"] = bool(np.array_equal(np.isfinite(ref),
+                                                                 np.isfinite(got)))
     return out
 
 
@@ -619,9 +614,11 @@ def main():
         "build_ms": round(info.build_ms, 2),
         "autotune_ms_wall": round(tune_ms, 1),
     }
-    if w.kind == "precision" and rank == 0:
-        torch.cuda.synchronize()
-        line["precision"] = precision_report(w, frames, oi, os_, od)
+    # The timed steps' results for the first frames, kept for the precision
+    # report (the legs below write the same output buffers).
+    n_check = min(4, n_frames)
+    checked = [None if a is None else a[:n_check].cpu().numpy()
+               for a in (oi, os_ if w.errors else None, od if w.azimuthal_std else None)]
     if not args.no_extras and rank == 0:
         # plain one-frame-per-launch GPU path on the same resident frames,
         # with the lane mapping tuned for one-frame launches
@@ -638,9 +635,15 @@ def main():
             step(L.dg_integrate_device_plain, nplain)
         p1.record(stream)
         torch.cuda.synchronize()
-        line["plain"] = {"value": round(nplain * reps / (p0.elapsed_time(p1) / 1000), 2),
-                         "unit": "frames/s", "frames": nplain * reps,
-                         "gather_variant": plan.gather_variant}
+        plain_s = p0.elapsed_time(p1) / 1000 / (nplain * reps)
+        # its own roofline: every launch reads the table and one frame
+        alg1 = E * 8 + (nb + 1) * 4 + nb * 8 + w.dim1 * w.dim2 * px + nb * k_out * 8
+        line["plain"] = {"value": round(1.0 / plain_s, 2), "unit": "frames/s",
+                         "frames": nplain * reps, "gather_variant": plan.gather_variant,
+                         "ms_per_frame": round(plain_s * 1000, 4),
+                         "alg_bytes_per_frame": alg1,
+                         "achieved_gbs": round(alg1 / plain_s / 1e9, 1),
+                         "frac": round(alg1 / plain_s / 1e9 / peak, 4)}
         plan.gather_variant = batch_variant
         if not w.n_azimuthal:
             line.update(masked_legs(w, plan, frames, stream, peak))
@@ -670,13 +673,18 @@ def main():
         if w.dtype in ("uint16", "uint32", "int32"):
             line["e2e_bslz4"] = bslz4_leg(w, plan, frames, n_frames, flags, hi, hs, hd, peak)
         if world == 1:
+            # the CPU leg: the oracle times the reference's algorithm on the
+            # host cores and, as the checker, states the GPU results' error
+            threads = os.cpu_count() or 1
+            tables = oracle_tables(w)
             fr_np = frames[:16].cpu().numpy()
-            rate, per_step, secs = cpu_reference(w, fr_np, os.cpu_count() or 1, 15.0, 3)
+            rate, per_step, secs = cpu_reference(w, fr_np, threads, 15.0, 3, tables)
             line["cpu_baseline"] = {
-                "value": round(rate, 3), "unit": "frames/s", "cores": os.cpu_count() or 1,
+                "value": round(rate, 3), "unit": "frames/s", "cores": threads,
                 "kind": "port",
                 "sample": f"{per_step * 3} frames of {w.name} in 3 timed samples; C restatement "
                           "of the reference's strict CSR row kernel and azimuthal spread"}
+            line["precision"] = precision_report(w, fr_np[:n_check], *checked, tables, threads)
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()

@@ -34,6 +34,7 @@ EXPORTS = [
     "dg_integrate_raw_device", "dg_host_alloc", "dg_host_free", "dg_host_is_pinned",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
+    "dg_multi_create", "dg_multi_destroy", "dg_multi_integrate",
     "dg_device_info_get", "dg_last_error",
 ]
 
@@ -80,6 +81,11 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "submitted", "completed", "failed", "launches", "coalesced_frames", "plan_builds",
         "plan_hits", "plan_evictions", "cache_bytes", "batch_us", "build_us")]
+
+
+class MultiItem(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("d_frames", C.c_void_p), ("n_frames", C.c_int64),
+                ("d_intensity", C.c_void_p), ("d_sigma", C.c_void_p), ("d_std", C.c_void_p)]
 
 
 class DeviceInfo(C.Structure):
@@ -152,6 +158,9 @@ def lib():
                                        P(C.c_uint64)]
         L.dg_server_poll.argtypes = [vp, C.c_uint64, C.c_int32, pd, pd, pd, pd]
         L.dg_server_stats_get.argtypes = [vp, P(ServerStats)]
+        L.dg_multi_create.argtypes = [C.c_int32, C.c_int32, P(vp)]
+        L.dg_multi_destroy.argtypes = [vp]
+        L.dg_multi_integrate.argtypes = [vp, P(MultiItem), C.c_int32, C.c_int32, C.c_uint32, vp]
         L.dg_device_info_get.argtypes = [C.c_int32, P(DeviceInfo)]
         L.dg_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.dg_last_error.restype = C.c_int32

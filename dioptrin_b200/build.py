@@ -33,6 +33,7 @@ SOURCES = {
     "dg_api.cu": [],
     "dg_server.cu": [],
     "dg_bslz4.cu": [],
+    "dg_multi.cu": [],
 }
 
 

@@ -1815,6 +1815,63 @@ __global__ void __launch_bounds__(256)
                            den_std, valid_std, n_rows, n_frames, out_i, out_s, out_d);
 }
 
+// Work-queue gather over several plans (dg_multi_integrate). A persistent
+// grid of entry-lane CTAs (lane mapping 2: 8 entry slices, 2 frames per lane,
+// 4 entries in flight) claims (plan, unit) items from one counter until every
+// plan's units are summed, so plans of very different sizes share one launch
+// and the GPU stays full to the last unit; then a grid-stride finalize walks
+// the (plan, row tile, frame block) items. A plan's sums are those of
+// mapping 2 launched for that plan alone, bit for bit.
+constexpr int kQueueSlices = 8, kQueueFpl = 2, kQueueU = 4;
+
+// The last descriptor whose prefix field (first unit or first tile) is at
+// most `item`: descriptors with nothing to do share the next one's prefix
+// and are skipped.
+template <bool TILES>
+__device__ __forceinline__ int queue_owner(const QueuePlan *__restrict__ plans, int n_plans,
+                                           int item) {
+    int lo = 0, hi = n_plans - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int first = TILES ? plans[mid].tile_first : plans[mid].unit_first;
+        if (first <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int MODE, typename P>
+__global__ void __launch_bounds__(kThreads)
+    k_gather_queue(QueueHeader *__restrict__ hdr, const QueuePlan *__restrict__ plans) {
+    __shared__ int s_item;
+    const int n_plans = hdr->n_plans, total = hdr->total_units;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();  // every thread has read s_item before it is claimed again
+        if (item >= total) return;
+        const QueuePlan &q = plans[queue_owner<false>(plans, n_plans, item)];
+        gather_unit<MODE, P, kQueueSlices, kQueueFpl, kQueueU>(
+            item - q.unit_first, q.unit, q.seg, q.entry, q.entry_std, q.entry_nlo, q.first_valid,
+            q.origin, static_cast<const P *>(q.frames), q.n_pixels, q.n_frames, q.n_segments,
+            q.partial, nullptr, 0);
+    }
+}
+
+template <int MODE, typename P>
+__global__ void __launch_bounds__(256)
+    k_finalize_queue(const QueueHeader *__restrict__ hdr, const QueuePlan *__restrict__ plans) {
+    const int n_plans = hdr->n_plans, total = hdr->total_tiles;
+    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+        const QueuePlan &q = plans[queue_owner<true>(plans, n_plans, tile)];
+        const int local = tile - q.tile_first;
+        finalize_tile<MODE, P>((local / q.frame_blocks) * kFinRows, (local % q.frame_blocks) * 32,
+                               q.partial, q.row_seg, q.seg_ids, q.den, q.den_std, q.valid_std,
+                               q.n_rows, q.n_frames, q.out_i, q.out_s, q.out_d);
+    }
+}
+
 // Raw sums per (frame, row) (IntermediateResult1d, lut/integrate.rs:372-379):
 // S and V from the partial sums; N and C from them too for the per-frame-mask
 // gather, else the plan's strict FP64 denominator and weight sum.
@@ -2552,6 +2609,89 @@ void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtyp
                          n_accumulators(mode, dtype == DG_F32 || dtype == DG_F64) *
                          std::min<int64_t>(256, (n_frames + 31) / 32 * 32);
     if (t.partial.count < size_t(need)) t.partial.alloc(size_t(need));
+}
+
+QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixels, int n_frames,
+                     double *oi, double *os, double *od) {
+    QueuePlan q{};
+    q.unit = t.unit.ptr;
+    q.seg = t.seg.ptr;
+    q.entry = t.entry.ptr;
+    q.entry_std = t.entry_std.ptr;
+    q.entry_nlo = t.entry_nlo.ptr;
+    q.first_valid = t.first_valid.ptr;
+    q.origin = t.origin.ptr;
+    q.frames = d_frames;
+    q.partial = t.partial.ptr;
+    q.row_seg = t.row_seg.ptr;
+    q.seg_ids = t.seg_ids.ptr;
+    q.den = t.den.ptr;
+    q.den_std = t.den_std.ptr;
+    q.valid_std = t.valid_std.ptr;
+    q.out_i = oi;
+    q.out_s = os;
+    q.out_d = od;
+    q.n_pixels = n_pixels;
+    q.n_frames = n_frames;
+    q.n_segments = t.n_segments;
+    q.n_units = n_frames > 0 ? t.n_units : 0;
+    q.n_rows = n_frames > 0 ? t.n_rows : 0;
+    q.frame_blocks = std::max(1, (n_frames + 31) / 32);
+    return q;
+}
+
+namespace {
+
+// Persistent grid of the work-queue gather: the CTAs one SM holds at once,
+// times the SMs (the CTAs then stay resident and claim items to the end).
+template <int MODE, typename P>
+int queue_gather_grid() {
+    static int grid = 0;
+    if (grid == 0) {
+        const size_t smem = size_t(kUnitCap) * (MODE == kSpread ? 16 : 8);
+        int per_sm = 0, dev = 0, sms = 0;
+        DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_queue<MODE, P>,
+                                                              kThreads, smem));
+        DG_CUDA(cudaGetDevice(&dev));
+        DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        grid = std::max(1, per_sm) * std::max(1, sms);
+    }
+    return grid;
+}
+
+template <int MODE, typename P>
+void queue_launch_typed(QueueHeader *hdr, const QueuePlan *plans, cudaStream_t s) {
+    const size_t smem = size_t(kUnitCap) * (MODE == kSpread ? 16 : 8);
+    k_gather_queue<MODE, P><<<queue_gather_grid<MODE, P>(), kThreads, smem, s>>>(hdr, plans);
+    DG_CUDA(cudaGetLastError());
+    int dev = 0, sms = 0;
+    DG_CUDA(cudaGetDevice(&dev));
+    DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    k_finalize_queue<MODE, P><<<8 * sms, 32 * kFinRows, 0, s>>>(hdr, plans);
+    DG_CUDA(cudaGetLastError());
+}
+
+template <typename P>
+void queue_launch_mode(int mode, QueueHeader *hdr, const QueuePlan *plans, cudaStream_t s) {
+    if (mode == kSpread) queue_launch_typed<kSpread, P>(hdr, plans, s);
+    else if (mode == kErrors) queue_launch_typed<kErrors, P>(hdr, plans, s);
+    else queue_launch_typed<kIntensity, P>(hdr, plans, s);
+}
+
+}  // namespace
+
+void queue_launch(int dtype, uint32_t flags, QueueHeader *hdr, const QueuePlan *plans,
+                  cudaStream_t s) {
+    const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
+                                                                                : kIntensity;
+    switch (dtype) {
+    case DG_U16: queue_launch_mode<uint16_t>(mode, hdr, plans, s); break;
+    case DG_U32: queue_launch_mode<uint32_t>(mode, hdr, plans, s); break;
+    case DG_I32: queue_launch_mode<int32_t>(mode, hdr, plans, s); break;
+    case DG_F32: queue_launch_mode<float>(mode, hdr, plans, s); break;
+    case DG_F64: queue_launch_mode<double>(mode, hdr, plans, s); break;
+    default: fail(DG_INVALID_INPUT, "unknown pixel dtype");
+    }
 }
 
 void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixels,

@@ -333,6 +333,41 @@ bool gather_writes_results(const GatherTable &t);
 // for a plan whose bin tiles need none, unless `any_mapping`).
 void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtype,
                       bool any_mapping = false);
+// Work-queue gather over several plans (dg_multi.cu, dg_gather.cu): one
+// descriptor per (plan, batch of frames), after a header. The gather's CTAs
+// claim (plan, unit) items from `counter` until total_units are done; the
+// finalize walks (plan, row tile, frame block) items. Prefix indices give
+// each plan's first unit and first finalize tile.
+struct QueuePlan {
+    const int2 *unit;
+    const int4 *seg;
+    const int2 *entry;
+    const float4 *entry_std;
+    const float *entry_nlo;
+    const int32_t *first_valid;
+    const int32_t *origin;
+    const void *frames;
+    double *partial;
+    const int32_t *row_seg;
+    const int32_t *seg_ids;
+    const double *den;
+    const double *den_std;
+    const int32_t *valid_std;
+    double *out_i, *out_s, *out_d;
+    int64_t n_pixels;
+    int32_t n_frames, n_segments, n_units, n_rows;
+    int32_t unit_first, tile_first, frame_blocks, pad;
+};
+struct QueueHeader {
+    int32_t n_plans, total_units, total_tiles, counter;  // counter: 0 before each launch
+};
+// Fills a descriptor from a plan's gather table (prefix fields left 0).
+QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixels, int n_frames,
+                     double *oi, double *os, double *od);
+// Enqueues the work-queue gather and its finalize for descriptors already
+// in device memory (`hdr` followed by the descriptors) on `s`.
+void queue_launch(int dtype, uint32_t flags, QueueHeader *hdr, const QueuePlan *plans,
+                  cudaStream_t s);
 // The allocation-free path's fixed device array (dg_gather.cu): its address
 // on the current device, looked up on every call, and its size in doubles.
 double *noalloc_scratch(size_t *n_doubles);

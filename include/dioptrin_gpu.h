@@ -374,6 +374,40 @@ DG_EXPORT dg_status dg_server_poll(dg_server *server, uint64_t ticket, int32_t w
                          double *latency_us);
 DG_EXPORT dg_status dg_server_stats_get(dg_server *server, dg_server_stats *out);
 
+/* ---- Several plans in one launch (work-queue gather) ----
+ * No counterpart in the reference, whose engine launches one plan at a time
+ * (src/integration/cuda/device.rs:1417-1584; streaming driver
+ * src/batch/bounded.rs:172). A dg_multi integrates batches of device-resident
+ * frames of several plans together: a persistent grid of gather CTAs takes
+ * (plan, unit) work items from one counter until every plan's table is
+ * summed, so plans of very different sizes share the GPU without a launch
+ * per plan, and one finalize pass normalises all of them. The device work of
+ * a call (descriptor copy, gather, finalize) is a CUDA graph captured on the
+ * first call of each (dtype, flags) and replayed after that. Every plan is
+ * summed with the entry-lane lane mapping 2, so each item's results equal
+ * dg_integrate_device of that plan with mapping 2 selected, bit for bit.
+ * Items share one dtype and one set of flags; a plan appears in at most one
+ * item of a call; an item carries 0..256 frames. Calls on one dg_multi are
+ * serialised (a call waits until the previous one's device work is done
+ * before it rewrites the descriptors). Plans are locked for the call, as by
+ * dg_integrate_device. */
+typedef struct dg_multi dg_multi;
+typedef struct dg_multi_item {
+    dg_plan *plan;
+    const void *d_frames;   /* n_frames frames of the plan's shape, device memory */
+    int64_t n_frames;       /* 0..256 */
+    double *d_intensity;    /* n_frames x n_bins, device memory */
+    double *d_sigma;        /* with DG_ERRORS */
+    double *d_std;          /* with DG_AZIMUTHAL_STD (1D plans) */
+} dg_multi_item;
+DG_EXPORT dg_status dg_multi_create(int32_t device, int32_t max_plans, dg_multi **out);
+DG_EXPORT dg_status dg_multi_destroy(dg_multi *multi);
+/* Enqueues the items on `stream` (a cudaStream_t; NULL = the multi's own).
+ * No synchronisation: the caller owns completion. */
+DG_EXPORT dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items,
+                                       int32_t n_items, int32_t dtype, uint32_t flags,
+                                       void *stream);
+
 /* Device description; cuda_info (src/integration/cuda.rs:262-329). */
 typedef struct dg_device_info {
     int32_t available;

@@ -238,59 +238,76 @@ def precision_report(w, frames_np, gi, gs, gd, tables, threads: int):
     return out
 
 
-def run_serving(args):
-    """Mixed stream: seeded Poisson arrivals over six plans (Pilatus-1M,
-    Eiger-4M and Eiger-9M shapes, each as a 1D PixelSplit pattern and a 2D
-    supersampled n_ss=2 cake) through the request loop; halfway through, two
-    plans get a new PONI (distance +1 mm, rot1 +0.001), which forces a
-    rebuild. Frames are page-locked host frames submitted without a host copy.
-    Reports completed frames/s and submit-to-result latency, for the
-    coalescing loop and for the same arrivals served one request per launch
-    (the plain GPU path: max_coalesce 1)."""
-    import math
-    import threading
-    import numpy as np
-    import dioptrin_b200 as dg
-    from dioptrin_b200 import workloads as W
-    shapes = [W.PILATUS_1M, W.EIGER_4M, W.EIGER_9M]
-    specs = []  # (key, workload, method, n_radial, n_azimuthal, errors, std)
-    for i, w in enumerate(shapes):
-        specs.append((2 * i + 1, w, "pixel_split", (1250, 2000, 3000)[i], 0, True, i == 1))
-        specs.append((2 * i + 2, w, "supersampled", (500, 1000, 1000)[i], (180, 360, 360)[i],
-                      True, False))
+SERVE_CONFIG = ("mixed stream: 6 plans (Pilatus-1M, Eiger-4M, Eiger-9M shapes x 1D pixel_split "
+                "1250-3000 bins / 2D supersampled n_ss=2 500x180-1000x360), seeded Poisson "
+                "arrivals, page-locked host frames submitted without a host copy, the two "
+                "Eiger-9M plans get a new PONI halfway (rebuilt on the device), plans built "
+                "before the stream, 60 GB plan cache")
 
-    def integrator(w, method, moved=False):
+
+class Serving:
+    """Mixed stream through the request loop: six plans (Pilatus-1M, Eiger-4M
+    and Eiger-9M shapes, each as a 1D PixelSplit pattern and a 2D
+    supersampled n_ss=2 cake), seeded Poisson arrivals; halfway through, the
+    two Eiger-9M plans get a new PONI (distance +1 mm, rot1 +0.001), which
+    forces a rebuild. Frames are page-locked host frames submitted without a
+    host copy. A stream reports completed frames/s and submit-to-result
+    latency; with max_coalesce 1 the same arrivals are served one request
+    per launch (the plain GPU path)."""
+
+    def __init__(self):
+        import numpy as np
+        import dioptrin_b200 as dg
+        from dioptrin_b200 import workloads as W
+        self.np, self.dg = np, dg
+        shapes = [W.PILATUS_1M, W.EIGER_4M, W.EIGER_9M]
+        self.specs = []  # (key, workload, method, n_radial, n_azimuthal, errors, std)
+        for i, w in enumerate(shapes):
+            self.specs.append((2 * i + 1, w, "pixel_split", (1250, 2000, 3000)[i], 0, True,
+                               i == 1))
+            self.specs.append((2 * i + 2, w, "supersampled", (500, 1000, 1000)[i],
+                               (180, 360, 360)[i], True, False))
+        self.pools = {}
+        for key, w, method, nr, na, err, std in self.specs:
+            src = W.frames_numpy(w, 3)
+            self.pools[key] = dg.alloc_pinned(src.shape, src.dtype)
+            self.pools[key][:] = src
+
+    def integrator(self, w, method, moved=False):
         pd = w.poni_dict()
         if moved:
             pd = dict(pd, distance=pd["distance"] + 1e-3, rot1=pd["rot1"] + 1e-3)
-        it = dg.Integrator.from_poni_dict(pd, method=method, n_ss=2,
-                                          polarization_factor=w.polarization_factor)
+        it = self.dg.Integrator.from_poni_dict(pd, method=method, n_ss=2,
+                                               polarization_factor=w.polarization_factor)
         it.set_mask(w.mask())
         return it
 
-    pools = {}
-    for key, w, method, nr, na, err, std in specs:
-        src = W.frames_numpy(w, 3)
-        pools[key] = dg.alloc_pinned(src.shape, src.dtype)
-        pools[key][:] = src
-    rng = np.random.default_rng(20261203 + 5)
-    n = int(args.rate * args.seconds)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n))
-    picks = rng.integers(0, len(specs), n)
+    def register(self, loop, spec, moved=False):
+        import math
+        key, w, method, nr, na, err, std = spec
+        loop.register(key, self.integrator(w, method, moved), w.shape, nr, n_azimuthal=na,
+                      azimuthal_range=(-math.pi, math.pi) if na else None)
 
-    def stream(max_coalesce):
+    def stream(self, rate: float, seconds: float, max_coalesce: int) -> dict:
+        import threading
+        np, dg = self.np, self.dg
+        rng = np.random.default_rng(20261203 + 5)
+        n = int(rate * seconds)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        picks = rng.integers(0, len(self.specs), n)
         loop = dg.RequestLoop(cache_bytes=60 << 30, max_inflight_frames=1024,
                               max_coalesce=max_coalesce)
-        for key, w, method, nr, na, err, std in specs:
-            loop.register(key, integrator(w, method), w.shape, nr, n_azimuthal=na,
-                          azimuthal_range=(-math.pi, math.pi) if na else None)
+        for spec in self.specs:
+            key, w, method, nr, na, err, std = spec
+            self.register(loop, spec)
             # build, tune and warm every plan before the stream
-            loop.poll(loop.submit(key, pools[key][0], errors=err, azimuthal_std=std), key,
-                      errors=err, azimuthal_std=std)
+            loop.poll(loop.submit(key, self.pools[key][0], errors=err, azimuthal_std=std), key,
+                      errors=err, azimuthal_std=std, wait_ms=120000)
+        warm = loop.stats()
         tickets = [None] * n
-        t0 = time.perf_counter()
-        half = args.seconds / 2
+        half = seconds / 2
         moved = {"done": False}
+        t0 = time.perf_counter()
 
         def producer(lane, lanes):
             for k in range(lane, n, lanes):
@@ -299,12 +316,10 @@ def run_serving(args):
                     time.sleep(wait)
                 if lane == 0 and not moved["done"] and arrivals[k] >= half:
                     moved["done"] = True
-                    for key, w, method, nr, na, err, std in (specs[2], specs[5]):
-                        loop.register(key, integrator(w, method, moved=True), w.shape, nr,
-                                      n_azimuthal=na,
-                                      azimuthal_range=(-math.pi, math.pi) if na else None)
-                key, w, method, nr, na, err, std = specs[int(picks[k])]
-                frame = pools[key][k % len(pools[key])]
+                    for spec in (self.specs[4], self.specs[5]):
+                        self.register(loop, spec, moved=True)
+                key, w, method, nr, na, err, std = self.specs[int(picks[k])]
+                frame = self.pools[key][k % len(self.pools[key])]
                 tickets[k] = (key, loop.submit(key, frame, errors=err, azimuthal_std=std,
                                                wait_ms=60000, borrow=True), err, std,
                               time.perf_counter() - t0)
@@ -323,28 +338,41 @@ def run_serving(args):
         loop.close()
         lat = np.array(lat) / 1000.0
         submitted = max(tk[4] for tk in tickets)
-        return {"value": round(n / elapsed, 2),
+        return {"offered": rate, "value": round(n / elapsed, 2), "unit": "frames/s",
                 "p50_ms": round(float(np.percentile(lat, 50)), 3),
                 "p99_ms": round(float(np.percentile(lat, 99)), 3),
                 "max_ms": round(float(lat.max()), 3),
-                "achieved_submit_rate": round(n / submitted, 1),
+                "achieved_submit_rate": round(n / submitted, 1), "requests": n,
                 "seconds": round(elapsed, 3),
-                "server": {k: int(v) for k, v in st.items()}}
+                "server": {k: int(v) - (0 if k == "cache_bytes" else int(warm[k]))
+                           for k, v in st.items()}}
 
-    main = stream(32)
-    plain = stream(1)
+
+def serve_leg(rates=(1000.0, 2500.0), seconds: float = 2.0) -> dict:
+    """The mixed-stream part of the metric for the default bench line: the
+    coalescing loop and the plain path (one request per launch) on the same
+    arrivals, at each offered rate."""
+    sv = Serving()
+    out = {"config": SERVE_CONFIG, "seconds_per_stream": seconds, "loop": [], "plain": []}
+    for rate in rates:
+        out["loop"].append(sv.stream(rate, seconds, 32))
+        out["plain"].append(sv.stream(rate, seconds, 1))
+    return out
+
+
+def run_serving(args):
+    sv = Serving()
+    main = sv.stream(args.rate, args.seconds, 32)
+    plain = sv.stream(args.rate, args.seconds, 1)
     line = {
         "metric": "mixed_stream_frames_per_s", "value": main["value"],
         "unit": "frames/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
         "p50_ms": main["p50_ms"], "p99_ms": main["p99_ms"], "max_ms": main["max_ms"],
         "offered_rate": args.rate, "achieved_submit_rate": main["achieved_submit_rate"],
-        "requests": n, "seconds": main["seconds"], "server": main["server"],
+        "requests": main["requests"], "seconds": main["seconds"], "server": main["server"],
         "plain": plain,
-        "config": {"workload": "mixed stream: 6 plans (Pilatus-1M, Eiger-4M, Eiger-9M shapes "
-                               "x 1D pixel_split 1250-3000 bins / 2D supersampled n_ss=2 "
-                               "500x180-1000x360), page-locked host frames submitted "
-                               "without a host copy, 2 mid-stream PONI changes",
-                   "cache_bytes": 60 << 30, "max_coalesce": 32, "max_inflight_frames": 1024,
+        "config": {"workload": SERVE_CONFIG, "cache_bytes": 60 << 30, "max_coalesce": 32,
+                   "max_inflight_frames": 1024,
                    "plain": "the same arrivals, one request per launch (max_coalesce 1)"},
     }
     print(json.dumps(line), flush=True)
@@ -685,6 +713,12 @@ def main():
                 "sample": f"{per_step * 3} frames of {w.name} in 3 timed samples; C restatement "
                           "of the reference's strict CSR row kernel and azimuthal spread"}
             line["precision"] = precision_report(w, fr_np[:n_check], *checked, tables, threads)
+        if world == 1 and w.name == "eiger4m_ps2000_b256":
+            # the second half of the metric: mixed-stream p50/p99 against the
+            # plain path (plans built before each stream)
+            del frames, oi, os_, od
+            torch.cuda.empty_cache()
+            line["serve"] = serve_leg()
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()

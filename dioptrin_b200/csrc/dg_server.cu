@@ -1,19 +1,30 @@
 // Request loop: continuous batching of single-frame requests across plans.
 //
 // Requests are admitted while in-flight slots remain (a submit waits, bounded,
-// for a slot). Worker threads take the oldest queued request, coalesce every
-// queued request with the same plan key, dtype and flags behind it (up to
-// max_coalesce) into one launch, and publish results per request. Plans live
-// in an HBM cache bounded by bytes: a miss builds the plan on the device, and
-// least-recently-used plans that no worker is using are evicted until the
-// cache fits. Four workers run batches concurrently on their own streams,
-// so one batch's copies overlap another's gather. A submit copies its frame
-// into a pooled pinned buffer outside the server lock; the worker copies the
-// pinned buffers straight to the device. Re-registering a key (a changed
-// PONI) gives it a new generation: the next request rebuilds the plan, and
-// the stale plan is destroyed once no worker uses it. Each request's result
-// is identical alone and in any mix: the gather's arithmetic depends only on
-// the plan, never on which frames share a launch.
+// for a slot). Worker threads take the oldest queued request whose plan is
+// built, coalesce every queued request with the same plan key, dtype and
+// flags behind it (up to max_coalesce) into one launch, and publish results
+// per request; requests of other built plans with the same dtype and flags
+// join the batch (up to eight plans), which runs as one work-queue gather
+// (dg_multi: a persistent grid over (plan, unit) items, replayed as a CUDA
+// graph). Four workers run batches concurrently on their own streams, so one
+// batch's copies overlap another's gather; their staging grows stream-ordered
+// and is kept. max_coalesce 1 serves one request per launch on the plan's own
+// tuned lane mapping (the plain path). Plans live in an HBM cache bounded by
+// bytes and are managed by one builder thread: a request for a plan that is
+// not built asks the builder and stays queued while the workers serve other
+// plans; the builder builds the plan on the device, tunes it once per key
+// for small launches, allocates its partial sums for the largest launch,
+// admits it by evicting least-recently-used plans that no worker is using,
+// and destroys evicted and stale plans, so no worker ever waits for a build
+// or a free. A submit copies its frame into a pooled pinned buffer outside
+// the server lock (or borrows the caller's); the worker copies the pinned
+// buffers straight to the device. Re-registering a key (a changed PONI)
+// gives it a new generation: the next request rebuilds the plan, and the
+// stale plan is destroyed once no worker uses it. A build that fails fails
+// the requests of that generation. Each request's result is identical alone
+// and in any mix: the gather's arithmetic depends only on the plan, never on
+// which frames or plans share a launch.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -110,7 +121,7 @@ std::string last_error_text() {
 struct dg_server {
     dg_server_config cfg{};
     std::mutex mu;
-    std::condition_variable cv_work, cv_done, cv_slot;
+    std::condition_variable cv_work, cv_done, cv_slot, cv_build;
     std::unordered_map<uint64_t, PlanSpec> specs;
     std::unordered_map<uint64_t, CacheEntry> cache;
     std::deque<Request *> queue;
@@ -121,22 +132,31 @@ struct dg_server {
     dg_server_stats stats{};
     bool stop = false;
     std::vector<std::thread> workers;
+    std::thread builder;
     PinnedPool pinned;
-    std::vector<CacheEntry> retired;  // stale plans still in use
+    std::vector<CacheEntry> retired;    // stale plans still in use by a worker
+    std::vector<dg_plan *> to_destroy;  // plans no worker uses, for the builder
     uint64_t next_generation = 1;
-    std::unordered_map<uint64_t, int> building;  // keys a worker is building now
+    // Plans to build, once per key and generation: the first request's dtype
+    // and flags tune the new plan.
+    std::deque<uint64_t> build_queue;
+    std::unordered_map<uint64_t, std::pair<int32_t, uint32_t>> build_pending;
+    struct BuildFailure {
+        uint64_t generation;
+        dg_status status;
+        std::string message;
+    };
+    std::unordered_map<uint64_t, BuildFailure> failed;
     std::unordered_map<uint64_t, int32_t> tuned;  // key -> lane mapping its last plan used
 
-    // Returns a plan for `key` with a user reference, building it on a miss and
-    // evicting idle LRU plans to stay within the byte budget. Called unlocked.
     // A new plan's lane mapping, tuned for the small coalesced launches of the
     // loop on zero frames of the request's type (timing does not depend on
-    // the values); left at the default if anything fails.
+    // the values); left at the default if anything fails. Builder thread.
     void tune(dg_plan *plan, int32_t dtype, uint32_t flags) {
         const int64_t nf = std::max(1, std::min(8, cfg.max_coalesce));
         const size_t bytes = size_t(plan->dim1) * plan->dim2 * px_size(dtype) * size_t(nf);
         void *d = nullptr;
-        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+        if (cudaMallocAsync(&d, bytes, plan->stream) != cudaSuccess) {
             (void)cudaGetLastError();
             return;
         }
@@ -144,284 +164,397 @@ struct dg_server {
         if (dg_plan_autotune(plan, d, dtype, nf, flags & (DG_ERRORS | DG_AZIMUTHAL_STD), nullptr,
                              nullptr, nullptr, 0) != DG_OK)
             (void)last_error_text();
-        cudaFree(d);
+        cudaFreeAsync(d, plan->stream);
+        cudaStreamSynchronize(plan->stream);
     }
 
-    dg_plan *acquire(uint64_t key, int32_t dtype, uint32_t flags, std::string &err,
-                     dg_status &st) {
-        PlanSpec spec;
-        {
-            std::unique_lock<std::mutex> lock(mu);
-            spec = specs.at(key);
-            auto it = cache.find(key);
-            if (it != cache.end() && it->second.generation == spec.generation) {
-                it->second.users++;
-                it->second.last_use = ++use_clock;
-                stats.plan_hits++;
-                return it->second.plan;
-            }
-            if (it != cache.end()) retire_locked(it);
-            building[key]++;
-        }
-        struct Built {
-            dg_server *s;
-            uint64_t key;
-            ~Built() {
-                std::lock_guard<std::mutex> lock(s->mu);
-                if (--s->building[key] == 0) s->building.erase(key);
-            }
-        } built{this, key};
-        const auto t_build = Clock::now();
-        dg_plan *plan = nullptr;
-        st = dg_plan_create(&spec.geometry, &spec.method, spec.mask.empty() ? nullptr : spec.mask.data(),
-                            spec.dim1, spec.dim2, spec.n_radial, spec.n_azimuthal,
-                            spec.has_az_range ? spec.az_range : nullptr, &plan);
-        if (st != DG_OK) {
-            err = last_error_text();
-            return nullptr;
-        }
-        // A rebuilt key (new PONI, same shape and bins) keeps the mapping its
-        // previous plan was tuned to; a new key is tuned once.
-        int32_t known = -1;
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            auto t = tuned.find(key);
-            if (t != tuned.end()) known = t->second;
-        }
-        if (known < 0 || dg_plan_variant(plan, known, nullptr, nullptr) != DG_OK) {
-            tune(plan, dtype, flags);
-            int32_t v = 0;
-            dg_plan_variant(plan, -1, &v, nullptr);
-            std::lock_guard<std::mutex> lock(mu);
-            tuned[key] = v;
-        }
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            stats.build_us += int64_t(
-                std::chrono::duration<double, std::micro>(Clock::now() - t_build).count());
-        }
-        dg_plan_info info{};
-        dg_plan_query(plan, &info);
-        std::vector<dg_plan *> evicted;
-        dg_plan *result = nullptr;
-        {
-            std::unique_lock<std::mutex> lock(mu);
-            auto it = cache.find(key);
-            if (it != cache.end() && it->second.generation != spec.generation) {
-                retire_locked(it);
-                it = cache.end();
-            }
-            if (it != cache.end()) {  // another worker built it meanwhile
-                evicted.push_back(plan);
-                it->second.users++;
-                it->second.last_use = ++use_clock;
-                result = it->second.plan;
-            } else {
-                stats.plan_builds++;
-                // Admission by memory: evict idle plans, oldest first.
-                while (cache_bytes + info.device_bytes > cfg.cache_bytes) {
-                    uint64_t victim = 0, oldest = UINT64_MAX;
-                    for (auto &kv : cache)
-                        if (kv.second.users == 0 && kv.second.last_use < oldest) {
-                            oldest = kv.second.last_use;
-                            victim = kv.first;
-                        }
-                    if (oldest == UINT64_MAX) break;  // everything busy: over budget briefly
-                    cache_bytes -= cache[victim].bytes;
-                    evicted.push_back(cache[victim].plan);
-                    cache.erase(victim);
-                    stats.plan_evictions++;
-                }
-                CacheEntry e;
-                e.plan = plan;
-                e.bytes = info.device_bytes;
-                e.users = 1;
-                e.last_use = ++use_clock;
-                e.generation = spec.generation;
-                cache[key] = e;
-                cache_bytes += e.bytes;
-                result = plan;
-            }
-        }
-        for (dg_plan *p : evicted) dg_plan_destroy(p);
-        return result;
+    // Queues a build of `key` unless one is queued or running (lock held).
+    void request_build_locked(uint64_t key, int32_t dtype, uint32_t flags) {
+        if (build_pending.count(key)) return;
+        build_pending[key] = {dtype, flags};
+        build_queue.push_back(key);
+        cv_build.notify_one();
     }
 
-    // Moves a stale cache entry out of the cache (lock held): destroyed now
-    // if idle, else when its last user releases it.
+    // Moves a stale cache entry out of the cache (lock held): to the builder
+    // for destruction now if idle, else when its last user releases it.
     void retire_locked(std::unordered_map<uint64_t, CacheEntry>::iterator it) {
         cache_bytes -= it->second.bytes;
         if (it->second.users == 0) {
-            dg_plan *p = it->second.plan;
-            cache.erase(it);
-            dg_plan_destroy(p);  // not in use by any worker
-            return;
+            to_destroy.push_back(it->second.plan);
+            cv_build.notify_one();
+        } else {
+            retired.push_back(it->second);
         }
-        retired.push_back(it->second);
         cache.erase(it);
     }
 
     void release(uint64_t key, dg_plan *plan) {
-        dg_plan *dead = nullptr;
-        {
-            std::unique_lock<std::mutex> lock(mu);
-            auto it = cache.find(key);
-            if (it != cache.end() && it->second.plan == plan) {
-                if (it->second.users > 0) it->second.users--;
-            } else {
-                for (size_t i = 0; i < retired.size(); ++i)
-                    if (retired[i].plan == plan) {
-                        if (--retired[i].users == 0) {
-                            dead = plan;
-                            retired.erase(retired.begin() + long(i));
-                        }
-                        break;
-                    }
-            }
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end() && it->second.plan == plan) {
+            if (it->second.users > 0) it->second.users--;
+            return;
         }
-        if (dead) dg_plan_destroy(dead);
+        for (size_t i = 0; i < retired.size(); ++i)
+            if (retired[i].plan == plan) {
+                if (--retired[i].users == 0) {
+                    to_destroy.push_back(plan);
+                    retired.erase(retired.begin() + long(i));
+                    cv_build.notify_one();
+                }
+                return;
+            }
+    }
+
+    // Builds, tunes and admits plans, and destroys the ones the cache let go:
+    // every device allocation and free of a plan happens on this thread, so
+    // the workers' streams never wait for a build or an eviction.
+    void builder_main() {
+        cudaSetDevice(cfg.device);
+        for (;;) {
+            std::vector<dg_plan *> dead;
+            uint64_t key = 0;
+            bool have = false;
+            PlanSpec spec;
+            std::pair<int32_t, uint32_t> hint{DG_U32, 0};
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                cv_build.wait(lock, [&] {
+                    return stop || !build_queue.empty() || !to_destroy.empty();
+                });
+                dead.swap(to_destroy);
+                if (!build_queue.empty() && !stop) {
+                    key = build_queue.front();
+                    build_queue.pop_front();
+                    spec = specs.at(key);
+                    hint = build_pending.at(key);
+                    have = true;
+                }
+                if (!have && stop && dead.empty()) break;
+            }
+            for (dg_plan *p : dead) dg_plan_destroy(p);
+            if (!have) continue;
+            const auto t_build = Clock::now();
+            dg_plan *plan = nullptr;
+            dg_status st = dg_plan_create(&spec.geometry, &spec.method,
+                                          spec.mask.empty() ? nullptr : spec.mask.data(),
+                                          spec.dim1, spec.dim2, spec.n_radial, spec.n_azimuthal,
+                                          spec.has_az_range ? spec.az_range : nullptr, &plan);
+            if (st != DG_OK) {
+                const std::string msg = last_error_text();
+                {
+                    std::lock_guard<std::mutex> lock(mu);
+                    failed[key] = {spec.generation, st, msg};
+                    build_pending.erase(key);
+                }
+                cv_work.notify_all();
+                continue;
+            }
+            // A rebuilt key (new PONI, same shape and bins) keeps the mapping
+            // its previous plan was tuned to; a new key is tuned once.
+            int32_t known = -1;
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                auto t = tuned.find(key);
+                if (t != tuned.end()) known = t->second;
+            }
+            if (known < 0 || dg_plan_variant(plan, known, nullptr, nullptr) != DG_OK) {
+                tune(plan, hint.first, hint.second);
+                int32_t v = 0;
+                dg_plan_variant(plan, -1, &v, nullptr);
+                std::lock_guard<std::mutex> lock(mu);
+                tuned[key] = v;
+            }
+            // Partial sums for the largest coalesced launch, allocated now
+            // rather than by a worker's first batch (the work-queue gather
+            // sums every plan with partial sums).
+            {
+                std::lock_guard<std::mutex> lock(plan->mu);
+                cudaSetDevice(plan->device);
+                try {
+                    dg::reserve_partials(plan->gather, cfg.max_coalesce, hint.second, hint.first,
+                                         cfg.max_coalesce > 1);
+                } catch (const dg::Error &) {
+                }
+            }
+            dg_plan_info info{};
+            dg_plan_query(plan, &info);
+            std::vector<dg_plan *> evicted;
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                build_pending.erase(key);
+                stats.build_us += int64_t(
+                    std::chrono::duration<double, std::micro>(Clock::now() - t_build).count());
+                if (specs.at(key).generation != spec.generation) {
+                    evicted.push_back(plan);  // re-registered while building
+                } else {
+                    auto old = cache.find(key);
+                    if (old != cache.end()) retire_locked(old);
+                    stats.plan_builds++;
+                    // Admission by memory: evict idle plans, oldest first.
+                    while (cache_bytes + info.device_bytes > cfg.cache_bytes) {
+                        uint64_t victim = 0, oldest = UINT64_MAX;
+                        for (auto &kv : cache)
+                            if (kv.second.users == 0 && kv.second.last_use < oldest) {
+                                oldest = kv.second.last_use;
+                                victim = kv.first;
+                            }
+                        if (oldest == UINT64_MAX) break;  // everything busy: over budget briefly
+                        cache_bytes -= cache[victim].bytes;
+                        evicted.push_back(cache[victim].plan);
+                        cache.erase(victim);
+                        stats.plan_evictions++;
+                    }
+                    CacheEntry e;
+                    e.plan = plan;
+                    e.bytes = info.device_bytes;
+                    e.last_use = ++use_clock;
+                    e.generation = spec.generation;
+                    cache[key] = e;
+                    cache_bytes += e.bytes;
+                }
+            }
+            cv_work.notify_all();
+            for (dg_plan *p : evicted) dg_plan_destroy(p);
+        }
+    }
+
+    // Finishes a request (lock held; notify after).
+    void finish_locked(Request *r, dg_status st, const std::string &err) {
+        r->status = st;
+        r->error = err;
+        r->done = true;
+        r->latency_us = std::chrono::duration<double, std::micro>(Clock::now() - r->submitted).count();
+        if (st == DG_OK) stats.completed++;
+        else stats.failed++;
+        if (!r->borrowed) pinned.put(r->frame_bytes, r->frame);
+        r->frame = nullptr;
+        inflight--;
+    }
+
+    // One batch of a worker: up to max_coalesce queued requests of each of up
+    // to kPlansPerLaunch built plans, all of one dtype and one set of flags.
+    struct Group {
+        uint64_t key = 0;
+        dg_plan *plan = nullptr;
+        std::vector<Request *> reqs;
+        size_t in_off = 0, out_off = 0;
+    };
+    static constexpr int kPlansPerLaunch = 8;
+
+    // The cached plan of `key` if it is built for the current generation,
+    // with a user reference taken (lock held).
+    dg_plan *take_ready_locked(uint64_t key) {
+        auto c = cache.find(key);
+        if (c == cache.end() || c->second.generation != specs.at(key).generation) return nullptr;
+        c->second.users++;
+        c->second.last_use = ++use_clock;
+        stats.plan_hits++;
+        return c->second.plan;
     }
 
     void worker_main() {
         cudaSetDevice(cfg.device);
         cudaStream_t stream = nullptr;
         cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+        // Coalescing batches run through the work-queue gather: all their
+        // plans in one graph launch, every plan summed with the same lane
+        // mapping, so a request's result does not depend on its company.
+        // max_coalesce 1 is the plain path: one request per launch on the
+        // plan's own tuned mapping.
+        const bool plain = cfg.max_coalesce <= 1;
+        dg_multi *multi = nullptr;
+        if (!plain && dg_multi_create(cfg.device, kPlansPerLaunch, &multi) != DG_OK) multi = nullptr;
         unsigned char *d_in = nullptr;
         double *d_out = nullptr, *h_out = nullptr;
         size_t in_cap = 0, out_cap = 0;
         for (;;) {
-            std::vector<Request *> batch;
+            std::vector<Group> groups;
+            bool failed_some = false;
             {
                 std::unique_lock<std::mutex> lock(mu);
                 cv_work.wait_for(lock, std::chrono::microseconds(std::max(cfg.poll_us, 50)),
                                  [&] { return stop || !queue.empty(); });
                 if (stop && queue.empty()) break;
-                if (queue.empty()) continue;
-                // the oldest request whose plan no other worker is building
-                auto hit = queue.begin();
-                while (hit != queue.end() && building.count((*hit)->key)) ++hit;
-                if (hit == queue.end()) {
-                    lock.unlock();
-                    std::this_thread::sleep_for(std::chrono::microseconds(200));
-                    continue;
-                }
-                Request *head = *hit;
-                queue.erase(hit);
-                batch.push_back(head);
-                for (auto it = queue.begin(); it != queue.end() &&
-                                              int(batch.size()) < cfg.max_coalesce;) {
+                // The oldest request whose plan is built heads the batch;
+                // requests of plans not built yet ask the builder and wait in
+                // the queue; requests whose build failed fail.
+                auto it = queue.begin();
+                while (it != queue.end()) {
                     Request *r = *it;
-                    if (r->key == head->key && r->dtype == head->dtype && r->flags == head->flags) {
-                        batch.push_back(r);
+                    if (dg_plan *p = take_ready_locked(r->key)) {
+                        Group g;
+                        g.key = r->key;
+                        g.plan = p;
+                        g.reqs.push_back(r);
+                        groups.push_back(std::move(g));
                         it = queue.erase(it);
-                    } else {
-                        ++it;
+                        break;
                     }
+                    auto f = failed.find(r->key);
+                    if (f != failed.end() && f->second.generation == specs.at(r->key).generation) {
+                        finish_locked(r, f->second.status, f->second.message);
+                        failed_some = true;
+                        it = queue.erase(it);
+                        continue;
+                    }
+                    request_build_locked(r->key, r->dtype, r->flags);
+                    ++it;
                 }
-            }
-            Request *head = batch.front();
-            std::string err;
-            dg_status st = DG_OK;
-            dg_plan *plan = acquire(head->key, head->dtype, head->flags, err, st);
-            if (plan) {
-                const size_t fb = head->frame_bytes;
-                const int64_t nb = plan->n_bins;
-                const int nout = 1 + ((head->flags & DG_ERRORS) ? 1 : 0) +
-                                 ((head->flags & DG_AZIMUTHAL_STD) ? 1 : 0);
-                const size_t nf = batch.size();
-                if (in_cap < nf * fb) {
-                    if (d_in) cudaFree(d_in);
-                    in_cap = nf * fb;
-                    if (cudaMalloc(&d_in, in_cap) != cudaSuccess) {
-                        (void)cudaGetLastError();
-                        d_in = nullptr;
-                        in_cap = 0;
-                    }
-                }
-                if (out_cap < nf * size_t(nb) * nout) {
-                    if (d_out) cudaFree(d_out);
-                    if (h_out) cudaFreeHost(h_out);
-                    out_cap = nf * size_t(nb) * nout;
-                    if (cudaMalloc(&d_out, out_cap * 8) != cudaSuccess ||
-                        cudaMallocHost(&h_out, out_cap * 8) != cudaSuccess) {
-                        (void)cudaGetLastError();
-                        d_out = nullptr;
-                        h_out = nullptr;
-                        out_cap = 0;
-                    }
-                }
-                const auto t_batch = Clock::now();
-                if (!d_in || !d_out) {
-                    st = DG_DEVICE;
-                    err = "request loop staging allocation failed";
-                } else {
-                    for (size_t i = 0; i < nf; ++i)
-                        cudaMemcpyAsync(d_in + i * fb, batch[i]->frame, fb, cudaMemcpyHostToDevice,
-                                        stream);
-                    double *di = d_out, *ds = nullptr, *dd = nullptr;
-                    int k = 1;
-                    if (head->flags & DG_ERRORS) ds = d_out + nf * nb * k++;
-                    if (head->flags & DG_AZIMUTHAL_STD) dd = d_out + nf * nb * k++;
-                    st = dg_integrate_device(plan, d_in, head->dtype, int64_t(nf), head->flags, di,
-                                             ds, dd, stream);
-                    if (st != DG_OK) err = last_error_text();
-                    cudaMemcpyAsync(h_out, d_out, nf * nb * nout * 8, cudaMemcpyDeviceToHost,
-                                    stream);
-                    if (cudaStreamSynchronize(stream) != cudaSuccess && st == DG_OK) {
-                        st = DG_DEVICE;
-                        err = cudaGetErrorString(cudaGetLastError());
-                    }
-                    if (st == DG_OK && dg::bin_tile_wait_failed(plan->gather)) {
-                        st = DG_TIMEOUT;
-                        err = "bin-tile gather: a chunk-pipeline wait gave up after 1 s";
-                    }
-                    if (st == DG_OK) {
-                        for (size_t i = 0; i < nf; ++i) {
-                            Request *r = batch[i];
-                            int kk = 0;
-                            r->out_i.assign(h_out + i * nb, h_out + (i + 1) * nb);
-                            ++kk;
-                            if (ds) {
-                                r->out_s.assign(h_out + (kk * nf + i) * nb,
-                                                h_out + (kk * nf + i + 1) * nb);
-                                ++kk;
+                if (!groups.empty()) {
+                    // the requests behind it: its plan's, then other built plans'
+                    const Request *head = groups.front().reqs.front();
+                    for (it = queue.begin(); it != queue.end();) {
+                        Request *r = *it;
+                        if (r->dtype != head->dtype || r->flags != head->flags) {
+                            ++it;
+                            continue;
+                        }
+                        Group *g = nullptr;
+                        for (auto &x : groups)
+                            if (x.key == r->key) g = &x;
+                        if (!g && !plain && int(groups.size()) < kPlansPerLaunch) {
+                            if (dg_plan *p = take_ready_locked(r->key)) {
+                                groups.emplace_back();
+                                g = &groups.back();
+                                g->key = r->key;
+                                g->plan = p;
                             }
-                            if (dd)
-                                r->out_d.assign(h_out + (kk * nf + i) * nb,
-                                                h_out + (kk * nf + i + 1) * nb);
+                        }
+                        if (g && int(g->reqs.size()) < cfg.max_coalesce) {
+                            g->reqs.push_back(r);
+                            it = queue.erase(it);
+                        } else {
+                            ++it;
                         }
                     }
                 }
-                release(head->key, plan);
+            }
+            if (failed_some) {
+                cv_done.notify_all();
+                cv_slot.notify_all();
+            }
+            if (groups.empty()) continue;
+            const Request *head = groups.front().reqs.front();
+            const int nout = 1 + ((head->flags & DG_ERRORS) ? 1 : 0) +
+                             ((head->flags & DG_AZIMUTHAL_STD) ? 1 : 0);
+            size_t in_need = 0, out_need = 0, n_frames = 0;
+            for (auto &g : groups) {
+                g.in_off = in_need;
+                g.out_off = out_need;
+                in_need += g.reqs.size() * g.reqs.front()->frame_bytes;
+                out_need += g.reqs.size() * size_t(g.plan->n_bins) * nout;
+                n_frames += g.reqs.size();
+            }
+            std::string err;
+            dg_status st = DG_OK;
+            // Staging grows by doubling, stream-ordered on this worker's own
+            // stream (no device-wide synchronisation), and is kept.
+            if (in_cap < in_need) {
+                if (d_in) cudaFreeAsync(d_in, stream);
+                in_cap = std::max(in_need, 2 * in_cap);
+                if (cudaMallocAsync(reinterpret_cast<void **>(&d_in), in_cap, stream) != cudaSuccess) {
+                    (void)cudaGetLastError();
+                    d_in = nullptr;
+                    in_cap = 0;
+                }
+            }
+            if (out_cap < out_need) {
+                if (d_out) cudaFreeAsync(d_out, stream);
+                pinned.put(out_cap * 8, h_out);
+                out_cap = std::max(out_need, 2 * out_cap);
+                h_out = static_cast<double *>(pinned.get(out_cap * 8));
+                if (cudaMallocAsync(reinterpret_cast<void **>(&d_out), out_cap * 8, stream) !=
+                        cudaSuccess || !h_out) {
+                    (void)cudaGetLastError();
+                    d_out = nullptr;
+                    out_cap = 0;
+                }
+            }
+            const auto t_batch = Clock::now();
+            if (!d_in || !d_out || (!plain && !multi)) {
+                st = DG_DEVICE;
+                err = "request loop staging allocation failed";
+            } else {
+                std::vector<dg_multi_item> items;
+                for (auto &g : groups) {
+                    const size_t fb = g.reqs.front()->frame_bytes, nf = g.reqs.size();
+                    const size_t nb = size_t(g.plan->n_bins);
+                    for (size_t i = 0; i < nf; ++i)
+                        cudaMemcpyAsync(d_in + g.in_off + i * fb, g.reqs[i]->frame, fb,
+                                        cudaMemcpyHostToDevice, stream);
+                    dg_multi_item m{};
+                    m.plan = g.plan;
+                    m.d_frames = d_in + g.in_off;
+                    m.n_frames = int64_t(nf);
+                    double *o = d_out + g.out_off;
+                    int k = 0;
+                    m.d_intensity = o + nf * nb * k++;
+                    if (head->flags & DG_ERRORS) m.d_sigma = o + nf * nb * k++;
+                    if (head->flags & DG_AZIMUTHAL_STD) m.d_std = o + nf * nb * k++;
+                    items.push_back(m);
+                }
+                if (plain) {
+                    const dg_multi_item &m = items.front();
+                    st = dg_integrate_device(m.plan, m.d_frames, head->dtype, m.n_frames,
+                                             head->flags, m.d_intensity, m.d_sigma, m.d_std,
+                                             stream);
+                } else {
+                    st = dg_multi_integrate(multi, items.data(), int32_t(items.size()),
+                                            head->dtype, head->flags, stream);
+                }
+                if (st != DG_OK) err = last_error_text();
+                cudaMemcpyAsync(h_out, d_out, out_need * 8, cudaMemcpyDeviceToHost, stream);
+                if (cudaStreamSynchronize(stream) != cudaSuccess && st == DG_OK) {
+                    st = DG_DEVICE;
+                    err = cudaGetErrorString(cudaGetLastError());
+                }
+                for (auto &g : groups)
+                    if (st == DG_OK && dg::bin_tile_wait_failed(g.plan->gather)) {
+                        st = DG_TIMEOUT;
+                        err = "bin-tile gather: a chunk-pipeline wait gave up after 1 s";
+                    }
+                if (st == DG_OK) {
+                    for (auto &g : groups) {
+                        const size_t nf = g.reqs.size(), nb = size_t(g.plan->n_bins);
+                        const double *o = h_out + g.out_off;
+                        for (size_t i = 0; i < nf; ++i) {
+                            Request *r = g.reqs[i];
+                            int kk = 0;
+                            r->out_i.assign(o + i * nb, o + (i + 1) * nb);
+                            ++kk;
+                            if (head->flags & DG_ERRORS) {
+                                r->out_s.assign(o + (kk * nf + i) * nb, o + (kk * nf + i + 1) * nb);
+                                ++kk;
+                            }
+                            if (head->flags & DG_AZIMUTHAL_STD)
+                                r->out_d.assign(o + (kk * nf + i) * nb, o + (kk * nf + i + 1) * nb);
+                        }
+                    }
+                }
+            }
+            for (auto &g : groups) release(g.key, g.plan);
+            {
                 std::lock_guard<std::mutex> lock(mu);
                 stats.batch_us += int64_t(
                     std::chrono::duration<double, std::micro>(Clock::now() - t_batch).count());
-            }
-            {
-                std::unique_lock<std::mutex> lock(mu);
-                auto now = Clock::now();
                 stats.launches++;
-                if (batch.size() > 1) stats.coalesced_frames += int64_t(batch.size());
-                for (Request *r : batch) {
-                    r->status = st;
-                    r->error = err;
-                    r->done = true;
-                    r->latency_us =
-                        std::chrono::duration<double, std::micro>(now - r->submitted).count();
-                    if (st == DG_OK) stats.completed++;
-                    else stats.failed++;
-                    if (!r->borrowed) pinned.put(r->frame_bytes, r->frame);
-                    r->frame = nullptr;
-                    inflight--;
-                }
+                if (n_frames > 1) stats.coalesced_frames += int64_t(n_frames);
+                for (auto &g : groups)
+                    for (Request *r : g.reqs) finish_locked(r, st, err);
             }
             cv_done.notify_all();
             cv_slot.notify_all();
         }
-        if (d_in) cudaFree(d_in);
-        if (d_out) cudaFree(d_out);
-        if (h_out) cudaFreeHost(h_out);
-        if (stream) cudaStreamDestroy(stream);
+        if (d_in) cudaFreeAsync(d_in, stream);
+        if (d_out) cudaFreeAsync(d_out, stream);
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+        if (multi) dg_multi_destroy(multi);
+        pinned.put(out_cap * 8, h_out);
     }
 };
 
@@ -448,6 +581,7 @@ dg_status dg_server_create(const dg_server_config *config, dg_server **out) {
     auto s = std::make_unique<dg_server>();
     s->cfg = *config;
     for (int i = 0; i < 4; ++i) s->workers.emplace_back([p = s.get()] { p->worker_main(); });
+    s->builder = std::thread([p = s.get()] { p->builder_main(); });
     *out = s.release();
     return DG_OK;
 }
@@ -459,7 +593,10 @@ dg_status dg_server_destroy(dg_server *server) {
         server->stop = true;
     }
     server->cv_work.notify_all();
+    server->cv_build.notify_all();
     for (auto &t : server->workers) t.join();
+    server->builder.join();
+    for (dg_plan *p : server->to_destroy) dg_plan_destroy(p);
     for (auto &kv : server->cache) dg_plan_destroy(kv.second.plan);
     for (auto &e : server->retired) dg_plan_destroy(e.plan);
     for (auto &kv : server->requests)
@@ -494,6 +631,7 @@ dg_status dg_server_register(dg_server *server, uint64_t key, const dg_geometry 
         // cached plan is retired (now, or when its users finish).
         spec.generation = server->next_generation++;
         server->specs[key] = std::move(spec);
+        server->failed.erase(key);
         auto it = server->cache.find(key);
         if (it != server->cache.end()) server->retire_locked(it);
     }

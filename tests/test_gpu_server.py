@@ -123,3 +123,67 @@ def test_reregistered_plan_is_rebuilt(dg):
     np.testing.assert_allclose(b, ref, rtol=1e-5)  # the loop's plan has its own mapping
     assert not np.array_equal(a, b)
     loop.close()
+
+
+def test_plan_cache_evicts_by_memory_and_rebuilds_evicted_plans(dg):
+    # Three plans of a few MB each under a byte budget that holds two: the
+    # builder evicts the least recently used idle plan to admit a new one, an
+    # evicted plan is rebuilt on its next request, and every result equals
+    # the first one for the same frame.
+    poni = dict(pixel1=1e-4, pixel2=1e-4, distance=0.05, poni1=0.0103, poni2=0.0124,
+                rot1=0.01, wavelength=1e-10)
+    shape = (200, 240)
+    its = [dg.Integrator.from_poni_dict(dict(poni, distance=0.05 + 0.0005 * k),
+                                        method="pixel_split") for k in range(3)]
+    probe = dg.RequestLoop(max_coalesce=4)  # plan bytes include its partial sums
+    probe.register(0, its[0], shape, 300)
+    frame = np.random.default_rng(9).poisson(80.0, shape).astype(np.uint32)
+    probe.poll(probe.submit(0, frame, errors=True), 0, errors=True)
+    one = probe.stats()["cache_bytes"]
+    probe.close()
+    assert one > 0
+    loop = dg.RequestLoop(cache_bytes=int(2.5 * one), max_coalesce=4)
+    for k in range(3):
+        loop.register(k, its[k], shape, 300)
+    first = {}
+    for rnd in range(3):
+        for k in range(3):  # round robin over 3 plans: each request misses
+            got = loop.poll(loop.submit(k, frame, errors=True), k, errors=True)
+            if rnd == 0:
+                first[k] = got
+            else:
+                for a, b in zip(got[:2], first[k][:2]):
+                    assert np.array_equal(a, b)
+    st = loop.stats()
+    assert st["completed"] == 9 and st["failed"] == 0
+    assert st["plan_builds"] == 9 and st["plan_evictions"] >= 7
+    assert st["cache_bytes"] <= 2.5 * one
+    for k in range(3):
+        ref = its[k].integrate1d(frame, 300, True)
+        np.testing.assert_allclose(first[k][0], ref.intensity_array, rtol=1e-5)
+    loop.close()
+
+
+def test_a_plan_that_fails_to_build_fails_its_requests_only(dg):
+    loop = dg.RequestLoop()
+    good = dg.Integrator.from_poni_dict(dict(pixel1=1e-4, pixel2=1e-4, distance=0.05,
+                                             poni1=0.003, poni2=0.004, wavelength=1e-10),
+                                        method="pixel_split")
+    # q units need a wavelength; the Integrator checks it when the unit is
+    # set, so the wavelength is cleared afterwards and the device build
+    # rejects the configuration (check_configuration, cuda.rs:1001-1057)
+    bad = dg.Integrator.from_poni_dict(dict(pixel1=1e-4, pixel2=1e-4, distance=0.05,
+                                            poni1=0.003, poni2=0.004, wavelength=1e-10),
+                                       method="pixel_split", unit="q_nm^-1")
+    bad.poni.wavelength = 0.0
+    loop.register(1, good, (40, 50), 30)
+    loop.register(2, bad, (40, 50), 30)
+    frame = np.ones((40, 50), np.float32)
+    t_bad = loop.submit(2, frame)
+    t_good = loop.submit(1, frame)
+    assert np.isfinite(loop.poll(t_good, 1)[0]).all()
+    with pytest.raises(ValueError, match="[Ww]avelength"):
+        loop.poll(t_bad, 2)
+    st = loop.stats()
+    assert st["completed"] == 1 and st["failed"] == 1
+    loop.close()

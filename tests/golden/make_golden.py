@@ -1,8 +1,6 @@
-"""Regenerates the committed golden fixtures from the reference checkout.
+"""Regenerates the committed golden fixtures from a reference checkout.
 
-Run here, where the reference tree is mounted read-only:
-
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 
 It copies the reference's own pyFAI-derived geometry vectors
 (test_data/test_reference/*_pyFAI.txt, for test_data/v1.poni on a 10 x 20
@@ -44,4 +42,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

@@ -1047,7 +1047,7 @@ __global__ void __launch_bounds__(256)
 // chunk do not). Every wait is bounded (kBtWaitNs); a warp that gives up
 // ends the tile and sets a flag in mapped host memory that the host reports
 // as DG_TIMEOUT. Warp w owns row w of the tile and keeps its sums in
-// registers for the whole tile (double-word FP32, folded every kFlFlushPairs
+// registers for the whole tile (double-word FP32, folded every kBtFoldPairs
 // pairs of the row), then normalises and writes the results itself: no
 // partial sums, no finalize launch. Every row is summed in the same order for
 // every frame and batch.
@@ -1150,6 +1150,12 @@ struct BtCfg {
 #ifndef DG_BT_LARGEST_FIRST
 #define DG_BT_LARGEST_FIRST 1
 #endif
+// Pairs of a row summed in plain FP32 (each half of a packed accumulator
+// takes one entry per pair) before they are folded into the double-word sums.
+#ifndef DG_BT_FOLD_PAIRS
+#define DG_BT_FOLD_PAIRS 16
+#endif
+constexpr int kBtFoldPairs = DG_BT_FOLD_PAIRS;
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
 using Bt8 = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, 2, (DG_BT8_ROWS > 16 ? 2 : 4),
                   DG_BT8_BUFS, DG_BT8_AHEAD>;  // mapping 8
@@ -1572,14 +1578,14 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         for (; p + U2 <= p1; p += U2) {
             body(p, std::integral_constant<int, U2>{});
             since += U2;
-            if (since >= kFlFlushPairs) {
+            if (since >= kBtFoldPairs) {
                 since = 0;
                 fold();
             }
         }
         for (; p < p1; ++p) {
             body(p, std::integral_constant<int, 1>{});
-            if (++since >= kFlFlushPairs) {
+            if (++since >= kBtFoldPairs) {
                 since = 0;
                 fold();
             }

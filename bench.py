@@ -378,6 +378,93 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def reference_gpu_leg(w, plan, frames, stream, peak, reps: int = 5) -> dict:
+    """The reference's own CUDA gather (src/integration/cuda/kernels.cu,
+    compensated FP32), compiled from its source for sm_100a
+    (baseline/Makefile) and launched with its engine's layout rule and 256
+    frames per launch, on the same resident frames and the plan's masked
+    table in the reference's upload formats (u32 rows and columns, f32
+    weights, f64 denominators). It computes I and sigma (the reference's
+    spread has no GPU path), so its rate is set beside this build's
+    errors-only launch on the same frames; the results are compared."""
+    import numpy as np
+    import torch
+    from dioptrin_b200 import _native as N
+    path = os.path.join(ROOT, "baseline", "_ref", "libref_gather.so")
+    if not os.path.exists(path):
+        return {"unavailable": "baseline/_ref/libref_gather.so not built "
+                               "(make -C baseline REF=<reference checkout>)"}
+    R = C.CDLL(path)
+    R.ref_gather_layout.restype = C.c_char_p
+    R.ref_gather_layout.argtypes = [C.c_int64, C.c_int64, C.c_int]
+    R.ref_gather_launch.argtypes = [C.c_int, C.c_char_p, C.c_int] + [C.c_void_p] * 6 + \
+        [C.c_uint, C.c_uint, C.c_uint, C.c_void_p]
+    code = {"uint16": 0, "uint32": 1, "int32": 2, "float32": 3}.get(w.dtype)
+    if code is None:
+        return {"unavailable": f"the reference has no {w.dtype} CSR kernel"}
+    rp, col, wt, den = plan.export_table(0)
+    nb = len(den)
+    dev = frames.device
+    rows = torch.from_numpy(rp.astype(np.uint32)).to(dev)
+    cols = torch.from_numpy(col.astype(np.uint32)).to(dev)
+    wts = torch.from_numpy(wt.astype(np.float32)).to(dev)
+    dens = torch.from_numpy(den.astype(np.float64)).to(dev)
+    n = frames.shape[0]
+    out = torch.empty((n, nb, 2), dtype=torch.float64, device=dev)
+    layout = R.ref_gather_layout(len(col), nb, 1 if w.n_azimuthal else 0)
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def launch():
+        rc = R.ref_gather_launch(code, layout, 1, rows.data_ptr(), cols.data_ptr(),
+                                 wts.data_ptr(), dens.data_ptr(), frames.data_ptr(),
+                                 out.data_ptr(), w.dim1 * w.dim2, nb, n, sp)
+        if rc:
+            raise RuntimeError(f"reference gather launch failed: cudaError {rc}")
+
+    launch()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    # this build's errors-only integration of the same frames
+    oi = torch.empty((n, nb), dtype=torch.float64, device=dev)
+    os_ = torch.empty_like(oi)
+    L = N.lib()
+    dcode = {"uint16": 0, "uint32": 1, "int32": 2, "float32": 3, "float64": 4}[w.dtype]
+    N.check(L.dg_integrate_device(plan.handle, C.c_void_p(frames.data_ptr()), dcode, n,
+                                  N.DG_ERRORS, C.c_void_p(oi.data_ptr()),
+                                  C.c_void_p(os_.data_ptr()), None, sp))
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(reps):
+        N.check(L.dg_integrate_device(plan.handle, C.c_void_p(frames.data_ptr()), dcode, n,
+                                      N.DG_ERRORS, C.c_void_p(oi.data_ptr()),
+                                      C.c_void_p(os_.data_ptr()), None, sp))
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ours_ms = t0.elapsed_time(t1) / reps
+    ri, rs = out[..., 0], out[..., 1]
+    nz = ri != 0
+    rel = ((oi - ri).abs()[nz] / ri.abs()[nz]).max().item() if bool(nz.any()) else 0.0
+    alg = len(col) * 8 + (nb + 1) * 4 + nb * 8 + n * w.dim1 * w.dim2 * frames.element_size() + \
+        n * nb * 2 * 8
+    return {"kernel": f"{['u16_', 'u32_', 'i32_', ''][code]}compensated_{layout.decode()}_iv",
+            "layout": layout.decode(), "frames": n, "value": round(n / (ms / 1000), 2),
+            "unit": "frames/s", "ms_per_call": round(ms, 4),
+            "achieved_gbs": round(alg / (ms / 1000) / 1e9, 1),
+            "frac": round(alg / (ms / 1000) / 1e9 / peak, 4),
+            "ours_errors_only": {"value": round(n / (ours_ms / 1000), 2), "unit": "frames/s",
+                                 "ms_per_call": round(ours_ms, 4),
+                                 "gather_variant": plan.gather_variant},
+            "max_rel_diff_intensity": rel,
+            "build": "baseline/Makefile: the reference's kernels.cu, nvcc sm_100a --fmad=false"}
+
+
 def masked_legs(w, plan, frames, stream, peak, reps: int = 3) -> dict:
     """Device-resident frames through the per-frame-mask gather
     (dg_integrate_dynamic_device: a uint8 mask per frame, denominators summed
@@ -675,6 +762,7 @@ def main():
         plan.gather_variant = batch_variant
         if not w.n_azimuthal:
             line.update(masked_legs(w, plan, frames, stream, peak))
+        line["reference_gpu_kernel"] = reference_gpu_leg(w, plan, frames, stream, peak)
         # end to end through the public host API: pinned host frames in,
         # results back, every step
         host = torch.empty(frames.shape, dtype=frames.dtype, pin_memory=True)

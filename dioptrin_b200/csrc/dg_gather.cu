@@ -1146,6 +1146,11 @@ struct BtCfg {
 #ifndef DG_BT_DEFER_PX
 #define DG_BT_DEFER_PX 1
 #endif
+// With two frames per lane, the lane's two frames stored side by side in
+// shared memory (1: one 8-byte load per slot) or in separate frame rows (0).
+#ifndef DG_BT_PAIRED
+#define DG_BT_PAIRED 0
+#endif
 // Bin tiles run largest first (1) or in bin order (0).
 #ifndef DG_BT_LARGEST_FIRST
 #define DG_BT_LARGEST_FIRST 1
@@ -1153,7 +1158,7 @@ struct BtCfg {
 // Pairs of a row summed in plain FP32 (each half of a packed accumulator
 // takes one entry per pair) before they are folded into the double-word sums.
 #ifndef DG_BT_FOLD_PAIRS
-#define DG_BT_FOLD_PAIRS 16
+#define DG_BT_FOLD_PAIRS 32
 #endif
 constexpr int kBtFoldPairs = DG_BT_FOLD_PAIRS;
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
@@ -1260,6 +1265,14 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     const bool signal = !(withhold && blockIdx.x == 0 && warp == 0);
 
     auto pxbuf = [&](int b) { return reinterpret_cast<S *>(smem + size_t(b) * BUF); };
+    // Staged pixel of (local frame f, slot k). With two frames per lane the
+    // lane's frames l and l + 32 can sit side by side (PAIRED: one 8-byte
+    // shared load reads a slot for both; rows of 2 * STRIDE words, STRIDE odd,
+    // so the 16 lanes of a half-warp hit 16 distinct bank pairs).
+    constexpr bool PAIRED = DG_BT_PAIRED && F2 == 2 && MODE != kRaw;
+    auto pxi = [&](int f, int k) {
+        return PAIRED ? (f & 31) * 2 * STRIDE + 2 * k + (f >> 5) : f * STRIDE + k;
+    };
     auto pabuf = [&](int b) {
         return reinterpret_cast<float4 *>(smem + size_t(b) * BUF +
                                           size_t(CFG::kFrames) * STRIDE * 4);
@@ -1288,7 +1301,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     }
     // Column DCAP of every frame row is read by padding pairs and holds 0.
     for (int j = tid; j < NB * CFG::kFrames; j += NT) {
-        pxbuf(j / CFG::kFrames)[(j % CFG::kFrames) * STRIDE + DCAP] = S(0);
+        pxbuf(j / CFG::kFrames)[pxi(j % CFG::kFrames, DCAP)] = S(0);
         if constexpr (MODE == kRaw) mkbuf(j / CFG::kFrames)[(j % CFG::kFrames) * MS + DCAP] = 0;
     }
     __syncthreads();
@@ -1323,7 +1336,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
         const int per = (ch.y + KS - 1) / KS, s0 = (warp % KS) * per;
         const int k1 = min(ch.y, s0 + per), fw = warp / KS;
-        S *dst = pxbuf(b) + fw * STRIDE;
+        S *dst = pxbuf(b);
         const P *base = frames + int64_t(f0 + fw) * n_pixels;
         if constexpr (MODE == kRaw) {
 #pragma unroll
@@ -1355,9 +1368,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 for (int j = 0; j < FS; ++j) {
                     if (fw + j * FSTEP >= nv) break;
                     if constexpr (sizeof(P) == 4)
-                        cp_async4(dst + j * FSTEP * STRIDE + k, src + int64_t(j * FSTEP) * n_pixels);
+                        cp_async4(dst + pxi(fw + j * FSTEP, k), src + int64_t(j * FSTEP) * n_pixels);
                     else
-                        dst[j * FSTEP * STRIDE + k] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
+                        dst[pxi(fw + j * FSTEP, k)] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
                 }
             }
         }
@@ -1377,13 +1390,13 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             const int dn = mbuf(c)[0];
             const int per = (dn + KS - 1) / KS, s0 = (warp % KS) * per;
             const int k1 = min(dn, s0 + per), fw = warp / KS;
-            S *dst = pxbuf(b) + fw * STRIDE;
+            S *dst = pxbuf(b);
 #pragma unroll
             for (int i = 0; i < KSTEP; ++i) {
                 const int k = s0 + lane + 32 * i;
 #pragma unroll
                 for (int j = 0; j < FS; ++j)
-                    if (k < k1 && fw + j * FSTEP < nv) dst[j * FSTEP * STRIDE + k] = pv[i][j];
+                    if (k < k1 && fw + j * FSTEP < nv) dst[pxi(fw + j * FSTEP, k)] = pv[i][j];
             }
         }
         if constexpr (MODE == kRaw) {
@@ -1480,7 +1493,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
         }
         const S *px[F2];
 #pragma unroll
-        for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + (lane + 32 * h) * STRIDE;
+        for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + pxi(lane + 32 * h, 0);
         const float4 *s_pa = pabuf(b);
         const float4 *s_pb = s_pa + PCAP;
         const f2 *s_pc = pcbuf(b);
@@ -1499,14 +1512,34 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 if constexpr (WIDE) eb[u] = s_pb[p + u];
                 if constexpr (SPREAD) ec[u] = s_pc[p + u];
             }
-#pragma unroll
-            for (int h = 0; h < F2; ++h) {
-                float v0[UU], v1[UU];
+            // the pair's pixels for this lane's frames
+            float vv0[F2][UU], vv1[F2][UU];
+            if constexpr (PAIRED) {
 #pragma unroll
                 for (int u = 0; u < UU; ++u) {
-                    v0[u] = float(px[h][__float_as_int(ea[u].x)]);
-                    v1[u] = float(px[h][__float_as_int(ea[u].y)]);
+                    using S2 = typename std::conditional<std::is_same<S, float>::value, float2,
+                               typename std::conditional<std::is_same<S, int32_t>::value, int2,
+                                                         uint2>::type>::type;
+                    const S2 a = *reinterpret_cast<const S2 *>(px[0] + 2 * __float_as_int(ea[u].x));
+                    const S2 b2 = *reinterpret_cast<const S2 *>(px[0] + 2 * __float_as_int(ea[u].y));
+                    vv0[0][u] = float(a.x);
+                    vv0[F2 - 1][u] = float(a.y);
+                    vv1[0][u] = float(b2.x);
+                    vv1[F2 - 1][u] = float(b2.y);
                 }
+            } else {
+#pragma unroll
+                for (int h = 0; h < F2; ++h)
+#pragma unroll
+                    for (int u = 0; u < UU; ++u) {
+                        vv0[h][u] = float(px[h][__float_as_int(ea[u].x)]);
+                        vv1[h][u] = float(px[h][__float_as_int(ea[u].y)]);
+                    }
+            }
+#pragma unroll
+            for (int h = 0; h < F2; ++h) {
+                float(&v0)[UU] = vv0[h];
+                float(&v1)[UU] = vv1[h];
                 if constexpr (MODE == kRaw) {
                     // Per-frame masks: {slot, slot, w, w}, {w*norm, w*norm, 0, 0};
                     // a masked entry adds nothing to S, V, N or C, whatever its
@@ -1674,7 +1707,8 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             const double mean = a1 / sw;
             const double m2 = v[2] - mean * a1;
             const double q = m2 / sw;
-            out_d[oo] = sqrt(q > 0.0 ? q : 0.0);
+            // one valid contribution: its deviation from itself is exactly 0
+            out_d[oo] = valid == 1 ? 0.0 : sqrt(q > 0.0 ? q : 0.0);
         }
     }
 }
@@ -1791,7 +1825,8 @@ __device__ __forceinline__ void finalize_tile(
                 const double mean = a1 / sw;
                 const double m2 = v[2] - mean * a1;
                 const double q = m2 / sw;
-                rd = sqrt(q > 0.0 ? q : 0.0);
+                // one valid contribution: its deviation from itself is exactly 0
+                rd = valid == 1 ? 0.0 : sqrt(q > 0.0 ? q : 0.0);
             }
         }
     }

@@ -324,15 +324,26 @@ class Serving:
                                                wait_ms=60000, borrow=True), err, std,
                               time.perf_counter() - t0)
 
+        lat = [0.0] * n
+
+        def consumer():
+            # results are taken as they finish, in submission order, as a
+            # client of the stream would
+            for k in range(n):
+                while tickets[k] is None:
+                    time.sleep(0.0002)
+                key, t, err, std, _ = tickets[k]
+                lat[k] = loop.poll(t, key, errors=err, azimuthal_std=std, wait_ms=60000)[3]
+
         lanes = 4
         threads = [threading.Thread(target=producer, args=(i, lanes)) for i in range(lanes)]
+        cons = threading.Thread(target=consumer)
+        cons.start()
         for th in threads:
             th.start()
         for th in threads:
             th.join()
-        lat = []
-        for key, t, err, std, _ in tickets:
-            lat.append(loop.poll(t, key, errors=err, azimuthal_std=std, wait_ms=60000)[3])
+        cons.join()
         elapsed = time.perf_counter() - t0
         st = loop.stats()
         loop.close()

@@ -66,12 +66,13 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kFlush = 16;  // terms per lane between double-word folds
 // Gather lane mappings a plan chooses from (launch_gather). Entry-lane
 // mappings, as (entry slices per frame group, frames per lane, entries per
-// lane per step): 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2);
-// frame-lane mappings (k_gather_fl), 2 CTAs per SM (5) or 1 CTA per SM with
-// the next frames prefetched while the current ones are summed (6); bin
-// tiles (k_gather_bins: 7, one frame per lane; 8, two), which write the
-// results themselves.
-constexpr int kVariantCount = 9;
+// lane per step): 0 (32,4,4), 1 (32,2,8), 2 (8,2,4), 3 (4,1,8), 4 (16,4,2),
+// and 9 (32,1,8), whose 32 lanes all take entries of one frame (the
+// one-frame launches of the plain path); frame-lane mappings (k_gather_fl),
+// 2 CTAs per SM (5) or 1 CTA per SM with the next frames prefetched while the
+// current ones are summed (6); bin tiles (k_gather_bins: 7, one frame per
+// lane; 8, two), which write the results themselves.
+constexpr int kVariantCount = 10;
 constexpr int kSegMax = 256;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
@@ -2086,7 +2087,7 @@ bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pix
                    int64_t mask_stride = 0, double *oi = nullptr, double *os = nullptr,
                    double *od = nullptr) {
     if constexpr (MODE == kRaw) {
-        if (variant >= 5) variant = 2;  // entry-lane mappings only
+        if (variant >= 5 && variant <= 8) variant = 2;  // entry-lane mappings only
     } else {
         if (variant == 7 || variant == 8) {
             const BinTiles &bt = t.bt[variant - 7];
@@ -2115,6 +2116,7 @@ bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pix
     case 1: k_gather<MODE, P, 32, 2, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
     case 2: k_gather<MODE, P, 8, 2, 4><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
     case 3: k_gather<MODE, P, 4, 1, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
+    case 9: k_gather<MODE, P, 32, 1, 8><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
     default: k_gather<MODE, P, 16, 4, 2><<<t.n_units, kThreads, smem, s>>>(DG_GATHER_ARGS); break;
     }
 #undef DG_GATHER_ARGS

@@ -11,15 +11,16 @@
 // batch's copies overlap another's gather; their staging grows stream-ordered
 // and is kept. max_coalesce 1 serves one request per launch on the plan's own
 // tuned lane mapping (the plain path). Plans live in an HBM cache bounded by
-// bytes and are managed by one builder thread: a request for a plan that is
-// not built asks the builder and stays queued while the workers serve other
+// bytes and are managed by two builder threads: a request for a plan that is
+// not built asks a builder and stays queued while the workers serve other
 // plans; the builder builds the plan on the device, tunes it once per key
 // for small launches, allocates its partial sums for the largest launch,
 // admits it by evicting least-recently-used plans that no worker is using,
 // and destroys evicted and stale plans, so no worker ever waits for a build
 // or a free. A submit copies its frame into a pooled pinned buffer outside
 // the server lock (or borrows the caller's); the worker copies the pinned
-// buffers straight to the device. Re-registering a key (a changed PONI)
+// buffers straight to the device, and each request's results straight back
+// into a pooled pinned buffer that dg_server_poll copies out and returns. Re-registering a key (a changed PONI)
 // gives it a new generation: the next request rebuilds the plan, and the
 // stale plan is destroyed once no worker uses it. A build that fails fails
 // the requests of that generation. Each request's result is identical alone
@@ -92,7 +93,12 @@ struct Request {
     bool borrowed = false;
     Clock::time_point submitted;
     double latency_us = 0;
-    std::vector<double> out_i, out_s, out_d;
+    // Results in a pooled page-locked buffer: nout arrays of n_bins doubles
+    // (intensity, then sigma, then spread as requested), copied there from
+    // the device and out of it by dg_server_poll.
+    double *res = nullptr;
+    size_t res_bytes = 0;
+    int64_t n_bins = 0;
     dg_status status = DG_OK;
     std::string error;
     bool done = false;
@@ -132,7 +138,7 @@ struct dg_server {
     dg_server_stats stats{};
     bool stop = false;
     std::vector<std::thread> workers;
-    std::thread builder;
+    std::vector<std::thread> builders;
     PinnedPool pinned;
     std::vector<CacheEntry> retired;    // stale plans still in use by a worker
     std::vector<dg_plan *> to_destroy;  // plans no worker uses, for the builder
@@ -330,6 +336,10 @@ struct dg_server {
         else stats.failed++;
         if (!r->borrowed) pinned.put(r->frame_bytes, r->frame);
         r->frame = nullptr;
+        if (st != DG_OK && r->res) {
+            pinned.put(r->res_bytes, r->res);
+            r->res = nullptr;
+        }
         inflight--;
     }
 
@@ -367,7 +377,7 @@ struct dg_server {
         dg_multi *multi = nullptr;
         if (!plain && dg_multi_create(cfg.device, kPlansPerLaunch, &multi) != DG_OK) multi = nullptr;
         unsigned char *d_in = nullptr;
-        double *d_out = nullptr, *h_out = nullptr;
+        double *d_out = nullptr;
         size_t in_cap = 0, out_cap = 0;
         for (;;) {
             std::vector<Group> groups;
@@ -462,18 +472,26 @@ struct dg_server {
             }
             if (out_cap < out_need) {
                 if (d_out) cudaFreeAsync(d_out, stream);
-                pinned.put(out_cap * 8, h_out);
                 out_cap = std::max(out_need, 2 * out_cap);
-                h_out = static_cast<double *>(pinned.get(out_cap * 8));
                 if (cudaMallocAsync(reinterpret_cast<void **>(&d_out), out_cap * 8, stream) !=
-                        cudaSuccess || !h_out) {
+                    cudaSuccess) {
                     (void)cudaGetLastError();
                     d_out = nullptr;
                     out_cap = 0;
                 }
             }
+            // each request's results go from the device straight to its own
+            // pooled page-locked buffer
+            bool res_ok = true;
+            for (auto &g : groups)
+                for (Request *r : g.reqs) {
+                    r->n_bins = g.plan->n_bins;
+                    r->res_bytes = size_t(nout) * size_t(r->n_bins) * 8;
+                    r->res = static_cast<double *>(pinned.get(r->res_bytes));
+                    if (!r->res) res_ok = false;
+                }
             const auto t_batch = Clock::now();
-            if (!d_in || !d_out || (!plain && !multi)) {
+            if (!d_in || !d_out || !res_ok || (!plain && !multi)) {
                 st = DG_DEVICE;
                 err = "request loop staging allocation failed";
             } else {
@@ -505,7 +523,14 @@ struct dg_server {
                                             head->dtype, head->flags, stream);
                 }
                 if (st != DG_OK) err = last_error_text();
-                cudaMemcpyAsync(h_out, d_out, out_need * 8, cudaMemcpyDeviceToHost, stream);
+                for (auto &g : groups) {
+                    const size_t nf = g.reqs.size(), nb = size_t(g.plan->n_bins);
+                    for (size_t i = 0; i < nf; ++i)
+                        for (int k = 0; k < nout; ++k)
+                            cudaMemcpyAsync(g.reqs[i]->res + k * nb,
+                                            d_out + g.out_off + (k * nf + i) * nb, nb * 8,
+                                            cudaMemcpyDeviceToHost, stream);
+                }
                 if (cudaStreamSynchronize(stream) != cudaSuccess && st == DG_OK) {
                     st = DG_DEVICE;
                     err = cudaGetErrorString(cudaGetLastError());
@@ -515,24 +540,6 @@ struct dg_server {
                         st = DG_TIMEOUT;
                         err = "bin-tile gather: a chunk-pipeline wait gave up after 1 s";
                     }
-                if (st == DG_OK) {
-                    for (auto &g : groups) {
-                        const size_t nf = g.reqs.size(), nb = size_t(g.plan->n_bins);
-                        const double *o = h_out + g.out_off;
-                        for (size_t i = 0; i < nf; ++i) {
-                            Request *r = g.reqs[i];
-                            int kk = 0;
-                            r->out_i.assign(o + i * nb, o + (i + 1) * nb);
-                            ++kk;
-                            if (head->flags & DG_ERRORS) {
-                                r->out_s.assign(o + (kk * nf + i) * nb, o + (kk * nf + i + 1) * nb);
-                                ++kk;
-                            }
-                            if (head->flags & DG_AZIMUTHAL_STD)
-                                r->out_d.assign(o + (kk * nf + i) * nb, o + (kk * nf + i + 1) * nb);
-                        }
-                    }
-                }
             }
             for (auto &g : groups) release(g.key, g.plan);
             {
@@ -554,7 +561,6 @@ struct dg_server {
             cudaStreamDestroy(stream);
         }
         if (multi) dg_multi_destroy(multi);
-        pinned.put(out_cap * 8, h_out);
     }
 };
 
@@ -581,7 +587,8 @@ dg_status dg_server_create(const dg_server_config *config, dg_server **out) {
     auto s = std::make_unique<dg_server>();
     s->cfg = *config;
     for (int i = 0; i < 4; ++i) s->workers.emplace_back([p = s.get()] { p->worker_main(); });
-    s->builder = std::thread([p = s.get()] { p->builder_main(); });
+    // two builders: a rebuild of one large plan does not hold up another's
+    for (int i = 0; i < 2; ++i) s->builders.emplace_back([p = s.get()] { p->builder_main(); });
     *out = s.release();
     return DG_OK;
 }
@@ -595,12 +602,15 @@ dg_status dg_server_destroy(dg_server *server) {
     server->cv_work.notify_all();
     server->cv_build.notify_all();
     for (auto &t : server->workers) t.join();
-    server->builder.join();
+    for (auto &t : server->builders) t.join();
     for (dg_plan *p : server->to_destroy) dg_plan_destroy(p);
     for (auto &kv : server->cache) dg_plan_destroy(kv.second.plan);
     for (auto &e : server->retired) dg_plan_destroy(e.plan);
-    for (auto &kv : server->requests)
-        if (kv.second->frame) server->pinned.put(kv.second->frame_bytes, kv.second->frame);
+    for (auto &kv : server->requests) {
+        if (kv.second->frame && !kv.second->borrowed)
+            server->pinned.put(kv.second->frame_bytes, kv.second->frame);
+        if (kv.second->res) server->pinned.put(kv.second->res_bytes, kv.second->res);
+    }
     delete server;
     return DG_OK;
 }
@@ -695,9 +705,17 @@ dg_status dg_server_poll(dg_server *server, uint64_t ticket, int32_t wait_ms, do
         return server_fail(DG_TIMEOUT, "request not finished");
     dg_status st = r->status;
     if (st == DG_OK) {
-        if (oi) std::copy(r->out_i.begin(), r->out_i.end(), oi);
-        if (os && !r->out_s.empty()) std::copy(r->out_s.begin(), r->out_s.end(), os);
-        if (od && !r->out_d.empty()) std::copy(r->out_d.begin(), r->out_d.end(), od);
+        const int64_t nb = r->n_bins;
+        int k = 0;
+        if (oi) std::memcpy(oi, r->res, size_t(nb) * 8);
+        ++k;
+        if (r->flags & DG_ERRORS) {
+            if (os) std::memcpy(os, r->res + k * nb, size_t(nb) * 8);
+            ++k;
+        }
+        if ((r->flags & DG_AZIMUTHAL_STD) && od) std::memcpy(od, r->res + k * nb, size_t(nb) * 8);
+        server->pinned.put(r->res_bytes, r->res);
+        r->res = nullptr;
     } else {
         server_fail(st, r->error);
     }

@@ -732,7 +732,8 @@ def main():
                      "traffic": MEASURED_TRAFFIC.get((w.name, variant, n_frames)),
                      "peak_kind": peak_kind,
                      "kernel": ("k_gather_bins" if variant in (7, 8) else
-                                "k_gather_fl" if variant in (5, 6) else "k_gather"),
+                                "k_gather_fl" if variant in (5, 6) else
+                                "k_rows" if variant == 10 else "k_gather"),
                      "alg_bytes_per_launch": alg,
                      "kernel_ms_per_launch": round(per_launch_s * 1000, 4)},
         "clocks": clk,

@@ -71,8 +71,9 @@ constexpr int kFlush = 16;  // terms per lane between double-word folds
 // one-frame launches of the plain path); frame-lane mappings (k_gather_fl),
 // 2 CTAs per SM (5) or 1 CTA per SM with the next frames prefetched while the
 // current ones are summed (6); bin tiles (k_gather_bins: 7, one frame per
-// lane; 8, two), which write the results themselves.
-constexpr int kVariantCount = 10;
+// lane; 8, two), which write the results themselves; row warps (k_rows, 10)
+// for launches of a few frames, which write them too.
+constexpr int kVariantCount = 11;
 constexpr int kSegMax = 256;
 constexpr int kUnitCap = 3008;  // 16-byte entries in the 48 KB default shared memory
 
@@ -481,6 +482,250 @@ __global__ void __launch_bounds__(kThreads)
     gather_unit<MODE, P, SLICES, FPL, U>(blockIdx.x, units, segs, entry, entry_std, entry_nlo,
                                          first_valid, origin_entry, frames, n_pixels, n_frames,
                                          n_segments, partial, masks, mask_stride);
+}
+
+// ---------------------------------------------------------------------------
+// Row warps (lane mapping 10): launches of a few frames. A batch amortises
+// the table over its frames; one frame reads every entry once, so what
+// counts there is keeping enough loads in flight and doing nothing else: no
+// staging, no partial sums, no second launch. A row of at most kRowsLong
+// entries is one warp's (eight rows per CTA), a longer one the whole CTA's
+// (largest first, so the long rows start early). Threads stride the row's
+// entries (coalesced), kRowsU of them in flight each, load the pixels of F
+// frames per entry and sum in FP64; the warp (then the CTA's warps in a fixed
+// order) adds the threads' sums by a fixed butterfly and one thread writes the
+// results (normalize_bin, prepared.rs:985-996; the spread's closing formulas,
+// azimuthal.rs:96-104). The spread is shifted by the row's origin as in the
+// other mappings, in FP64: t = s - o*n with n the entry's FP32 pair.
+constexpr int kRowsLong = 512;
+constexpr int kRowsU = 4;
+constexpr int kRowsThreads = 256;
+
+template <typename P>
+__device__ __forceinline__ double load_px_d(const P *__restrict__ f, uint32_t i) {
+    return double(__ldg(f + i));
+}
+
+// Butterfly sum over the 32 lanes: every lane ends with the same value (IEEE
+// addition is commutative, so partners compute the same sums).
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, m));
+    return v;
+}
+
+// Shared memory of a row-warp CTA: the warps' sums of a long row.
+constexpr int kRowsWarps = kRowsThreads / 32;
+using RowsRed = double[kRowsWarps][4 * kMaxAcc];
+
+// One row-warp item of a plan's batch (q.item[k]); every thread of the CTA
+// calls it. F frames per pass over the entries.
+template <int MODE, typename P, int F>
+__device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s_red) {
+    constexpr int NA = NAcc<MODE, P>::value;
+    constexpr bool SPREAD = MODE == kSpread;
+    constexpr int NW = kRowsWarps;
+    const int2 *__restrict__ items = qp.item;
+    const int32_t *__restrict__ rows = qp.rows;
+    const int32_t *__restrict__ row_ptr = qp.row_ptr;
+    const int2 *__restrict__ entry = qp.entry;
+    const float4 *__restrict__ entry_std = qp.entry_std;
+    const float *__restrict__ entry_nlo = qp.entry_nlo;
+    const int32_t *__restrict__ first_valid = qp.first_valid;
+    const int32_t *__restrict__ origin_entry = qp.origin;
+    const double *__restrict__ den = qp.den;
+    const double *__restrict__ den_std = qp.den_std;
+    const int32_t *__restrict__ valid_std = qp.valid_std;
+    const P *__restrict__ frames = static_cast<const P *>(qp.frames);
+    const int64_t n_pixels = qp.n_pixels;
+    const int n_frames = qp.n_frames, n_rows = qp.n_rows;
+    double *__restrict__ out_i = qp.out_i;
+    double *__restrict__ out_s = qp.out_s;
+    double *__restrict__ out_d = qp.out_d;
+    const int2 it = items[k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool whole = it.y == 0;  // one long row for the whole CTA
+    if (!whole && warp >= it.y) return;  // no CTA-wide barrier in this case
+    const int row = rows[it.x + (whole ? 0 : warp)];
+    const int e0 = row_ptr[row], e1 = row_ptr[row + 1];
+    const int li = whole ? int(threadIdx.x) : lane, nl = whole ? kRowsThreads : 32;
+    const int org = SPREAD ? origin_entry[row] : -1, fvalid = SPREAD ? first_valid[row] : -1;
+    for (int f0 = 0; f0 < n_frames; f0 += F) {
+        const P *fr[F];
+#pragma unroll
+        for (int q = 0; q < F; ++q) fr[q] = frames + int64_t(min(f0 + q, n_frames - 1)) * n_pixels;
+        double o[F];
+#pragma unroll
+        for (int q = 0; q < F; ++q)
+            o[q] = SPREAD ? double(row_origin<P>(entry_std, org, fvalid, e1, fr[q])) : 0.0;
+        double acc[F][NA];
+#pragma unroll
+        for (int q = 0; q < F; ++q)
+#pragma unroll
+            for (int a = 0; a < NA; ++a) acc[q][a] = 0.0;
+        for (int j0 = e0 + li; j0 < e1; j0 += nl * kRowsU) {
+            float4 es[kRowsU];
+            float nlo[kRowsU];
+            int2 en[kRowsU];
+            double x[kRowsU][F];
+#pragma unroll
+            for (int u = 0; u < kRowsU; ++u) {
+                const int j = j0 + nl * u;
+                const bool in = j < e1;
+                uint32_t col = 0;
+                if constexpr (SPREAD) {
+                    es[u] = in ? entry_std[j] : make_float4(0.f, 0.f, 1.f, 0.f);
+                    nlo[u] = in ? entry_nlo[j] : 0.f;
+                    col = uint32_t(__float_as_int(es[u].x));
+                } else {
+                    en[u] = in ? entry[j] : make_int2(0, 0);
+                    col = uint32_t(en[u].x);
+                }
+#pragma unroll
+                for (int q = 0; q < F; ++q) x[u][q] = in ? load_px_d<P>(fr[q], col) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kRowsU; ++u) {
+                if (j0 + nl * u >= e1) break;
+                if constexpr (SPREAD) {
+                    const double c = es[u].y, cr = es[u].w;
+                    const double n = __dadd_rn(double(es[u].z), double(nlo[u]));
+                    const double c2 = __dmul_rn(c, c);
+#pragma unroll
+                    for (int q = 0; q < F; ++q) {
+                        const double v = x[u][q];
+                        if (is_float_px<P>() && !isfinite(v)) {
+                            acc[q][NA - 2] = __dadd_rn(acc[q][NA - 2], __dmul_rn(c, n));
+                            acc[q][NA - 1] = __dadd_rn(acc[q][NA - 1], c > 0.0 ? 1.0 : 0.0);
+                            continue;
+                        }
+                        acc[q][0] = __fma_rn(c, v, acc[q][0]);
+                        acc[q][1] = __fma_rn(c2, is_unsigned_px<P>() ? v : fmax(v, 0.0), acc[q][1]);
+                        const double t = __fma_rn(-o[q], n, v);
+                        acc[q][2] = __fma_rn(__dmul_rn(cr, t), t, acc[q][2]);
+                        acc[q][kSpreadA] = __fma_rn(c, t, acc[q][kSpreadA]);
+                    }
+                } else {
+                    const double c = __int_as_float(en[u].y);
+                    const double c2 = __dmul_rn(c, c);
+#pragma unroll
+                    for (int q = 0; q < F; ++q) {
+                        acc[q][0] = __fma_rn(c, x[u][q], acc[q][0]);
+                        if (MODE == kErrors)
+                            acc[q][1] = __fma_rn(c2, is_unsigned_px<P>() ? x[u][q] : fmax(x[u][q], 0.0),
+                                                 acc[q][1]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < F; ++q)
+#pragma unroll
+            for (int a = 0; a < NA; ++a) acc[q][a] = warp_sum_d(acc[q][a]);
+        if (whole) {
+            if (lane == 0)
+#pragma unroll
+                for (int q = 0; q < F; ++q)
+#pragma unroll
+                    for (int a = 0; a < NA; ++a) s_red[warp][q * NA + a] = acc[q][a];
+            __syncthreads();
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int q = 0; q < F; ++q)
+#pragma unroll
+                    for (int a = 0; a < NA; ++a) {
+                        double v = s_red[0][q * NA + a];
+                        for (int w = 1; w < NW; ++w) v = __dadd_rn(v, s_red[w][q * NA + a]);
+                        acc[q][a] = v;
+                    }
+            __syncthreads();  // s_red is rewritten by the next frames
+            if (threadIdx.x != 0) continue;
+        } else if (lane != 0) {
+            continue;
+        }
+#pragma unroll
+        for (int q = 0; q < F; ++q) {
+            if (f0 + q >= n_frames) break;
+            const double *v = acc[q];
+            const int64_t oo = int64_t(f0 + q) * n_rows + row;
+            if constexpr (!SPREAD) {
+                const double n = den[row];
+                out_i[oo] = n == 0.0 ? 0.0 : v[0] / n;
+                if (MODE == kErrors) {
+                    const double s2 = n == 0.0 ? 0.0 : v[1] / (n * n);
+                    out_s[oo] = sqrt(s2 > 0.0 ? s2 : 0.0);
+                }
+            } else {
+                int valid = valid_std[row];
+                double sw = den_std[row];
+                if (NA == 6) {
+                    valid -= int(v[NA - 1] + 0.5);
+                    sw -= v[NA - 2];
+                }
+                if (valid <= 0 || !(sw > 0.0)) {
+                    out_i[oo] = 0.0;
+                    if (out_s) out_s[oo] = 0.0;
+                    out_d[oo] = __longlong_as_double(0x7ff8000000000000ll);
+                    continue;
+                }
+                const double a1 = v[kSpreadA];
+                out_i[oo] = v[0] / sw;
+                if (out_s) out_s[oo] = sqrt(v[1] > 0.0 ? v[1] : 0.0) / sw;
+                const double mean = a1 / sw;
+                const double q2 = (v[2] - mean * a1) / sw;
+                // one valid contribution: its deviation from itself is exactly 0
+                out_d[oo] = valid == 1 ? 0.0 : sqrt(q2 > 0.0 ? q2 : 0.0);
+            }
+        }
+    }
+}
+
+// Lane mapping 10 for one plan's batch: one CTA per item.
+template <int MODE, typename P, int F>
+__global__ void __launch_bounds__(kRowsThreads) k_rows(const QueuePlan q) {
+    __shared__ RowsRed s_red;
+    rows_item<MODE, P, F>(q, blockIdx.x, s_red);
+}
+
+// Frames per pass of a row-warp launch of nf frames: one pass for up to
+// four frames.
+__host__ __device__ constexpr int rows_pass_frames(int nf) { return nf <= 1 ? 1 : nf <= 2 ? 2 : 4; }
+
+// Work-queue gather over several plans (dg_multi_integrate). A persistent
+// grid of row-warp CTAs claims (plan, item) items from one counter until
+// every plan's items are summed, so plans of very different sizes share one
+// launch and the GPU stays full to the last item. A plan's results are those
+// of lane mapping 10 launched for that plan alone, bit for bit. No CTA waits
+// on another: a claim is one atomic add, and a CTA that finds the counter
+// past the end returns.
+template <int MODE, typename P>
+__global__ void __launch_bounds__(kRowsThreads)
+    k_rows_queue(QueueHeader *__restrict__ hdr, const QueuePlan *__restrict__ plans) {
+    __shared__ RowsRed s_red;
+    __shared__ int s_item;
+    const int n_plans = hdr->n_plans, total = hdr->total_items;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();  // every thread has read s_item before it is claimed again
+        if (item >= total) return;
+        // the last descriptor whose first item is at most `item` (plans with
+        // no items share the next one's prefix and are skipped)
+        int lo = 0, hi = n_plans - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (plans[mid].item_first <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const QueuePlan &q = plans[lo];
+        const int k = item - q.item_first;
+        switch (rows_pass_frames(q.n_frames)) {
+        case 1: rows_item<MODE, P, 1>(q, k, s_red); break;
+        case 2: rows_item<MODE, P, 2>(q, k, s_red); break;
+        default: rows_item<MODE, P, 4>(q, k, s_red); break;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1380,16 +1625,34 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                                    ? load_px<P>(base + mb[MH + k] + int64_t(j * FSTEP) * n_pixels, 0u)
                                    : S(0);
             }
+        } else if constexpr (sizeof(P) == 4) {
+            // This lane's slots s0 + lane + 32 i and their pixel indices, read
+            // once; then frame by frame, one address add and one copy per
+            // (slot, frame).
+            int idx[KSTEP];
+            bool kin[KSTEP];
+#pragma unroll
+            for (int i = 0; i < KSTEP; ++i) {
+                const int k = s0 + lane + 32 * i;
+                kin[i] = k < k1;
+                idx[i] = kin[i] ? mb[MH + k] : 0;
+            }
+#pragma unroll
+            for (int j = 0; j < FS; ++j) {
+                const int f = fw + j * FSTEP;
+                if (f >= nv) break;
+                const P *fsrc = base + int64_t(j * FSTEP) * n_pixels;
+#pragma unroll
+                for (int i = 0; i < KSTEP; ++i)
+                    if (kin[i]) cp_async4(dst + pxi(f, s0 + lane + 32 * i), fsrc + idx[i]);
+            }
         } else {
             for (int k = s0 + lane; k < k1; k += 32) {
                 const P *src = base + mb[MH + k];
 #pragma unroll
                 for (int j = 0; j < FS; ++j) {
                     if (fw + j * FSTEP >= nv) break;
-                    if constexpr (sizeof(P) == 4)
-                        cp_async4(dst + pxi(fw + j * FSTEP, k), src + int64_t(j * FSTEP) * n_pixels);
-                    else
-                        dst[pxi(fw + j * FSTEP, k)] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
+                    dst[pxi(fw + j * FSTEP, k)] = load_px<P>(src + int64_t(j * FSTEP) * n_pixels, 0u);
                 }
             }
         }
@@ -1875,63 +2138,6 @@ __global__ void __launch_bounds__(256)
                            den_std, valid_std, n_rows, n_frames, out_i, out_s, out_d);
 }
 
-// Work-queue gather over several plans (dg_multi_integrate). A persistent
-// grid of entry-lane CTAs (lane mapping 2: 8 entry slices, 2 frames per lane,
-// 4 entries in flight) claims (plan, unit) items from one counter until every
-// plan's units are summed, so plans of very different sizes share one launch
-// and the GPU stays full to the last unit; then a grid-stride finalize walks
-// the (plan, row tile, frame block) items. A plan's sums are those of
-// mapping 2 launched for that plan alone, bit for bit.
-constexpr int kQueueSlices = 8, kQueueFpl = 2, kQueueU = 4;
-
-// The last descriptor whose prefix field (first unit or first tile) is at
-// most `item`: descriptors with nothing to do share the next one's prefix
-// and are skipped.
-template <bool TILES>
-__device__ __forceinline__ int queue_owner(const QueuePlan *__restrict__ plans, int n_plans,
-                                           int item) {
-    int lo = 0, hi = n_plans - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        const int first = TILES ? plans[mid].tile_first : plans[mid].unit_first;
-        if (first <= item) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-template <int MODE, typename P>
-__global__ void __launch_bounds__(kThreads)
-    k_gather_queue(QueueHeader *__restrict__ hdr, const QueuePlan *__restrict__ plans) {
-    __shared__ int s_item;
-    const int n_plans = hdr->n_plans, total = hdr->total_units;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, 1);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();  // every thread has read s_item before it is claimed again
-        if (item >= total) return;
-        const QueuePlan &q = plans[queue_owner<false>(plans, n_plans, item)];
-        gather_unit<MODE, P, kQueueSlices, kQueueFpl, kQueueU>(
-            item - q.unit_first, q.unit, q.seg, q.entry, q.entry_std, q.entry_nlo, q.first_valid,
-            q.origin, static_cast<const P *>(q.frames), q.n_pixels, q.n_frames, q.n_segments,
-            q.partial, nullptr, 0);
-    }
-}
-
-template <int MODE, typename P>
-__global__ void __launch_bounds__(256)
-    k_finalize_queue(const QueueHeader *__restrict__ hdr, const QueuePlan *__restrict__ plans) {
-    const int n_plans = hdr->n_plans, total = hdr->total_tiles;
-    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
-        const QueuePlan &q = plans[queue_owner<true>(plans, n_plans, tile)];
-        const int local = tile - q.tile_first;
-        finalize_tile<MODE, P>((local / q.frame_blocks) * kFinRows, (local % q.frame_blocks) * 32,
-                               q.partial, q.row_seg, q.seg_ids, q.den, q.den_std, q.valid_std,
-                               q.n_rows, q.n_frames, q.out_i, q.out_s, q.out_d);
-    }
-}
-
 // Raw sums per (frame, row) (IntermediateResult1d, lut/integrate.rs:372-379):
 // S and V from the partial sums; N and C from them too for the per-frame-mask
 // gather, else the plan's strict FP64 denominator and weight sum.
@@ -2095,8 +2301,23 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
         t.withhold_test, t.cnt.ptr, oc, raw, masks, mask_stride);
 }
 
+// Row warps (mapping 10): F frames per pass over a row's entries, so a
+// launch of up to four frames reads every entry once.
+template <int MODE, typename P>
+void launch_rows(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, double *oi,
+                 double *os, double *od, cudaStream_t s) {
+    const QueuePlan q = queue_plan(t, fp, n_pixels, nf, oi, os, od);
+    const unsigned grid = unsigned(q.n_items);
+    switch (rows_pass_frames(nf)) {
+    case 1: k_rows<MODE, P, 1><<<grid, kRowsThreads, 0, s>>>(q); break;
+    case 2: k_rows<MODE, P, 2><<<grid, kRowsThreads, 0, s>>>(q); break;
+    default: k_rows<MODE, P, 4><<<grid, kRowsThreads, 0, s>>>(q); break;
+    }
+    DG_CUDA(cudaGetLastError());
+}
+
 // Launches lane mapping `variant`; returns true when the kernel wrote the
-// normalised results to oi/os/od itself (mappings 7, 8), false when it left
+// normalised results to oi/os/od itself (mappings 7, 8, 10), false when it left
 // partial sums for k_finalize. Those mappings need the outputs; callers without
 // them (raw sums) get the frame-lane or an entry-lane mapping instead.
 template <int MODE, typename P>
@@ -2105,8 +2326,15 @@ bool launch_gather(const GatherTable &t, int variant, const P *fp, int64_t n_pix
                    int64_t mask_stride = 0, double *oi = nullptr, double *os = nullptr,
                    double *od = nullptr) {
     if constexpr (MODE == kRaw) {
-        if (variant >= 5 && variant <= 8) variant = 2;  // entry-lane mappings only
+        if ((variant >= 5 && variant <= 8) || variant == 10) variant = 2;  // entry-lane mappings only
     } else {
+        if (variant == 10) {
+            if (oi && t.rw_n_items > 0) {
+                launch_rows<MODE, P>(t, fp, n_pixels, nf, oi, os, od, s);
+                return true;
+            }
+            variant = 2;
+        }
         if (variant == 7 || variant == 8) {
             const BinTiles &bt = t.bt[variant - 7];
             if (oi && bt.n_items > 0) {
@@ -2651,6 +2879,35 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     }
     DG_CUDA(cudaMemcpyAsync(out.row_seg.ptr, row_seg.data(), row_seg.size() * 4,
                             cudaMemcpyHostToDevice, s));
+    // Row warps (mapping 10): long rows one per CTA, longest first; the
+    // others eight per CTA in row order.
+    std::vector<int32_t> rw_ptr, rw_rows;
+    std::vector<int2> rw_items;
+    if (table.nnz <= INT32_MAX && nb > 0) {
+        rw_ptr.assign(rp.begin(), rp.end());
+        for (int64_t r = 0; r < nb; ++r)
+            if (rp[size_t(r) + 1] - rp[size_t(r)] > kRowsLong) rw_rows.push_back(int32_t(r));
+        std::stable_sort(rw_rows.begin(), rw_rows.end(), [&](int32_t a, int32_t b) {
+            return rp[size_t(a) + 1] - rp[size_t(a)] > rp[size_t(b) + 1] - rp[size_t(b)];
+        });
+        for (size_t i = 0; i < rw_rows.size(); ++i) rw_items.push_back(make_int2(int(i), 0));
+        const size_t first_short = rw_rows.size();
+        for (int64_t r = 0; r < nb; ++r)
+            if (rp[size_t(r) + 1] - rp[size_t(r)] <= kRowsLong) rw_rows.push_back(int32_t(r));
+        for (size_t i = first_short; i < rw_rows.size(); i += kRowsThreads / 32)
+            rw_items.push_back(make_int2(int(i), int(std::min<size_t>(kRowsThreads / 32,
+                                                                      rw_rows.size() - i))));
+        out.rw_row_ptr.alloc(rw_ptr.size());
+        out.rw_rows.alloc(rw_rows.size());
+        out.rw_item.alloc(rw_items.size());
+        DG_CUDA(cudaMemcpyAsync(out.rw_row_ptr.ptr, rw_ptr.data(), rw_ptr.size() * 4,
+                                cudaMemcpyHostToDevice, s));
+        DG_CUDA(cudaMemcpyAsync(out.rw_rows.ptr, rw_rows.data(), rw_rows.size() * 4,
+                                cudaMemcpyHostToDevice, s));
+        DG_CUDA(cudaMemcpyAsync(out.rw_item.ptr, rw_items.data(), rw_items.size() * sizeof(int2),
+                                cudaMemcpyHostToDevice, s));
+        out.rw_n_items = int32_t(rw_items.size());
+    }
     DG_CUDA(cudaStreamSynchronize(s));
     build_fl_units(out, table, segs, [&](int cap, int max_segs, std::vector<int4> &fl) {
         group(cap, max_segs, [&](int first, int n) { fl.push_back(make_int4(first, n, 0, 0)); });
@@ -2658,6 +2915,7 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
 }
 
 bool gather_writes_results(const GatherTable &t) {
+    if (t.variant == 10) return t.rw_n_items > 0;
     return (t.variant == 7 || t.variant == 8) && t.bt[t.variant - 7].n_items > 0;
 }
 
@@ -2675,29 +2933,25 @@ void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtyp
 QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixels, int n_frames,
                      double *oi, double *os, double *od) {
     QueuePlan q{};
-    q.unit = t.unit.ptr;
-    q.seg = t.seg.ptr;
+    q.item = t.rw_item.ptr;
+    q.rows = t.rw_rows.ptr;
+    q.row_ptr = t.rw_row_ptr.ptr;
     q.entry = t.entry.ptr;
     q.entry_std = t.entry_std.ptr;
     q.entry_nlo = t.entry_nlo.ptr;
     q.first_valid = t.first_valid.ptr;
     q.origin = t.origin.ptr;
-    q.frames = d_frames;
-    q.partial = t.partial.ptr;
-    q.row_seg = t.row_seg.ptr;
-    q.seg_ids = t.seg_ids.ptr;
     q.den = t.den.ptr;
     q.den_std = t.den_std.ptr;
     q.valid_std = t.valid_std.ptr;
+    q.frames = d_frames;
     q.out_i = oi;
     q.out_s = os;
     q.out_d = od;
     q.n_pixels = n_pixels;
     q.n_frames = n_frames;
-    q.n_segments = t.n_segments;
-    q.n_units = n_frames > 0 ? t.n_units : 0;
-    q.n_rows = n_frames > 0 ? t.n_rows : 0;
-    q.frame_blocks = std::max(1, (n_frames + 31) / 32);
+    q.n_rows = t.n_rows;
+    q.n_items = n_frames > 0 ? t.rw_n_items : 0;
     return q;
 }
 
@@ -2709,10 +2963,9 @@ template <int MODE, typename P>
 int queue_gather_grid() {
     static int grid = 0;
     if (grid == 0) {
-        const size_t smem = size_t(kUnitCap) * (MODE == kSpread ? 16 : 8);
         int per_sm = 0, dev = 0, sms = 0;
-        DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_queue<MODE, P>,
-                                                              kThreads, smem));
+        DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rows_queue<MODE, P>,
+                                                              kRowsThreads, 0));
         DG_CUDA(cudaGetDevice(&dev));
         DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         grid = std::max(1, per_sm) * std::max(1, sms);
@@ -2722,13 +2975,7 @@ int queue_gather_grid() {
 
 template <int MODE, typename P>
 void queue_launch_typed(QueueHeader *hdr, const QueuePlan *plans, cudaStream_t s) {
-    const size_t smem = size_t(kUnitCap) * (MODE == kSpread ? 16 : 8);
-    k_gather_queue<MODE, P><<<queue_gather_grid<MODE, P>(), kThreads, smem, s>>>(hdr, plans);
-    DG_CUDA(cudaGetLastError());
-    int dev = 0, sms = 0;
-    DG_CUDA(cudaGetDevice(&dev));
-    DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    k_finalize_queue<MODE, P><<<8 * sms, 32 * kFinRows, 0, s>>>(hdr, plans);
+    k_rows_queue<MODE, P><<<queue_gather_grid<MODE, P>(), kRowsThreads, 0, s>>>(hdr, plans);
     DG_CUDA(cudaGetLastError());
 }
 
@@ -3035,6 +3282,7 @@ bool gather_variant_available(const GatherTable &t, int variant) {
     if (variant < 0 || variant >= kVariantCount) return false;
     if (variant == 5 || variant == 6) return t.fl_n_units > 0;
     if (variant == 7 || variant == 8) return t.bt[variant - 7].n_items > 0;
+    if (variant == 10) return t.rw_n_items > 0;
     return true;
 }
 

@@ -300,6 +300,14 @@ struct GatherTable {
     DeviceArray<double> cnt;
     // Bin tiles (k_gather_bins), mappings 7 and 8; see dg_gather.cu.
     BinTiles bt[2];
+    // Row warps (k_rows), mapping 10: row pointers, rows with more than
+    // kRowsLong entries (longest first) then the others, and one item per
+    // CTA: {first row in rw_rows, 0} for a long row, {first, count <= 8} for
+    // short rows taken one per warp.
+    int32_t rw_n_items = 0;
+    DeviceArray<int32_t> rw_row_ptr;
+    DeviceArray<int32_t> rw_rows;
+    DeviceArray<int2> rw_item;
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     int withhold_test = 0;            // bin tiles: stall one warp (dg_plan_test_wait_timeout)
     int32_t flip_rows = 0, flip_cols = 0;  // frames stored bottom row first (0: detector order)
@@ -333,39 +341,38 @@ bool gather_writes_results(const GatherTable &t);
 // for a plan whose bin tiles need none, unless `any_mapping`).
 void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtype,
                       bool any_mapping = false);
-// Work-queue gather over several plans (dg_multi.cu, dg_gather.cu): one
-// descriptor per (plan, batch of frames), after a header. The gather's CTAs
-// claim (plan, unit) items from `counter` until total_units are done; the
-// finalize walks (plan, row tile, frame block) items. Prefix indices give
-// each plan's first unit and first finalize tile.
+// Row warps (k_rows, lane mapping 10) over one plan's batch, and the
+// work-queue gather over several plans (dg_multi.cu, dg_gather.cu): one
+// descriptor per (plan, batch of frames), after a header. The queue's
+// persistent CTAs claim (plan, row item) items from `counter` until
+// total_items are done; item_first is the prefix index of a plan's first
+// item.
 struct QueuePlan {
-    const int2 *unit;
-    const int4 *seg;
+    const int2 *item;
+    const int32_t *rows;
+    const int32_t *row_ptr;
     const int2 *entry;
     const float4 *entry_std;
     const float *entry_nlo;
     const int32_t *first_valid;
     const int32_t *origin;
-    const void *frames;
-    double *partial;
-    const int32_t *row_seg;
-    const int32_t *seg_ids;
     const double *den;
     const double *den_std;
     const int32_t *valid_std;
+    const void *frames;
     double *out_i, *out_s, *out_d;
     int64_t n_pixels;
-    int32_t n_frames, n_segments, n_units, n_rows;
-    int32_t unit_first, tile_first, frame_blocks, pad;
+    int32_t n_frames, n_rows, n_items, item_first;
 };
 struct QueueHeader {
-    int32_t n_plans, total_units, total_tiles, counter;  // counter: 0 before each launch
+    int32_t n_plans, total_items, counter, pad;  // counter: 0 before each launch
 };
-// Fills a descriptor from a plan's gather table (prefix fields left 0).
+// Fills a descriptor from a plan's gather table (item_first left 0); n_items
+// is 0 when the table has no row-warp items (more than 2^31 entries).
 QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixels, int n_frames,
                      double *oi, double *os, double *od);
-// Enqueues the work-queue gather and its finalize for descriptors already
-// in device memory (`hdr` followed by the descriptors) on `s`.
+// Enqueues the work-queue gather for descriptors already in device memory
+// (`hdr` followed by the descriptors) on `s`.
 void queue_launch(int dtype, uint32_t flags, QueueHeader *hdr, const QueuePlan *plans,
                   cudaStream_t s);
 // The allocation-free path's fixed device array (dg_gather.cu): its address

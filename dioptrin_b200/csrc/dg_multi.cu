@@ -3,14 +3,16 @@
 // A dg_multi holds the device descriptors of one call (a header and one
 // QueuePlan per plan batch) and, per pixel type and output set, a CUDA graph
 // of the call's device work: the copy of the descriptors from page-locked
-// host staging, the work-queue gather (a persistent grid whose CTAs claim
-// (plan, unit) items from a counter the copy resets) and its grid-stride
-// finalize. The graph is captured on the first call of its kind and replayed
-// after that, the descriptors changing between calls while the graph stays
-// the same: one graph launch per batch of plans, whatever their number and
-// sizes. The reference's streaming driver (src/batch/bounded.rs:172) and its
-// engine's pipelined tiles (src/integration/cuda/device.rs:1417-1584) keep
-// one plan per launch.
+// host staging and the work-queue gather (a persistent grid of row-warp CTAs
+// that claim (plan, row item) items from a counter the copy resets and write
+// each row's results themselves). The graph is captured on the first call of
+// its kind and replayed after that, the descriptors changing between calls
+// while the graph stays the same: one graph launch per batch of plans,
+// whatever their number and sizes. No plan scratch is used, so calls on
+// different streams that share plans are not ordered against each other. The
+// reference's streaming driver (src/batch/bounded.rs:172) and its engine's
+// pipelined tiles (src/integration/cuda/device.rs:1417-1584) keep one plan
+// per launch.
 #include <algorithm>
 #include <cstring>
 #include <functional>
@@ -179,30 +181,25 @@ dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items, int32_
         multi->pending = false;
         auto *hdr = reinterpret_cast<dg::QueueHeader *>(multi->host);
         auto *desc = reinterpret_cast<dg::QueuePlan *>(multi->host + sizeof(dg::QueueHeader));
-        int32_t units = 0, tiles = 0, n = 0;
+        int32_t items_total = 0, n = 0;
         for (int32_t i = 0; i < n_items; ++i) {
             const dg_multi_item &it = items[i];
             if (it.n_frames == 0) continue;
-            dg::GatherTable &t = it.plan->gather;
-            dg::reserve_partials(t, it.n_frames, flags, dtype, true);
+            const dg::GatherTable &t = it.plan->gather;
             dg::QueuePlan q = dg::queue_plan(
                 t, it.d_frames, int64_t(it.plan->dim1) * it.plan->dim2, int(it.n_frames),
                 it.d_intensity, (flags & DG_ERRORS) ? it.d_sigma : nullptr,
                 (flags & DG_AZIMUTHAL_STD) ? it.d_std : nullptr);
-            q.unit_first = units;
-            q.tile_first = tiles;
-            units += q.n_units;
-            tiles += (q.n_rows + 7) / 8 * q.frame_blocks;
+            if (q.n_items <= 0 && t.n_rows > 0)
+                fail(DG_UNSUPPORTED, "the work-queue gather needs a table of at most 2^31 entries");
+            q.item_first = items_total;
+            items_total += q.n_items;
             desc[n++] = q;
         }
         if (n == 0) return;
         hdr->n_plans = n;
-        hdr->total_units = units;
-        hdr->total_tiles = tiles;
+        hdr->total_items = items_total;
         hdr->counter = 0;
-        // Partial sums of a plan are ordered across streams (ScratchOrder).
-        for (int32_t i = 0; i < n_items; ++i)
-            if (items[i].n_frames) items[i].plan->gather.scratch.wait(s);
         const auto key = std::make_pair(dtype, flags);
         auto g = multi->graphs.find(key);
         if (g == multi->graphs.end()) {
@@ -231,12 +228,8 @@ dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items, int32_
         DG_CUDA(cudaGraphLaunch(g->second, s));
         DG_CUDA(cudaEventRecord(multi->done, s));
         multi->pending = true;
-        for (int32_t i = 0; i < n_items; ++i) {
-            if (!items[i].n_frames) continue;
-            dg::GatherTable &t = items[i].plan->gather;
-            t.scratch.mark(s);
-            t.launches += 2;
-        }
+        for (int32_t i = 0; i < n_items; ++i)
+            if (items[i].n_frames) items[i].plan->gather.launches += 1;
     });
 }
 

@@ -6,26 +6,27 @@
 // flags behind it (up to max_coalesce) into one launch, and publish results
 // per request; requests of other built plans with the same dtype and flags
 // join the batch (up to eight plans), which runs as one work-queue gather
-// (dg_multi: a persistent grid over (plan, unit) items, replayed as a CUDA
-// graph). Four workers run batches concurrently on their own streams, so one
-// batch's copies overlap another's gather; their staging grows stream-ordered
-// and is kept. max_coalesce 1 serves one request per launch on the plan's own
-// tuned lane mapping (the plain path). Plans live in an HBM cache bounded by
-// bytes and are managed by two builder threads: a request for a plan that is
-// not built asks a builder and stays queued while the workers serve other
-// plans; the builder builds the plan on the device, tunes it once per key
-// for small launches, allocates its partial sums for the largest launch,
-// admits it by evicting least-recently-used plans that no worker is using,
-// and destroys evicted and stale plans, so no worker ever waits for a build
-// or a free. A submit copies its frame into a pooled pinned buffer outside
-// the server lock (or borrows the caller's); the worker copies the pinned
-// buffers straight to the device, and each request's results straight back
-// into a pooled pinned buffer that dg_server_poll copies out and returns. Re-registering a key (a changed PONI)
-// gives it a new generation: the next request rebuilds the plan, and the
-// stale plan is destroyed once no worker uses it. A build that fails fails
-// the requests of that generation. Each request's result is identical alone
-// and in any mix: the gather's arithmetic depends only on the plan, never on
-// which frames or plans share a launch.
+// (dg_multi: a persistent grid of row-warp CTAs over (plan, row item) items,
+// replayed as a CUDA graph, no partial sums). Four workers run batches
+// concurrently on their own streams, so one batch's copies overlap another's
+// gather; their staging grows stream-ordered and is kept. max_coalesce 1
+// serves one request per launch on the plan's own lane mapping, tuned for
+// one frame (the plain path). Plans live in an HBM cache bounded by bytes
+// and are managed by two builder threads: a request for a plan that is not
+// built asks a builder and stays queued while the workers serve other plans;
+// the builder builds the plan on the device (for the plain path also tunes
+// it once per key and allocates its partial sums), admits it by evicting
+// least-recently-used plans that no worker is using, and destroys evicted
+// and stale plans, so no worker ever waits for a build or a free. A submit
+// copies its frame into a pooled pinned buffer outside the server lock (or
+// borrows the caller's); the worker copies the pinned buffers straight to the
+// device, and each request's results straight back into a pooled pinned
+// buffer that dg_server_poll copies out and returns. Re-registering a key (a
+// changed PONI) gives it a new generation: the next request rebuilds the
+// plan, and the stale plan is destroyed once no worker uses it. A build that
+// fails fails the requests of that generation. Each request's result is
+// identical alone and in any mix: the gather's arithmetic depends only on the
+// plan, never on which frames or plans share a launch.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -155,11 +156,11 @@ struct dg_server {
     std::unordered_map<uint64_t, BuildFailure> failed;
     std::unordered_map<uint64_t, int32_t> tuned;  // key -> lane mapping its last plan used
 
-    // A new plan's lane mapping, tuned for the small coalesced launches of the
-    // loop on zero frames of the request's type (timing does not depend on
+    // A new plan's lane mapping for the plain path's one-request launches,
+    // tuned on a zero frame of the request's type (timing does not depend on
     // the values); left at the default if anything fails. Builder thread.
     void tune(dg_plan *plan, int32_t dtype, uint32_t flags) {
-        const int64_t nf = std::max(1, std::min(8, cfg.max_coalesce));
+        const int64_t nf = 1;
         const size_t bytes = size_t(plan->dim1) * plan->dim2 * px_size(dtype) * size_t(nf);
         void *d = nullptr;
         if (cudaMallocAsync(&d, bytes, plan->stream) != cudaSuccess) {
@@ -257,30 +258,30 @@ struct dg_server {
                 cv_work.notify_all();
                 continue;
             }
-            // A rebuilt key (new PONI, same shape and bins) keeps the mapping
-            // its previous plan was tuned to; a new key is tuned once.
-            int32_t known = -1;
-            {
-                std::lock_guard<std::mutex> lock(mu);
-                auto t = tuned.find(key);
-                if (t != tuned.end()) known = t->second;
-            }
-            if (known < 0 || dg_plan_variant(plan, known, nullptr, nullptr) != DG_OK) {
-                tune(plan, hint.first, hint.second);
-                int32_t v = 0;
-                dg_plan_variant(plan, -1, &v, nullptr);
-                std::lock_guard<std::mutex> lock(mu);
-                tuned[key] = v;
-            }
-            // Partial sums for the largest coalesced launch, allocated now
-            // rather than by a worker's first batch (the work-queue gather
-            // sums every plan with partial sums).
-            {
+            // The plain path launches each request on the plan's own lane
+            // mapping: a rebuilt key (new PONI, same shape and bins) keeps the
+            // mapping its previous plan was tuned to, a new key is tuned once,
+            // and partial sums (if the mapping uses any) are allocated now
+            // rather than by a worker's first launch. The coalescing path's
+            // work-queue gather (row warps) needs neither.
+            if (cfg.max_coalesce <= 1) {
+                int32_t known = -1;
+                {
+                    std::lock_guard<std::mutex> lock(mu);
+                    auto t = tuned.find(key);
+                    if (t != tuned.end()) known = t->second;
+                }
+                if (known < 0 || dg_plan_variant(plan, known, nullptr, nullptr) != DG_OK) {
+                    tune(plan, hint.first, hint.second);
+                    int32_t v = 0;
+                    dg_plan_variant(plan, -1, &v, nullptr);
+                    std::lock_guard<std::mutex> lock(mu);
+                    tuned[key] = v;
+                }
                 std::lock_guard<std::mutex> lock(plan->mu);
                 cudaSetDevice(plan->device);
                 try {
-                    dg::reserve_partials(plan->gather, cfg.max_coalesce, hint.second, hint.first,
-                                         cfg.max_coalesce > 1);
+                    dg::reserve_partials(plan->gather, 1, hint.second, hint.first);
                 } catch (const dg::Error &) {
                 }
             }

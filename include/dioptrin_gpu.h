@@ -378,14 +378,17 @@ DG_EXPORT dg_status dg_server_stats_get(dg_server *server, dg_server_stats *out)
  * No counterpart in the reference, whose engine launches one plan at a time
  * (src/integration/cuda/device.rs:1417-1584; streaming driver
  * src/batch/bounded.rs:172). A dg_multi integrates batches of device-resident
- * frames of several plans together: a persistent grid of gather CTAs takes
- * (plan, unit) work items from one counter until every plan's table is
+ * frames of several plans together: a persistent grid of row-warp CTAs takes
+ * (plan, row item) work items from one counter until every plan's table is
  * summed, so plans of very different sizes share the GPU without a launch
- * per plan, and one finalize pass normalises all of them. The device work of
- * a call (descriptor copy, gather, finalize) is a CUDA graph captured on the
- * first call of each (dtype, flags) and replayed after that. Every plan is
- * summed with the entry-lane lane mapping 2, so each item's results equal
- * dg_integrate_device of that plan with mapping 2 selected, bit for bit.
+ * per plan; each row's results are written by the CTA that sums it (no
+ * partial sums, no second pass). The device work of a call (descriptor copy,
+ * gather) is a CUDA graph captured on the first call of each (dtype, flags)
+ * and replayed after that. Every plan is summed as by lane mapping 10, so
+ * each item's results equal dg_integrate_device of that plan with mapping 10
+ * selected, bit for bit. DG_UNSUPPORTED for a table of more than 2^31
+ * entries. Meant for small batches (a frame pass reads the table once per
+ * four frames). No kernel of the call waits on another.
  * Items share one dtype and one set of flags; a plan appears in at most one
  * item of a call; an item carries 0..256 frames. Calls on one dg_multi are
  * serialised (a call waits until the previous one's device work is done

@@ -1,15 +1,15 @@
 """Several plans in one launch: the work-queue gather (dg_multi_integrate).
 
-A persistent grid of gather CTAs claims (plan, unit) items from one counter
-until every plan of the call is summed, then one finalize normalises them
-all; the device work is a CUDA graph captured on the first call and replayed
-after it. Each plan is summed with lane mapping 2, so every item's results
-must equal dg_integrate_device on that plan with mapping 2 selected, bit for
-bit, whatever the other plans of the call and their sizes, on the first
-(captured) call and on replays with other frames and frame counts; and they
-must match the CPU oracle within the parity tolerance. A call whose items
-carry no frames does nothing; bad calls are rejected and leave the plans
-usable."""
+A persistent grid of row-warp CTAs claims (plan, row item) items from one
+counter until every plan of the call is summed, each row's results written by
+the CTA that sums it; the device work is a CUDA graph captured on the first
+call and replayed after it. Each plan is summed as lane mapping 10 sums it, so
+every item's results must equal dg_integrate_device on that plan with mapping
+10 selected, bit for bit, whatever the other plans of the call and their
+sizes, on the first (captured) call and on replays with other frames and frame
+counts (one, two and several frames per pass); and they must match the CPU
+oracle within the parity tolerance. A call whose items carry no frames does
+nothing; bad calls are rejected and leave the plans usable."""
 import ctypes as C
 
 import numpy as np
@@ -93,10 +93,10 @@ def test_multi_equals_each_plan_alone(dg, flags):
     from dioptrin_b200 import _native as N
     plans = _plans(dg)
     for p, _, _, _ in plans:
-        p.gather_variant = 2
+        p.gather_variant = 10
     h = _multi()
     gen = np.random.default_rng(5 + flags)
-    for rnd, counts in enumerate([(5, 70, 3), (33, 1, 64), (0, 9, 2)]):
+    for rnd, counts in enumerate([(5, 70, 3), (33, 1, 64), (0, 9, 2), (1, 2, 1)]):
         frames = [torch.from_numpy(gen.poisson(50.0 + 20 * k, (n,) + shape).astype(np.uint16))
                   .cuda() for k, ((_, shape, _, _), n) in enumerate(zip(plans, counts))]
         items = [(p, f, nb) for (p, _, nb, _), f in zip(plans, frames)]

@@ -498,7 +498,11 @@ __global__ void __launch_bounds__(kThreads)
 // azimuthal.rs:96-104). The spread is shifted by the row's origin as in the
 // other mappings, in FP64: t = s - o*n with n the entry's FP32 pair.
 constexpr int kRowsLong = 512;
-constexpr int kRowsU = 4;
+constexpr int kRowsTiny = 64;  // rows of at most this many entries take 8 lanes
+#ifndef DG_ROWS_U
+#define DG_ROWS_U 4
+#endif
+constexpr int kRowsU = DG_ROWS_U;
 constexpr int kRowsThreads = 256;
 
 template <typename P>
@@ -511,6 +515,12 @@ __device__ __forceinline__ double load_px_d(const P *__restrict__ f, uint32_t i)
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, m));
+    return v;
+}
+// The same over each group of 8 lanes (the warp's four tiny rows).
+__device__ __forceinline__ double group8_sum_d(double v) {
+#pragma unroll
+    for (int m = 4; m > 0; m >>= 1) v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, m));
     return v;
 }
 
@@ -544,11 +554,17 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
     double *__restrict__ out_d = qp.out_d;
     const int2 it = items[k];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool whole = it.y == 0;  // one long row for the whole CTA
-    if (!whole && warp >= it.y) return;  // no CTA-wide barrier in this case
-    const int row = rows[it.x + (whole ? 0 : warp)];
-    const int e0 = row_ptr[row], e1 = row_ptr[row + 1];
-    const int li = whole ? int(threadIdx.x) : lane, nl = whole ? kRowsThreads : 32;
+    // {first, 0}: one long row for the whole CTA; {first, n > 0}: a row per
+    // warp; {first, -n}: tiny rows, 8 lanes each (four per warp).
+    const bool whole = it.y == 0, tiny = it.y < 0;
+    if (!whole && !tiny && warp >= it.y) return;  // no CTA-wide barrier in this case
+    const int sub = int(threadIdx.x) >> 3;
+    if (tiny && (sub & ~3) >= -it.y) return;  // a warp whose four rows are all past the end
+    const bool live = !tiny || sub < -it.y;    // lanes past the end still shuffle
+    const int row = rows[it.x + (whole ? 0 : tiny ? (live ? sub : 0) : warp)];
+    const int e0 = row_ptr[row], e1 = live ? row_ptr[row + 1] : e0;
+    const int li = whole ? int(threadIdx.x) : tiny ? (lane & 7) : lane;
+    const int nl = whole ? kRowsThreads : tiny ? 8 : 32;
     const int org = SPREAD ? origin_entry[row] : -1, fvalid = SPREAD ? first_valid[row] : -1;
     for (int f0 = 0; f0 < n_frames; f0 += F) {
         const P *fr[F];
@@ -621,7 +637,8 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
 #pragma unroll
         for (int q = 0; q < F; ++q)
 #pragma unroll
-            for (int a = 0; a < NA; ++a) acc[q][a] = warp_sum_d(acc[q][a]);
+            for (int a = 0; a < NA; ++a)
+                acc[q][a] = tiny ? group8_sum_d(acc[q][a]) : warp_sum_d(acc[q][a]);
         if (whole) {
             if (lane == 0)
 #pragma unroll
@@ -640,7 +657,7 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
                     }
             __syncthreads();  // s_red is rewritten by the next frames
             if (threadIdx.x != 0) continue;
-        } else if (lane != 0) {
+        } else if (tiny ? ((lane & 7) != 0 || !live) : lane != 0) {
             continue;
         }
 #pragma unroll
@@ -771,6 +788,23 @@ using StagedPx = typename std::conditional<sizeof(P) == 4, P, float>::type;
 __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+// The same with the shared-memory address as a 32-bit integer, and a 32-bit
+// shared-memory load: address arithmetic stays in 32 bits.
+__device__ __forceinline__ void cp_async4_s(unsigned d, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ uint32_t lds32(unsigned a) {
+    uint32_t v;
+    asm volatile("ld.shared.b32 %0, [%1];\n" : "=r"(v) : "r"(a));
+    return v;
+}
+// A staged 4-byte pixel from its bits.
+template <typename S>
+__device__ __forceinline__ float staged_value(uint32_t b) {
+    if constexpr (std::is_same<S, float>::value) return __uint_as_float(b);
+    else if constexpr (std::is_same<S, int32_t>::value) return float(int32_t(b));
+    else return float(b);
 }
 
 // Packed FP32x2 arithmetic (round to nearest, per element as the scalar
@@ -1397,6 +1431,11 @@ struct BtCfg {
 #ifndef DG_BT_PAIRED
 #define DG_BT_PAIRED 0
 #endif
+// Shared-memory addresses of the bin tiles' pixel copies and pixel loads
+// kept as 32-bit integers (1) or left to the compiler (0).
+#ifndef DG_BT_SADDR
+#define DG_BT_SADDR 1
+#endif
 // Bin tiles run largest first (1) or in bin order (0).
 #ifndef DG_BT_LARGEST_FIRST
 #define DG_BT_LARGEST_FIRST 1
@@ -1642,9 +1681,17 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 const int f = fw + j * FSTEP;
                 if (f >= nv) break;
                 const P *fsrc = base + int64_t(j * FSTEP) * n_pixels;
+#if DG_BT_SADDR
+                const unsigned drow = smem_addr(dst + pxi(f, s0 + lane));
+                constexpr unsigned kStep = 4u * (PAIRED ? 64u : 32u);  // 32 slots on
+#pragma unroll
+                for (int i = 0; i < KSTEP; ++i)
+                    if (kin[i]) cp_async4_s(drow + kStep * unsigned(i), fsrc + idx[i]);
+#else
 #pragma unroll
                 for (int i = 0; i < KSTEP; ++i)
                     if (kin[i]) cp_async4(dst + pxi(f, s0 + lane + 32 * i), fsrc + idx[i]);
+#endif
             }
         } else {
             for (int k = s0 + lane; k < k1; k += 32) {
@@ -1774,8 +1821,12 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             continue;
         }
         const S *px[F2];
+        unsigned pxa[F2];  // the same as 32-bit shared-memory addresses
 #pragma unroll
-        for (int h = 0; h < F2; ++h) px[h] = pxbuf(b) + pxi(lane + 32 * h, 0);
+        for (int h = 0; h < F2; ++h) {
+            px[h] = pxbuf(b) + pxi(lane + 32 * h, 0);
+            pxa[h] = smem_addr(px[h]);
+        }
         const float4 *s_pa = pabuf(b);
         const float4 *s_pb = s_pa + PCAP;
         const f2 *s_pc = pcbuf(b);
@@ -1809,6 +1860,16 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                     vv1[0][u] = float(b2.x);
                     vv1[F2 - 1][u] = float(b2.y);
                 }
+            } else if constexpr (DG_BT_SADDR && MODE != kRaw) {
+#pragma unroll
+                for (int h = 0; h < F2; ++h)
+#pragma unroll
+                    for (int u = 0; u < UU; ++u) {
+                        vv0[h][u] = staged_value<S>(
+                            lds32(pxa[h] + 4u * unsigned(__float_as_int(ea[u].x))));
+                        vv1[h][u] = staged_value<S>(
+                            lds32(pxa[h] + 4u * unsigned(__float_as_int(ea[u].y))));
+                    }
             } else {
 #pragma unroll
                 for (int h = 0; h < F2; ++h)
@@ -2891,12 +2952,19 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
             return rp[size_t(a) + 1] - rp[size_t(a)] > rp[size_t(b) + 1] - rp[size_t(b)];
         });
         for (size_t i = 0; i < rw_rows.size(); ++i) rw_items.push_back(make_int2(int(i), 0));
-        const size_t first_short = rw_rows.size();
+        auto len = [&](int64_t r) { return rp[size_t(r) + 1] - rp[size_t(r)]; };
+        const size_t first_mid = rw_rows.size();
         for (int64_t r = 0; r < nb; ++r)
-            if (rp[size_t(r) + 1] - rp[size_t(r)] <= kRowsLong) rw_rows.push_back(int32_t(r));
-        for (size_t i = first_short; i < rw_rows.size(); i += kRowsThreads / 32)
-            rw_items.push_back(make_int2(int(i), int(std::min<size_t>(kRowsThreads / 32,
+            if (len(r) <= kRowsLong && len(r) > kRowsTiny) rw_rows.push_back(int32_t(r));
+        for (size_t i = first_mid; i < rw_rows.size(); i += kRowsWarps)
+            rw_items.push_back(make_int2(int(i), int(std::min<size_t>(kRowsWarps,
                                                                       rw_rows.size() - i))));
+        const size_t first_tiny = rw_rows.size();
+        for (int64_t r = 0; r < nb; ++r)
+            if (len(r) <= kRowsTiny) rw_rows.push_back(int32_t(r));
+        for (size_t i = first_tiny; i < rw_rows.size(); i += 4 * kRowsWarps)
+            rw_items.push_back(make_int2(int(i), -int(std::min<size_t>(4 * kRowsWarps,
+                                                                       rw_rows.size() - i))));
         out.rw_row_ptr.alloc(rw_ptr.size());
         out.rw_rows.alloc(rw_rows.size());
         out.rw_item.alloc(rw_items.size());

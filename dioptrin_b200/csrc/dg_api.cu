@@ -185,7 +185,8 @@ int64_t dg_plan::device_bytes() const {
          gather.fl_pair_c.bytes() +
          gather.fl_pair_s.bytes() + gather.fl_seg_org.bytes() + gather.entry_raw.bytes() +
          gather.cnt.bytes() + gather.bt[0].bytes() + gather.bt[1].bytes() +
-         gather.rw_row_ptr.bytes() + gather.rw_rows.bytes() + gather.rw_item.bytes();
+         gather.rw_row_ptr.bytes() + gather.rw_rows.bytes() + gather.rw_item.bytes() +
+         gather.px_norm.bytes();
     b += stage_in.bytes() + stage_out.bytes() + stage_comp.bytes() + stage_desc.bytes() +
          stage_mask.bytes();
     return b;

@@ -531,7 +531,7 @@ using RowsRed = double[kRowsWarps][4 * kMaxAcc];
 // One row-warp item of a plan's batch (q.item[k]); every thread of the CTA
 // calls it. F frames per pass over the entries.
 template <int MODE, typename P, int F>
-__device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s_red) {
+__device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, RowsRed &s_red) {
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
     constexpr int NW = kRowsWarps;
@@ -540,7 +540,7 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
     const int32_t *__restrict__ row_ptr = qp.row_ptr;
     const int2 *__restrict__ entry = qp.entry;
     const float4 *__restrict__ entry_std = qp.entry_std;
-    const float *__restrict__ entry_nlo = qp.entry_nlo;
+    const float2 *__restrict__ px_norm = qp.px_norm;
     const int32_t *__restrict__ first_valid = qp.first_valid;
     const int32_t *__restrict__ origin_entry = qp.origin;
     const double *__restrict__ den = qp.den;
@@ -566,7 +566,8 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
     const int li = whole ? int(threadIdx.x) : tiny ? (lane & 7) : lane;
     const int nl = whole ? kRowsThreads : tiny ? 8 : 32;
     const int org = SPREAD ? origin_entry[row] : -1, fvalid = SPREAD ? first_valid[row] : -1;
-    for (int f0 = 0; f0 < n_frames; f0 += F) {
+    // frames [F*fb, F*fb + F) of the batch, one pass
+    for (int f0 = F * fb; f0 < n_frames && f0 < F * fb + F; f0 += F) {
         const P *fr[F];
 #pragma unroll
         for (int q = 0; q < F; ++q) fr[q] = frames + int64_t(min(f0 + q, n_frames - 1)) * n_pixels;
@@ -580,23 +581,16 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
 #pragma unroll
             for (int a = 0; a < NA; ++a) acc[q][a] = 0.0;
         for (int j0 = e0 + li; j0 < e1; j0 += nl * kRowsU) {
-            float4 es[kRowsU];
-            float nlo[kRowsU];
+            float2 nn[kRowsU];
             int2 en[kRowsU];
             double x[kRowsU][F];
 #pragma unroll
             for (int u = 0; u < kRowsU; ++u) {
                 const int j = j0 + nl * u;
                 const bool in = j < e1;
-                uint32_t col = 0;
-                if constexpr (SPREAD) {
-                    es[u] = in ? entry_std[j] : make_float4(0.f, 0.f, 1.f, 0.f);
-                    nlo[u] = in ? entry_nlo[j] : 0.f;
-                    col = uint32_t(__float_as_int(es[u].x));
-                } else {
-                    en[u] = in ? entry[j] : make_int2(0, 0);
-                    col = uint32_t(en[u].x);
-                }
+                en[u] = in ? entry[j] : make_int2(0, 0);
+                const uint32_t col = uint32_t(en[u].x);
+                if constexpr (SPREAD) nn[u] = in ? px_norm[col] : make_float2(0.f, 0.f);
 #pragma unroll
                 for (int q = 0; q < F; ++q) x[u][q] = in ? load_px_d<P>(fr[q], col) : 0.0;
             }
@@ -604,8 +598,14 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
             for (int u = 0; u < kRowsU; ++u) {
                 if (j0 + nl * u >= e1) break;
                 if constexpr (SPREAD) {
-                    const double c = es[u].y, cr = es[u].w;
-                    const double n = __dadd_rn(double(es[u].z), double(nlo[u]));
+                    // valid for the spread (azimuthal.rs:62-75): c > 0 and n
+                    // finite and > 0 ({0, 0} marks an invalid n); an invalid
+                    // entry adds nothing
+                    const float cf = __int_as_float(en[u].y);
+                    const bool ok = nn[u].x > 0.f && cf > 0.f && cf <= 3.40282347e+38f;
+                    const double c = ok ? double(cf) : 0.0;
+                    const double cr = ok ? double(__fdiv_rn(cf, nn[u].x)) : 0.0;
+                    const double n = ok ? __dadd_rn(double(nn[u].x), double(nn[u].y)) : 1.0;
                     const double c2 = __dmul_rn(c, c);
 #pragma unroll
                     for (int q = 0; q < F; ++q) {
@@ -697,21 +697,21 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, RowsRed &s
     }
 }
 
-// Lane mapping 10 for one plan's batch: one CTA per item.
+// Lane mapping 10 for one plan's batch: one CTA per (item, frame block).
 template <int MODE, typename P, int F>
 __global__ void __launch_bounds__(kRowsThreads) k_rows(const QueuePlan q) {
     __shared__ RowsRed s_red;
-    rows_item<MODE, P, F>(q, blockIdx.x, s_red);
+    rows_item<MODE, P, F>(q, blockIdx.x, blockIdx.y, s_red);
 }
 
-// Frames per pass of a row-warp launch of nf frames: one pass for up to
-// four frames.
+// Frames per pass (and per frame block) of a row-warp launch of nf frames.
 __host__ __device__ constexpr int rows_pass_frames(int nf) { return nf <= 1 ? 1 : nf <= 2 ? 2 : 4; }
 
 // Work-queue gather over several plans (dg_multi_integrate). A persistent
-// grid of row-warp CTAs claims (plan, item) items from one counter until
-// every plan's items are summed, so plans of very different sizes share one
-// launch and the GPU stays full to the last item. A plan's results are those
+// grid of row-warp CTAs claims (plan, row item, frame block) tiles from one
+// counter until every plan's tiles are summed, so plans of very different
+// sizes and batch sizes share one launch and the GPU stays full to the last
+// tile. A plan's results are those
 // of lane mapping 10 launched for that plan alone, bit for bit. No CTA waits
 // on another: a claim is one atomic add, and a CTA that finds the counter
 // past the end returns.
@@ -736,11 +736,14 @@ __global__ void __launch_bounds__(kRowsThreads)
             else hi = mid - 1;
         }
         const QueuePlan &q = plans[lo];
-        const int k = item - q.item_first;
+        // (row item, frame block) tiles of the plan, the frame blocks of an
+        // item one after another (its entries are still in L2 for the next)
+        const int local = item - q.item_first;
+        const int k = local / q.frame_blocks, fb = local - k * q.frame_blocks;
         switch (rows_pass_frames(q.n_frames)) {
-        case 1: rows_item<MODE, P, 1>(q, k, s_red); break;
-        case 2: rows_item<MODE, P, 2>(q, k, s_red); break;
-        default: rows_item<MODE, P, 4>(q, k, s_red); break;
+        case 1: rows_item<MODE, P, 1>(q, k, fb, s_red); break;
+        case 2: rows_item<MODE, P, 2>(q, k, fb, s_red); break;
+        default: rows_item<MODE, P, 4>(q, k, fb, s_red); break;
         }
     }
 }
@@ -2269,6 +2272,25 @@ __global__ void k_pack_raw(const int64_t *__restrict__ row_ptr, int n_rows,
 // its first valid entry and its origin entry (the heaviest valid, row_origin).
 // The spread's n is stored as the pair (n_hi, n_lo): n_hi = FP32(n) in
 // entry_std, n_lo = FP32(n - n_hi) in entry_nlo.
+// Per-pixel norm as an FP32 pair for the row warps' spread, at frame
+// storage index i: the detector pixel itself, or, for frames stored bottom row
+// first (rows > 0), the pixel of the mirrored row.
+__global__ void k_px_norm(const double *__restrict__ norm, int64_t n_px, int rows, int cols,
+                          float2 *__restrict__ out) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_px;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        int64_t j = i;
+        if (rows > 0) {
+            const int64_t r = i / cols;
+            j = (rows - 1 - r) * cols + (i - r * cols);
+        }
+        const double n = norm[j];
+        const bool ok = isfinite(n) && n > 0.0;
+        const float hi = ok ? __double2float_rn(n) : 0.f;
+        out[i] = make_float2(hi, ok ? __double2float_rn(n - double(hi)) : 0.f);
+    }
+}
+
 __global__ void k_pack(const int64_t *__restrict__ row_ptr, int n_rows,
                        const int32_t *__restrict__ col, const double *__restrict__ w,
                        const double *__restrict__ norm, int2 *__restrict__ entry,
@@ -2362,13 +2384,14 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
         t.withhold_test, t.cnt.ptr, oc, raw, masks, mask_stride);
 }
 
-// Row warps (mapping 10): F frames per pass over a row's entries, so a
-// launch of up to four frames reads every entry once.
+// Row warps (mapping 10): F frames per pass over a row's entries, one CTA
+// per (row item, block of F frames), so a launch of up to four frames reads
+// every entry once and a larger one once per four frames.
 template <int MODE, typename P>
 void launch_rows(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, double *oi,
                  double *os, double *od, cudaStream_t s) {
     const QueuePlan q = queue_plan(t, fp, n_pixels, nf, oi, os, od);
-    const unsigned grid = unsigned(q.n_items);
+    const dim3 grid(unsigned(q.n_items), unsigned(q.frame_blocks));
     switch (rows_pass_frames(nf)) {
     case 1: k_rows<MODE, P, 1><<<grid, kRowsThreads, 0, s>>>(q); break;
     case 2: k_rows<MODE, P, 2><<<grid, kRowsThreads, 0, s>>>(q); break;
@@ -2860,6 +2883,11 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     out.first_valid.alloc(size_t(table.n_rows));
     out.origin.alloc(size_t(table.n_rows));
     denominators(table, d_norm, s, out.den.ptr);
+    const int64_t n_px = int64_t(dim1) * dim2;
+    out.px_norm.alloc(size_t(std::max<int64_t>(n_px, 1)));
+    if (n_px > 0)
+        k_px_norm<<<unsigned(std::min<int64_t>((n_px + 255) / 256, 148 * 16)), 256, 0, s>>>(
+            d_norm, n_px, 0, 0, out.px_norm.ptr);
     const unsigned rb = unsigned((table.n_rows + 127) / 128);
     if (table.n_rows > 0)
         k_pack<<<rb, 128, 0, s>>>(table.row_ptr.ptr, int(table.n_rows), table.col.ptr, table.w.ptr,
@@ -3007,6 +3035,7 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
     q.entry = t.entry.ptr;
     q.entry_std = t.entry_std.ptr;
     q.entry_nlo = t.entry_nlo.ptr;
+    q.px_norm = t.px_norm.ptr;
     q.first_valid = t.first_valid.ptr;
     q.origin = t.origin.ptr;
     q.den = t.den.ptr;
@@ -3020,6 +3049,8 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
     q.n_frames = n_frames;
     q.n_rows = t.n_rows;
     q.n_items = n_frames > 0 ? t.rw_n_items : 0;
+    q.frame_blocks = std::max(1, (n_frames + rows_pass_frames(n_frames) - 1) /
+                                     rows_pass_frames(n_frames));
     return q;
 }
 
@@ -3148,6 +3179,19 @@ void run_gather(GatherTable &t, const void *d_frames, int dtype, int64_t n_pixel
 
 namespace {
 
+// Swaps detector rows r and rows - 1 - r of a per-pixel array.
+__global__ void k_flip_px_norm(float2 *__restrict__ a, int rows, int cols) {
+    const int64_t half = int64_t(rows / 2) * cols;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < half;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = i / cols, c = i - r * cols;
+        const int64_t j = (rows - 1 - r) * cols + c;
+        const float2 t = a[i];
+        a[i] = a[j];
+        a[j] = t;
+    }
+}
+
 // Row flip of a pixel index for frames stored bottom row first.
 __device__ __forceinline__ int32_t flip_px(int32_t j, int rows, int cols) {
     const int32_t r = j / cols, c = j - r * cols;
@@ -3189,6 +3233,11 @@ __global__ void k_flip_meta(int32_t *__restrict__ meta, int64_t n_rec, int words
 void flip_gather_rows(GatherTable &t, int32_t dim1, int32_t dim2, cudaStream_t s) {
     t.flip_rows = dim1;
     t.flip_cols = dim2;
+    // per-pixel norms to frame storage order: rows r and dim1 - 1 - r swapped
+    const int64_t half = int64_t(dim1 / 2) * dim2;
+    if (t.px_norm.ptr && half > 0)
+        k_flip_px_norm<<<unsigned(std::min<int64_t>((half + 255) / 256, 148 * 16)), 256, 0, s>>>(
+            t.px_norm.ptr, dim1, dim2);
     const int64_t n_px = t.fl_px.ptr ? int64_t(t.fl_px.count) : 0;
     if (t.nnz + n_px > 0)
         k_flip_rows<<<148 * 8, 256, 0, s>>>(t.entry.ptr, t.entry_std.ptr, t.nnz, t.fl_px.ptr,

@@ -305,6 +305,10 @@ struct GatherTable {
     // CTA: {first row in rw_rows, 0} for a long row, {first, count <= 8} for
     // short rows taken one per warp.
     int32_t rw_n_items = 0;
+    // Per pixel (frame storage order) its norm n as an FP32 pair {n, n - n32},
+    // {0, 0} where n is not finite or not positive: the row warps' spread
+    // reads the 8-byte entries and gathers n beside the pixel.
+    DeviceArray<float2> px_norm;
     DeviceArray<int32_t> rw_row_ptr;
     DeviceArray<int32_t> rw_rows;
     DeviceArray<int2> rw_item;
@@ -344,9 +348,9 @@ void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtyp
 // Row warps (k_rows, lane mapping 10) over one plan's batch, and the
 // work-queue gather over several plans (dg_multi.cu, dg_gather.cu): one
 // descriptor per (plan, batch of frames), after a header. The queue's
-// persistent CTAs claim (plan, row item) items from `counter` until
-// total_items are done; item_first is the prefix index of a plan's first
-// item.
+// persistent CTAs claim (plan, row item, frame block) tiles from `counter`
+// until total_items are done; item_first is the prefix index of a plan's
+// first tile.
 struct QueuePlan {
     const int2 *item;
     const int32_t *rows;
@@ -354,6 +358,7 @@ struct QueuePlan {
     const int2 *entry;
     const float4 *entry_std;
     const float *entry_nlo;
+    const float2 *px_norm;
     const int32_t *first_valid;
     const int32_t *origin;
     const double *den;
@@ -362,7 +367,11 @@ struct QueuePlan {
     const void *frames;
     double *out_i, *out_s, *out_d;
     int64_t n_pixels;
-    int32_t n_frames, n_rows, n_items, item_first;
+    int32_t n_frames, n_rows;
+    int32_t n_items;       // row items
+    int32_t frame_blocks;  // blocks of up to four frames (one pass each)
+    int32_t item_first;    // the work queue: first (item, frame block) tile
+    int32_t pad;
 };
 struct QueueHeader {
     int32_t n_plans, total_items, counter, pad;  // counter: 0 before each launch

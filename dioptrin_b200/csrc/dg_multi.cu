@@ -4,8 +4,8 @@
 // QueuePlan per plan batch) and, per pixel type and output set, a CUDA graph
 // of the call's device work: the copy of the descriptors from page-locked
 // host staging and the work-queue gather (a persistent grid of row-warp CTAs
-// that claim (plan, row item) items from a counter the copy resets and write
-// each row's results themselves). The graph is captured on the first call of
+// that claim (plan, row item, block of four frames) tiles from a counter the
+// copy resets and write each row's results themselves). The graph is captured on the first call of
 // its kind and replayed after that, the descriptors changing between calls
 // while the graph stays the same: one graph launch per batch of plans,
 // whatever their number and sizes. No plan scratch is used, so calls on
@@ -14,6 +14,7 @@
 // pipelined tiles (src/integration/cuda/device.rs:1417-1584) keep one plan
 // per launch.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -193,7 +194,9 @@ dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items, int32_
             if (q.n_items <= 0 && t.n_rows > 0)
                 fail(DG_UNSUPPORTED, "the work-queue gather needs a table of at most 2^31 entries");
             q.item_first = items_total;
-            items_total += q.n_items;
+            const int64_t tiles = int64_t(q.n_items) * q.frame_blocks;
+            if (items_total + tiles > INT32_MAX) fail(DG_UNSUPPORTED, "too many tiles for one launch");
+            items_total += int32_t(tiles);
             desc[n++] = q;
         }
         if (n == 0) return;

@@ -379,8 +379,8 @@ DG_EXPORT dg_status dg_server_stats_get(dg_server *server, dg_server_stats *out)
  * (src/integration/cuda/device.rs:1417-1584; streaming driver
  * src/batch/bounded.rs:172). A dg_multi integrates batches of device-resident
  * frames of several plans together: a persistent grid of row-warp CTAs takes
- * (plan, row item) work items from one counter until every plan's table is
- * summed, so plans of very different sizes share the GPU without a launch
+ * (plan, row item, block of four frames) tiles from one counter until every
+ * plan's table is summed, so plans of very different sizes share the GPU without a launch
  * per plan; each row's results are written by the CTA that sums it (no
  * partial sums, no second pass). The device work of a call (descriptor copy,
  * gather) is a CUDA graph captured on the first call of each (dtype, flags)

@@ -707,6 +707,9 @@ __global__ void __launch_bounds__(kRowsThreads) k_rows(const QueuePlan q) {
 // Frames per pass (and per frame block) of a row-warp launch of nf frames.
 __host__ __device__ constexpr int rows_pass_frames(int nf) { return nf <= 1 ? 1 : nf <= 2 ? 2 : 4; }
 
+// Tiles a work-queue CTA claims at once (one atomic add per claim).
+constexpr int kQueueClaim = 4;
+
 // Work-queue gather over several plans (dg_multi_integrate). A persistent
 // grid of row-warp CTAs claims (plan, row item, frame block) tiles from one
 // counter until every plan's tiles are summed, so plans of very different
@@ -722,28 +725,33 @@ __global__ void __launch_bounds__(kRowsThreads)
     __shared__ int s_item;
     const int n_plans = hdr->n_plans, total = hdr->total_items;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, 1);
+        if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, kQueueClaim);
         __syncthreads();
-        const int item = s_item;
+        const int first = s_item;
         __syncthreads();  // every thread has read s_item before it is claimed again
-        if (item >= total) return;
-        // the last descriptor whose first item is at most `item` (plans with
-        // no items share the next one's prefix and are skipped)
+        if (first >= total) return;
+        // the last descriptor whose first tile is at most `first` (plans with
+        // no tiles share the next one's prefix and are skipped)
         int lo = 0, hi = n_plans - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (plans[mid].item_first <= item) lo = mid;
+            if (plans[mid].item_first <= first) lo = mid;
             else hi = mid - 1;
         }
-        const QueuePlan &q = plans[lo];
-        // (row item, frame block) tiles of the plan, the frame blocks of an
-        // item one after another (its entries are still in L2 for the next)
-        const int local = item - q.item_first;
-        const int k = local / q.frame_blocks, fb = local - k * q.frame_blocks;
-        switch (rows_pass_frames(q.n_frames)) {
-        case 1: rows_item<MODE, P, 1>(q, k, fb, s_red); break;
-        case 2: rows_item<MODE, P, 2>(q, k, fb, s_red); break;
-        default: rows_item<MODE, P, 4>(q, k, fb, s_red); break;
+        const int last = min(first + kQueueClaim, total);
+        for (int item = first; item < last; ++item) {
+            while (lo + 1 < n_plans && plans[lo + 1].item_first <= item) ++lo;
+            const QueuePlan &q = plans[lo];
+            // (row item, frame block) tiles of the plan, the frame blocks of
+            // an item one after another (its entries are still in L2 for the
+            // next)
+            const int local = item - q.item_first;
+            const int k = local / q.frame_blocks, fb = local - k * q.frame_blocks;
+            switch (rows_pass_frames(q.n_frames)) {
+            case 1: rows_item<MODE, P, 1>(q, k, fb, s_red); break;
+            case 2: rows_item<MODE, P, 2>(q, k, fb, s_red); break;
+            default: rows_item<MODE, P, 4>(q, k, fb, s_red); break;
+            }
         }
     }
 }

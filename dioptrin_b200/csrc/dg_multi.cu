@@ -195,7 +195,8 @@ dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items, int32_
                 fail(DG_UNSUPPORTED, "the work-queue gather needs a table of at most 2^31 entries");
             q.item_first = items_total;
             const int64_t tiles = int64_t(q.n_items) * q.frame_blocks;
-            if (items_total + tiles > INT32_MAX) fail(DG_UNSUPPORTED, "too many tiles for one launch");
+            if (items_total + tiles > INT32_MAX / 2)
+                fail(DG_UNSUPPORTED, "too many tiles for one launch");
             items_total += int32_t(tiles);
             desc[n++] = q;
         }

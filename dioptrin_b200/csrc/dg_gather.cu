@@ -566,8 +566,20 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
     const int li = whole ? int(threadIdx.x) : tiny ? (lane & 7) : lane;
     const int nl = whole ? kRowsThreads : tiny ? 8 : 32;
     const int org = SPREAD ? origin_entry[row] : -1, fvalid = SPREAD ? first_valid[row] : -1;
+    // The entries of a step are loaded one step ahead (software pipelined), so
+    // a step's pixel gathers and the next step's entry loads are in flight
+    // together; the first step's entries go out before the origin's loads.
+    auto load_entries = [&](int j0, int2 (&en)[kRowsU]) {
+#pragma unroll
+        for (int u = 0; u < kRowsU; ++u) {
+            const int j = j0 + nl * u;
+            en[u] = j < e1 ? entry[j] : make_int2(0, 0);
+        }
+    };
     // frames [F*fb, F*fb + F) of the batch, one pass
     for (int f0 = F * fb; f0 < n_frames && f0 < F * fb + F; f0 += F) {
+        int2 en[kRowsU];
+        load_entries(e0 + li, en);
         const P *fr[F];
 #pragma unroll
         for (int q = 0; q < F; ++q) fr[q] = frames + int64_t(min(f0 + q, n_frames - 1)) * n_pixels;
@@ -582,18 +594,17 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
             for (int a = 0; a < NA; ++a) acc[q][a] = 0.0;
         for (int j0 = e0 + li; j0 < e1; j0 += nl * kRowsU) {
             float2 nn[kRowsU];
-            int2 en[kRowsU];
             double x[kRowsU][F];
 #pragma unroll
             for (int u = 0; u < kRowsU; ++u) {
-                const int j = j0 + nl * u;
-                const bool in = j < e1;
-                en[u] = in ? entry[j] : make_int2(0, 0);
+                const bool in = j0 + nl * u < e1;
                 const uint32_t col = uint32_t(en[u].x);
                 if constexpr (SPREAD) nn[u] = in ? px_norm[col] : make_float2(0.f, 0.f);
 #pragma unroll
                 for (int q = 0; q < F; ++q) x[u][q] = in ? load_px_d<P>(fr[q], col) : 0.0;
             }
+            int2 nx[kRowsU];
+            load_entries(j0 + nl * kRowsU, nx);
 #pragma unroll
             for (int u = 0; u < kRowsU; ++u) {
                 if (j0 + nl * u >= e1) break;
@@ -633,6 +644,8 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
                     }
                 }
             }
+#pragma unroll
+            for (int u = 0; u < kRowsU; ++u) en[u] = nx[u];
         }
 #pragma unroll
         for (int q = 0; q < F; ++q)
@@ -3064,8 +3077,13 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
 
 namespace {
 
-// Persistent grid of the work-queue gather: the CTAs one SM holds at once,
-// times the SMs (the CTAs then stay resident and claim items to the end).
+// Persistent grid of the work-queue gather: kQueueCtasPerSm CTAs per SM
+// (the CTAs stay resident and claim tiles to the end). Fewer than an SM
+// holds, so that the queues of several request-loop workers, and plan builds,
+// run beside each other rather than one after another.
+#ifndef DG_QUEUE_CTAS_PER_SM
+#define DG_QUEUE_CTAS_PER_SM 1
+#endif
 template <int MODE, typename P>
 int queue_gather_grid() {
     static int grid = 0;
@@ -3075,7 +3093,7 @@ int queue_gather_grid() {
                                                               kRowsThreads, 0));
         DG_CUDA(cudaGetDevice(&dev));
         DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        grid = std::max(1, per_sm) * std::max(1, sms);
+        grid = std::max(1, std::min(per_sm, DG_QUEUE_CTAS_PER_SM)) * std::max(1, sms);
     }
     return grid;
 }

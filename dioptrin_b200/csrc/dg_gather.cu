@@ -566,20 +566,8 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
     const int li = whole ? int(threadIdx.x) : tiny ? (lane & 7) : lane;
     const int nl = whole ? kRowsThreads : tiny ? 8 : 32;
     const int org = SPREAD ? origin_entry[row] : -1, fvalid = SPREAD ? first_valid[row] : -1;
-    // The entries of a step are loaded one step ahead (software pipelined), so
-    // a step's pixel gathers and the next step's entry loads are in flight
-    // together; the first step's entries go out before the origin's loads.
-    auto load_entries = [&](int j0, int2 (&en)[kRowsU]) {
-#pragma unroll
-        for (int u = 0; u < kRowsU; ++u) {
-            const int j = j0 + nl * u;
-            en[u] = j < e1 ? entry[j] : make_int2(0, 0);
-        }
-    };
     // frames [F*fb, F*fb + F) of the batch, one pass
     for (int f0 = F * fb; f0 < n_frames && f0 < F * fb + F; f0 += F) {
-        int2 en[kRowsU];
-        load_entries(e0 + li, en);
         const P *fr[F];
 #pragma unroll
         for (int q = 0; q < F; ++q) fr[q] = frames + int64_t(min(f0 + q, n_frames - 1)) * n_pixels;
@@ -594,17 +582,18 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
             for (int a = 0; a < NA; ++a) acc[q][a] = 0.0;
         for (int j0 = e0 + li; j0 < e1; j0 += nl * kRowsU) {
             float2 nn[kRowsU];
+            int2 en[kRowsU];
             double x[kRowsU][F];
 #pragma unroll
             for (int u = 0; u < kRowsU; ++u) {
-                const bool in = j0 + nl * u < e1;
+                const int j = j0 + nl * u;
+                const bool in = j < e1;
+                en[u] = in ? entry[j] : make_int2(0, 0);
                 const uint32_t col = uint32_t(en[u].x);
                 if constexpr (SPREAD) nn[u] = in ? px_norm[col] : make_float2(0.f, 0.f);
 #pragma unroll
                 for (int q = 0; q < F; ++q) x[u][q] = in ? load_px_d<P>(fr[q], col) : 0.0;
             }
-            int2 nx[kRowsU];
-            load_entries(j0 + nl * kRowsU, nx);
 #pragma unroll
             for (int u = 0; u < kRowsU; ++u) {
                 if (j0 + nl * u >= e1) break;
@@ -644,8 +633,6 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
                     }
                 }
             }
-#pragma unroll
-            for (int u = 0; u < kRowsU; ++u) en[u] = nx[u];
         }
 #pragma unroll
         for (int q = 0; q < F; ++q)
@@ -884,6 +871,24 @@ struct Acc2 {
         return __dadd_rn(double(h.x) + double(l.x), double(h.y) + double(l.y));
     }
 };
+
+// The same packed partial folded into one FP64 sum instead (both halves
+// added in FP64, even then odd): four registers instead of six.
+struct AccP64 {
+    f2 p;
+    double d;
+    __device__ __forceinline__ void zero() {
+        p = 0ull;
+        d = 0.0;
+    }
+    __device__ __forceinline__ void flush() {
+        const float2 h = upk(p);
+        d = __dadd_rn(__dadd_rn(d, double(h.x)), double(h.y));
+        p = 0ull;
+    }
+    __device__ __forceinline__ double value() const { return d; }
+};
+
 
 // Dynamic shared memory of k_gather_fl: entry pairs, pixel list, one or
 // (double-buffered) two sets of 32 frame rows, piece-boundary slots.
@@ -1460,6 +1465,12 @@ struct BtCfg {
 #ifndef DG_BT_SADDR
 #define DG_BT_SADDR 1
 #endif
+// Bin-tile sums per (row, frame): packed FP32 partials folded into an FP64
+// sum (1) or into double-word FP32 sums (0).
+#ifndef DG_BT_ACC64
+#define DG_BT_ACC64 1
+#endif
+using BtAcc = std::conditional<DG_BT_ACC64 != 0, AccP64, Acc2>::type;
 // Bin tiles run largest first (1) or in bin order (0).
 #ifndef DG_BT_LARGEST_FIRST
 #define DG_BT_LARGEST_FIRST 1
@@ -1657,6 +1668,11 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     constexpr bool DEFER = MODE == kRaw || DEFER_PX;
     S pv[DEFER_PX ? KSTEP : 1][FS];
     // The first of two halves of staging chunk c: mask loads and copies.
+    // The frames this warp stages (4-byte pixels), found once per tile.
+    const P *stage_frame[FS];
+#pragma unroll
+    for (int j = 0; j < FS; ++j)
+        stage_frame[j] = frames + int64_t(f0 + min(warp / KS + j * FSTEP, max(nv - 1, 0))) * n_pixels;
     auto stage_issue = [&](int c) {
         const int b = c % NB;
         const int32_t *mb = mbuf(c);
@@ -1692,26 +1708,30 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
             // This lane's slots s0 + lane + 32 i and their pixel indices, read
             // once; then frame by frame, one address add and one copy per
             // (slot, frame).
-            int idx[KSTEP];
+            uint32_t boff[KSTEP];  // byte offsets of the slots' pixels in a frame
             bool kin[KSTEP];
 #pragma unroll
             for (int i = 0; i < KSTEP; ++i) {
                 const int k = s0 + lane + 32 * i;
                 kin[i] = k < k1;
-                idx[i] = kin[i] ? mb[MH + k] : 0;
+                boff[i] = kin[i] ? uint32_t(mb[MH + k]) * uint32_t(sizeof(P)) : 0u;
             }
 #pragma unroll
             for (int j = 0; j < FS; ++j) {
                 const int f = fw + j * FSTEP;
                 if (f >= nv) break;
-                const P *fsrc = base + int64_t(j * FSTEP) * n_pixels;
 #if DG_BT_SADDR
+                const char *fsrc = reinterpret_cast<const char *>(stage_frame[j]);
                 const unsigned drow = smem_addr(dst + pxi(f, s0 + lane));
                 constexpr unsigned kStep = 4u * (PAIRED ? 64u : 32u);  // 32 slots on
 #pragma unroll
                 for (int i = 0; i < KSTEP; ++i)
-                    if (kin[i]) cp_async4_s(drow + kStep * unsigned(i), fsrc + idx[i]);
+                    if (kin[i]) cp_async4_s(drow + kStep * unsigned(i), fsrc + boff[i]);
 #else
+                const P *fsrc = base + int64_t(j * FSTEP) * n_pixels;
+                int idx[KSTEP];
+#pragma unroll
+                for (int i = 0; i < KSTEP; ++i) idx[i] = int(boff[i] / uint32_t(sizeof(P)));
 #pragma unroll
                 for (int i = 0; i < KSTEP; ++i)
                     if (kin[i]) cp_async4(dst + pxi(f, s0 + lane + 32 * i), fsrc + idx[i]);
@@ -1779,7 +1799,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
 
     // This warp's row: accumulators, fold counter and origin of each of the
     // lane's frames.
-    Acc2 acc[F2][NA];
+    BtAcc acc[F2][NA];
 #pragma unroll
     for (int h = 0; h < F2; ++h)
 #pragma unroll

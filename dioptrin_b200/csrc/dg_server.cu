@@ -2,10 +2,12 @@
 //
 // Requests are admitted while in-flight slots remain (a submit waits, bounded,
 // for a slot). Worker threads take the oldest queued request whose plan is
-// built, coalesce every queued request with the same plan key, dtype and
-// flags behind it (up to max_coalesce) into one launch, and publish results
-// per request; requests of other built plans with the same dtype and flags
-// join the batch (up to eight plans), which runs as one work-queue gather
+// built, coalesce the queued requests with the same plan key, dtype and
+// flags behind it (up to max_coalesce per plan) into one launch, and publish
+// results per request; requests of other built plans with the same dtype and
+// flags join the batch (up to eight plans, and at most a quarter of the queue,
+// so that a backlog spreads over the workers instead of piling into one
+// batch), which runs as one work-queue gather
 // (dg_multi: a persistent grid of row-warp CTAs over (plan, row item) items,
 // replayed as a CUDA graph, no partial sums). Four workers run batches
 // concurrently on their own streams, so one batch's copies overlap another's
@@ -353,6 +355,7 @@ struct dg_server {
         size_t in_off = 0, out_off = 0;
     };
     static constexpr int kPlansPerLaunch = 8;
+    static constexpr int kWorkers = 4;
 
     // The cached plan of `key` if it is built for the current generation,
     // with a user reference taken (lock held).
@@ -414,9 +417,14 @@ struct dg_server {
                     ++it;
                 }
                 if (!groups.empty()) {
-                    // the requests behind it: its plan's, then other built plans'
+                    // the requests behind it: its plan's, then other built
+                    // plans', at most a share of the queue per worker, so
+                    // the other workers' batches overlap this one's copies
+                    // and gather rather than wait for the next backlog
                     const Request *head = groups.front().reqs.front();
-                    for (it = queue.begin(); it != queue.end();) {
+                    const size_t share = (queue.size() + 1 + kWorkers - 1) / kWorkers;
+                    size_t taken = 1;
+                    for (it = queue.begin(); it != queue.end() && taken < share;) {
                         Request *r = *it;
                         if (r->dtype != head->dtype || r->flags != head->flags) {
                             ++it;
@@ -436,6 +444,7 @@ struct dg_server {
                         if (g && int(g->reqs.size()) < cfg.max_coalesce) {
                             g->reqs.push_back(r);
                             it = queue.erase(it);
+                            ++taken;
                         } else {
                             ++it;
                         }
@@ -587,7 +596,8 @@ dg_status dg_server_create(const dg_server_config *config, dg_server **out) {
         return server_fail(DG_INVALID_INPUT, "server limits must be positive");
     auto s = std::make_unique<dg_server>();
     s->cfg = *config;
-    for (int i = 0; i < 4; ++i) s->workers.emplace_back([p = s.get()] { p->worker_main(); });
+    for (int i = 0; i < dg_server::kWorkers; ++i)
+        s->workers.emplace_back([p = s.get()] { p->worker_main(); });
     // two builders: a rebuild of one large plan does not hold up another's
     for (int i = 0; i < 2; ++i) s->builders.emplace_back([p = s.get()] { p->builder_main(); });
     *out = s.release();

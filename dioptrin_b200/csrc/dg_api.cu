@@ -212,7 +212,12 @@ dg_status dg_plan_create(const dg_geometry *geometry, const dg_method *method,
         plan->n_radial = n_radial;
         plan->n_azimuthal = n_azimuthal;
         plan->n_bins = n_azimuthal ? int64_t(n_radial) * n_azimuthal : n_radial;
-        DG_CUDA(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking));
+        // The plan's own stream runs at the device's greatest priority: its
+        // build (and calls that pass no stream) go ahead of other queued work,
+        // e.g. a request loop's persistent gathers.
+        int least = 0, greatest = 0;
+        DG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        DG_CUDA(cudaStreamCreateWithPriority(&plan->stream, cudaStreamNonBlocking, greatest));
         cudaStream_t s = plan->stream;
         cudaEvent_t e0, e1;
         DG_CUDA(cudaEventCreate(&e0));

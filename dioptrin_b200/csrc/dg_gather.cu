@@ -1478,7 +1478,7 @@ using BtAcc = std::conditional<DG_BT_ACC64 != 0, AccP64, Acc2>::type;
 // Pairs of a row summed in plain FP32 (each half of a packed accumulator
 // takes one entry per pair) before they are folded into the double-word sums.
 #ifndef DG_BT_FOLD_PAIRS
-#define DG_BT_FOLD_PAIRS 32
+#define DG_BT_FOLD_PAIRS 64
 #endif
 constexpr int kBtFoldPairs = DG_BT_FOLD_PAIRS;
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
@@ -1673,8 +1673,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
 #pragma unroll
     for (int j = 0; j < FS; ++j)
         stage_frame[j] = frames + int64_t(f0 + min(warp / KS + j * FSTEP, max(nv - 1, 0))) * n_pixels;
-    auto stage_issue = [&](int c) {
-        const int b = c % NB;
+    auto stage_issue = [&](int c, int b) {  // b = c % NB
         const int32_t *mb = mbuf(c);
         const int4 ch = make_int4(0, mb[0], mb[2], mb[1]);  // {-, pixels, first pair, pairs}
         const int per = (ch.y + KS - 1) / KS, s0 = (warp % KS) * per;
@@ -1757,8 +1756,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     };
     // The second half: mask stores, then this thread's arrival on the
     // buffer's full barrier.
-    auto stage_finish = [&](int c) {
-        const int b = c % NB;
+    auto stage_finish = [&](int c, int b) {
         if constexpr (DEFER_PX) {
             const int dn = mbuf(c)[0];
             const int per = (dn + KS - 1) / KS, s0 = (warp % KS) * per;
@@ -1792,9 +1790,9 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                      : "memory");
         mbar_arrive(full + b);
     };
-    auto stage = [&](int c) {
-        stage_issue(c);
-        stage_finish(c);
+    auto stage = [&](int c, int b) {
+        stage_issue(c, b);
+        stage_finish(c, b);
     };
 
     // This warp's row: accumulators, fold counter and origin of each of the
@@ -1833,34 +1831,46 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     // entries are unevenly spread over the chunks even out over the tile.
     bool ok = true;
     for (int j = 0; j < AH + MA && j < nch; ++j) stage_meta(j);
+    static_assert(AH < NB, "the first chunks go to buffers 0..AH-1");
     for (int j = 0; j < AH && j < nch; ++j) {
         if (ok) ok = mbar_wait(rec + j % NM, unsigned(j / NM) & 1u);
-        if (ok) stage(j);
+        if (ok) stage(j, j);
     }
+    // Buffers and phases of chunks c and j = c + AH, kept as counters (c % NB
+    // and c / NB without a division per chunk).
+    int cb = 0, cq = 0, jb = AH, jq = 0;
     for (int c = 0; c < nch; ++c) {
         const int j = c + AH;
         bool pending = false;  // chunk j's second staging half, after chunk c
         if (j < nch) {
-            if (ok && j >= NB) ok = mbar_wait(empty + j % NB, unsigned(j / NB - 1) & 1u);
+            if (ok && j >= NB) ok = mbar_wait(empty + jb, unsigned(jq - 1) & 1u);
             if (ok && j + MA < nch) stage_meta(j + MA);
             if (ok) ok = mbar_wait(rec + j % NM, unsigned(j / NM) & 1u);
             if (ok) {
                 if constexpr (DEFER) {
-                    stage_issue(j);
+                    stage_issue(j, jb);
                     pending = true;
                 } else {
-                    stage(j);
+                    stage(j, jb);
                 }
             }
         }
-        if (ok) ok = mbar_wait(full + c % NB, unsigned(c / NB) & 1u);
+        if (ok) ok = mbar_wait(full + cb, unsigned(cq) & 1u);
         if (!__all_sync(0xffffffffu, ok)) {
             ok = false;
             break;
         }
-        const int b = c % NB;
+        const int b = cb, pb = jb;  // pb: chunk j's buffer, for its second half
+        if (++cb == NB) {
+            cb = 0;
+            ++cq;
+        }
+        if (++jb == NB) {
+            jb = 0;
+            ++jq;
+        }
         if (r >= nrows) {
-            if (pending) stage_finish(j);
+            if (pending) stage_finish(j, pb);
             if (lane == 0 && signal) mbar_arrive(empty + b);
             continue;
         }
@@ -2010,7 +2020,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 fold();
             }
         }
-        if (pending) stage_finish(j);
+        if (pending) stage_finish(j, pb);
         __syncwarp();
         if (lane == 0 && signal) mbar_arrive(empty + b);
     }

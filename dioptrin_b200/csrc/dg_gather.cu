@@ -1478,7 +1478,7 @@ using BtAcc = std::conditional<DG_BT_ACC64 != 0, AccP64, Acc2>::type;
 // Pairs of a row summed in plain FP32 (each half of a packed accumulator
 // takes one entry per pair) before they are folded into the double-word sums.
 #ifndef DG_BT_FOLD_PAIRS
-#define DG_BT_FOLD_PAIRS 64
+#define DG_BT_FOLD_PAIRS 32
 #endif
 constexpr int kBtFoldPairs = DG_BT_FOLD_PAIRS;
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7

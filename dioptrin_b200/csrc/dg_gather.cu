@@ -3107,31 +3107,37 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
 
 namespace {
 
-// Persistent grid of the work-queue gather: kQueueCtasPerSm CTAs per SM
-// (the CTAs stay resident and claim tiles to the end). Fewer than an SM
-// holds, so that the queues of several request-loop workers, and plan builds,
-// run beside each other rather than one after another.
-#ifndef DG_QUEUE_CTAS_PER_SM
-#define DG_QUEUE_CTAS_PER_SM 1
-#endif
+// Resident capacity of the work-queue gather: the CTAs the SMs hold at
+// once. A call's grid is one CTA per claim of tiles up to that capacity: a
+// small batch runs as an ordinary grid whose CTAs claim once, beside other
+// streams' kernels (a request loop's other workers, plan builds); a batch
+// larger than the GPU keeps every CTA resident, claiming until the queue is
+// empty.
 template <int MODE, typename P>
-int queue_gather_grid() {
-    static int grid = 0;
-    if (grid == 0) {
+int queue_capacity() {
+    static int cap = 0;
+    if (cap == 0) {
         int per_sm = 0, dev = 0, sms = 0;
         DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rows_queue<MODE, P>,
                                                               kRowsThreads, 0));
         DG_CUDA(cudaGetDevice(&dev));
         DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        grid = std::max(1, std::min(per_sm, DG_QUEUE_CTAS_PER_SM)) * std::max(1, sms);
+        cap = std::max(1, per_sm) * std::max(1, sms);
     }
-    return grid;
+    return cap;
 }
 
 template <int MODE, typename P>
 void queue_launch_typed(QueueHeader *hdr, const QueuePlan *plans, cudaStream_t s) {
-    k_rows_queue<MODE, P><<<queue_gather_grid<MODE, P>(), kRowsThreads, 0, s>>>(hdr, plans);
+    k_rows_queue<MODE, P><<<queue_capacity<MODE, P>(), kRowsThreads, 0, s>>>(hdr, plans);
     DG_CUDA(cudaGetLastError());
+}
+
+template <typename P>
+int queue_capacity_mode(int mode) {
+    if (mode == kSpread) return queue_capacity<kSpread, P>();
+    if (mode == kErrors) return queue_capacity<kErrors, P>();
+    return queue_capacity<kIntensity, P>();
 }
 
 template <typename P>
@@ -3142,6 +3148,22 @@ void queue_launch_mode(int mode, QueueHeader *hdr, const QueuePlan *plans, cudaS
 }
 
 }  // namespace
+
+int queue_grid(int dtype, uint32_t flags, int64_t total_tiles) {
+    const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
+                                                                                : kIntensity;
+    int cap = 1;
+    switch (dtype) {
+    case DG_U16: cap = queue_capacity_mode<uint16_t>(mode); break;
+    case DG_U32: cap = queue_capacity_mode<uint32_t>(mode); break;
+    case DG_I32: cap = queue_capacity_mode<int32_t>(mode); break;
+    case DG_F32: cap = queue_capacity_mode<float>(mode); break;
+    case DG_F64: cap = queue_capacity_mode<double>(mode); break;
+    default: fail(DG_INVALID_INPUT, "unknown pixel dtype");
+    }
+    const int64_t claims = (total_tiles + kQueueClaim - 1) / kQueueClaim;
+    return int(std::max<int64_t>(1, std::min<int64_t>(claims, cap)));
+}
 
 void queue_launch(int dtype, uint32_t flags, QueueHeader *hdr, const QueuePlan *plans,
                   cudaStream_t s) {

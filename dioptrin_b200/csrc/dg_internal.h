@@ -381,9 +381,13 @@ struct QueueHeader {
 QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixels, int n_frames,
                      double *oi, double *os, double *od);
 // Enqueues the work-queue gather for descriptors already in device memory
-// (`hdr` followed by the descriptors) on `s`.
+// (`hdr` followed by the descriptors) on `s`, at its resident capacity (the
+// request's grid is set per call, queue_grid).
 void queue_launch(int dtype, uint32_t flags, QueueHeader *hdr, const QueuePlan *plans,
                   cudaStream_t s);
+// The work-queue gather's grid for a call of total_tiles tiles: one CTA per
+// claim of tiles, at most the CTAs the SMs hold at once.
+int queue_grid(int dtype, uint32_t flags, int64_t total_tiles);
 // The allocation-free path's fixed device array (dg_gather.cu): its address
 // on the current device, looked up on every call, and its size in doubles.
 double *noalloc_scratch(size_t *n_doubles);

@@ -3,12 +3,15 @@
 // A dg_multi holds the device descriptors of one call (a header and one
 // QueuePlan per plan batch) and, per pixel type and output set, a CUDA graph
 // of the call's device work: the copy of the descriptors from page-locked
-// host staging and the work-queue gather (a persistent grid of row-warp CTAs
-// that claim (plan, row item, block of four frames) tiles from a counter the
-// copy resets and write each row's results themselves). The graph is captured on the first call of
-// its kind and replayed after that, the descriptors changing between calls
-// while the graph stays the same: one graph launch per batch of plans,
-// whatever their number and sizes. No plan scratch is used, so calls on
+// host staging and the work-queue gather (row-warp CTAs that claim (plan,
+// row item, block of four frames) tiles from a counter the copy resets and
+// write each row's results themselves). The graph is captured on the first
+// call of its kind and replayed after that, the descriptors and the gather's
+// grid changing between calls while the graph stays the same: one graph
+// launch per batch of plans, whatever their number and sizes. The grid is
+// one CTA per claim of tiles up to the CTAs the SMs hold at once, so a small
+// batch runs beside other streams' kernels and a large one keeps every CTA
+// resident, claiming until the queue is empty. No plan scratch is used, so calls on
 // different streams that share plans are not ordered against each other. The
 // reference's streaming driver (src/batch/bounded.rs:172) and its engine's
 // pipelined tiles (src/integration/cuda/device.rs:1417-1584) keep one plan
@@ -19,6 +22,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <vector>
 
 #include "dg_internal.h"
 
@@ -32,9 +36,20 @@ struct dg_multi {
     cudaStream_t capture = nullptr;      // graphs are captured here, launched anywhere
     cudaEvent_t done = nullptr;          // the last call's device work has finished
     bool pending = false;
-    std::map<std::pair<int32_t, uint32_t>, cudaGraphExec_t> graphs;
+    // Per (dtype, flags): the captured graph, its instance, and the gather's
+    // kernel node, whose grid is set for each call.
+    struct Graph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t kernel = nullptr;
+        cudaKernelNodeParams params{};
+    };
+    std::map<std::pair<int32_t, uint32_t>, Graph> graphs;
     ~dg_multi() {
-        for (auto &g : graphs) cudaGraphExecDestroy(g.second);
+        for (auto &g : graphs) {
+            if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+            if (g.second.graph) cudaGraphDestroy(g.second.graph);
+        }
         if (done) cudaEventDestroy(done);
         if (capture) cudaStreamDestroy(capture);
         if (host) cudaFreeHost(host);
@@ -223,13 +238,35 @@ dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items, int32_
                 throw;
             }
             DG_CUDA(cudaStreamEndCapture(multi->capture, &graph));
-            cudaGraphExec_t exec = nullptr;
-            const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            DG_CUDA(e);
-            g = multi->graphs.emplace(key, exec).first;
+            dg_multi::Graph entry;
+            entry.graph = graph;
+            size_t n_nodes = 0;
+            cudaError_t e = cudaGraphGetNodes(graph, nullptr, &n_nodes);
+            std::vector<cudaGraphNode_t> nodes(n_nodes);
+            if (e == cudaSuccess) e = cudaGraphGetNodes(graph, nodes.data(), &n_nodes);
+            for (size_t i = 0; e == cudaSuccess && i < n_nodes; ++i) {
+                cudaGraphNodeType type;
+                e = cudaGraphNodeGetType(nodes[i], &type);
+                if (e == cudaSuccess && type == cudaGraphNodeTypeKernel) {
+                    entry.kernel = nodes[i];
+                    e = cudaGraphKernelNodeGetParams(nodes[i], &entry.params);
+                }
+            }
+            if (e == cudaSuccess && !entry.kernel) e = cudaErrorInvalidValue;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&entry.exec, graph, 0);
+            if (e != cudaSuccess) {
+                if (entry.exec) cudaGraphExecDestroy(entry.exec);
+                cudaGraphDestroy(graph);
+                DG_CUDA(e);
+            }
+            g = multi->graphs.emplace(key, entry).first;
         }
-        DG_CUDA(cudaGraphLaunch(g->second, s));
+        // this call's grid: one CTA per claim of tiles, up to the resident
+        // capacity (the capture used the capacity)
+        dg_multi::Graph &gr = g->second;
+        gr.params.gridDim = dim3(unsigned(dg::queue_grid(dtype, flags, items_total)), 1, 1);
+        DG_CUDA(cudaGraphExecKernelNodeSetParams(gr.exec, gr.kernel, &gr.params));
+        DG_CUDA(cudaGraphLaunch(gr.exec, s));
         DG_CUDA(cudaEventRecord(multi->done, s));
         multi->pending = true;
         for (int32_t i = 0; i < n_items; ++i)

@@ -8,7 +8,7 @@
 // flags join the batch (up to eight plans, and at most a quarter of the queue,
 // so that a backlog spreads over the workers instead of piling into one
 // batch), which runs as one work-queue gather
-// (dg_multi: a persistent grid of row-warp CTAs over (plan, row item) items,
+// (dg_multi: row-warp CTAs claiming (plan, row item, frame block) tiles,
 // replayed as a CUDA graph, no partial sums). Four workers run batches
 // concurrently on their own streams, so one batch's copies overlap another's
 // gather; their staging grows stream-ordered and is kept. max_coalesce 1

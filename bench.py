@@ -359,7 +359,7 @@ class Serving:
                            for k, v in st.items()}}
 
 
-def serve_leg(rates=(1000.0, 2500.0), seconds: float = 2.0) -> dict:
+def serve_leg(rates=(1000.0, 2500.0), seconds: float = 4.0) -> dict:
     """The mixed-stream part of the metric for the default bench line: the
     coalescing loop and the plain path (one request per launch) on the same
     arrivals, at each offered rate."""

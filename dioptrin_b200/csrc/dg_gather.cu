@@ -707,8 +707,10 @@ __global__ void __launch_bounds__(kRowsThreads) k_rows(const QueuePlan q) {
 // Frames per pass (and per frame block) of a row-warp launch of nf frames.
 __host__ __device__ constexpr int rows_pass_frames(int nf) { return nf <= 1 ? 1 : nf <= 2 ? 2 : 4; }
 
-// Tiles a work-queue CTA claims at once (one atomic add per claim).
+// Tiles a resident work-queue CTA claims at once (one atomic add per claim),
+// and the most tiles a call runs as one CTA per tile.
 constexpr int kQueueClaim = 4;
+constexpr int64_t kQueueDirectTiles = int64_t(1) << 24;
 
 // Work-queue gather over several plans (dg_multi_integrate). A persistent
 // grid of row-warp CTAs claims (plan, row item, frame block) tiles from one
@@ -724,12 +726,21 @@ __global__ void __launch_bounds__(kRowsThreads)
     __shared__ RowsRed s_red;
     __shared__ int s_item;
     const int n_plans = hdr->n_plans, total = hdr->total_items;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, kQueueClaim);
-        __syncthreads();
-        const int first = s_item;
-        __syncthreads();  // every thread has read s_item before it is claimed again
-        if (first >= total) return;
+    // A grid that covers every tile takes tile blockIdx.x; a smaller one (a
+    // batch beyond the grid limit) stays resident and claims tiles.
+    const bool direct = int64_t(gridDim.x) >= int64_t(total);
+    for (int pass = 0;; ++pass) {
+        int first;
+        if (direct) {
+            first = int(blockIdx.x);
+            if (pass > 0 || first >= total) return;
+        } else {
+            if (threadIdx.x == 0) s_item = atomicAdd(&hdr->counter, kQueueClaim);
+            __syncthreads();
+            first = s_item;
+            __syncthreads();  // every thread has read s_item before it is claimed again
+            if (first >= total) return;
+        }
         // the last descriptor whose first tile is at most `first` (plans with
         // no tiles share the next one's prefix and are skipped)
         int lo = 0, hi = n_plans - 1;
@@ -738,7 +749,7 @@ __global__ void __launch_bounds__(kRowsThreads)
             if (plans[mid].item_first <= first) lo = mid;
             else hi = mid - 1;
         }
-        const int last = min(first + kQueueClaim, total);
+        const int last = direct ? first + 1 : min(first + kQueueClaim, total);
         for (int item = first; item < last; ++item) {
             while (lo + 1 < n_plans && plans[lo + 1].item_first <= item) ++lo;
             const QueuePlan &q = plans[lo];
@@ -3108,11 +3119,9 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
 namespace {
 
 // Resident capacity of the work-queue gather: the CTAs the SMs hold at
-// once. A call's grid is one CTA per claim of tiles up to that capacity: a
-// small batch runs as an ordinary grid whose CTAs claim once, beside other
-// streams' kernels (a request loop's other workers, plan builds); a batch
-// larger than the GPU keeps every CTA resident, claiming until the queue is
-// empty.
+// once, the grid of a call of more than kQueueDirectTiles tiles, whose CTAs
+// stay resident and claim tiles until the queue is empty. Smaller calls run
+// one CTA per tile (queue_grid).
 template <int MODE, typename P>
 int queue_capacity() {
     static int cap = 0;
@@ -3150,6 +3159,10 @@ void queue_launch_mode(int mode, QueueHeader *hdr, const QueuePlan *plans, cudaS
 }  // namespace
 
 int queue_grid(int dtype, uint32_t flags, int64_t total_tiles) {
+    // one CTA per tile (the hardware schedules them as CTAs retire, beside
+    // other streams' kernels); a batch of more tiles than kQueueDirectTiles
+    // runs the resident grid that claims them
+    if (total_tiles <= kQueueDirectTiles) return int(std::max<int64_t>(1, total_tiles));
     const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
                                                                                 : kIntensity;
     int cap = 1;

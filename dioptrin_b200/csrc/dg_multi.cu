@@ -9,9 +9,9 @@
 // call of its kind and replayed after that, the descriptors and the gather's
 // grid changing between calls while the graph stays the same: one graph
 // launch per batch of plans, whatever their number and sizes. The grid is
-// one CTA per claim of tiles up to the CTAs the SMs hold at once, so a small
-// batch runs beside other streams' kernels and a large one keeps every CTA
-// resident, claiming until the queue is empty. No plan scratch is used, so calls on
+// one CTA per tile, which the hardware schedules as CTAs retire, beside other
+// streams' kernels; a batch of more than 2^24 tiles runs a resident grid (the
+// CTAs the SMs hold at once) whose CTAs claim tiles until the queue is empty. No plan scratch is used, so calls on
 // different streams that share plans are not ordered against each other. The
 // reference's streaming driver (src/batch/bounded.rs:172) and its engine's
 // pipelined tiles (src/integration/cuda/device.rs:1417-1584) keep one plan

@@ -378,8 +378,8 @@ DG_EXPORT dg_status dg_server_stats_get(dg_server *server, dg_server_stats *out)
  * No counterpart in the reference, whose engine launches one plan at a time
  * (src/integration/cuda/device.rs:1417-1584; streaming driver
  * src/batch/bounded.rs:172). A dg_multi integrates batches of device-resident
- * frames of several plans together: a grid of row-warp CTAs (persistent when
- * the queue is larger than the GPU holds at once) takes
+ * frames of several plans together: a grid of row-warp CTAs (one per tile;
+ * resident and claiming for batches of more than 2^24 tiles) takes
  * (plan, row item, block of four frames) tiles from one counter until every
  * plan's table is summed, so plans of very different sizes share the GPU without a launch
  * per plan; each row's results are written by the CTA that sums it (no

@@ -526,8 +526,7 @@ __device__ __forceinline__ double group8_sum_d(double v) {
 
 // Shared memory of a row-warp CTA: the warps' sums of a long row.
 constexpr int kRowsWarps = kRowsThreads / 32;
-constexpr int kRowsMaxSums = 32;  // frames per pass x sums per frame, at most
-using RowsRed = double[kRowsWarps][kRowsMaxSums];
+using RowsRed = double[kRowsWarps][4 * kMaxAcc];
 
 // One row-warp item of a plan's batch (q.item[k]); every thread of the CTA
 // calls it. F frames per pass over the entries.
@@ -536,12 +535,6 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
     constexpr int NW = kRowsWarps;
-    static_assert(F * NA <= kRowsMaxSums, "a pass's sums fit the reduction buffer");
-    // entries in flight per thread: fewer as each entry feeds more frames
-    constexpr int U = F >= 16 ? 1 : F >= 8 ? 2 : kRowsU;
-    // staged pixel values: FP32 (as every mapping stages them), FP64 frames
-    // kept in FP64
-    using XT = typename std::conditional<std::is_same<P, double>::value, double, float>::type;
     const int2 *__restrict__ items = qp.item;
     const int32_t *__restrict__ rows = qp.rows;
     const int32_t *__restrict__ row_ptr = qp.row_ptr;
@@ -587,22 +580,22 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
         for (int q = 0; q < F; ++q)
 #pragma unroll
             for (int a = 0; a < NA; ++a) acc[q][a] = 0.0;
-        for (int j0 = e0 + li; j0 < e1; j0 += nl * U) {
-            float2 nn[U];
-            int2 en[U];
-            XT x[U][F];
+        for (int j0 = e0 + li; j0 < e1; j0 += nl * kRowsU) {
+            float2 nn[kRowsU];
+            int2 en[kRowsU];
+            double x[kRowsU][F];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
+            for (int u = 0; u < kRowsU; ++u) {
                 const int j = j0 + nl * u;
                 const bool in = j < e1;
                 en[u] = in ? entry[j] : make_int2(0, 0);
                 const uint32_t col = uint32_t(en[u].x);
                 if constexpr (SPREAD) nn[u] = in ? px_norm[col] : make_float2(0.f, 0.f);
 #pragma unroll
-                for (int q = 0; q < F; ++q) x[u][q] = in ? XT(__ldg(fr[q] + col)) : XT(0);
+                for (int q = 0; q < F; ++q) x[u][q] = in ? load_px_d<P>(fr[q], col) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
+            for (int u = 0; u < kRowsU; ++u) {
                 if (j0 + nl * u >= e1) break;
                 if constexpr (SPREAD) {
                     // valid for the spread (azimuthal.rs:62-75): c > 0 and n
@@ -712,11 +705,7 @@ __global__ void __launch_bounds__(kRowsThreads) k_rows(const QueuePlan q) {
 }
 
 // Frames per pass (and per frame block) of a row-warp launch of nf frames.
-// The spread (six sums per frame at most) takes up to four frames per pass,
-// the other modes up to sixteen.
-__host__ __device__ constexpr int rows_pass_frames(int nf, bool spread) {
-    return nf <= 1 ? 1 : nf <= 2 ? 2 : nf <= 4 || spread ? 4 : nf <= 8 ? 8 : 16;
-}
+__host__ __device__ constexpr int rows_pass_frames(int nf) { return nf <= 1 ? 1 : nf <= 2 ? 2 : 4; }
 
 // Tiles a resident work-queue CTA claims at once (one atomic add per claim),
 // and the most tiles a call runs as one CTA per tile.
@@ -769,16 +758,10 @@ __global__ void __launch_bounds__(kRowsThreads)
             // next)
             const int local = item - q.item_first;
             const int k = local / q.frame_blocks, fb = local - k * q.frame_blocks;
-            switch (rows_pass_frames(q.n_frames, MODE == kSpread)) {
+            switch (rows_pass_frames(q.n_frames)) {
             case 1: rows_item<MODE, P, 1>(q, k, fb, s_red); break;
             case 2: rows_item<MODE, P, 2>(q, k, fb, s_red); break;
-            case 4: rows_item<MODE, P, 4>(q, k, fb, s_red); break;
-            default:
-                if constexpr (MODE != kSpread) {
-                    if (q.n_frames <= 8) rows_item<MODE, P, 8>(q, k, fb, s_red);
-                    else rows_item<MODE, P, 16>(q, k, fb, s_red);
-                }
-                break;
+            default: rows_item<MODE, P, 4>(q, k, fb, s_red); break;
             }
         }
     }
@@ -2471,16 +2454,10 @@ void launch_rows(const GatherTable &t, const P *fp, int64_t n_pixels, int nf, do
                  double *os, double *od, cudaStream_t s) {
     const QueuePlan q = queue_plan(t, fp, n_pixels, nf, oi, os, od);
     const dim3 grid(unsigned(q.n_items), unsigned(q.frame_blocks));
-    switch (rows_pass_frames(nf, MODE == kSpread)) {
+    switch (rows_pass_frames(nf)) {
     case 1: k_rows<MODE, P, 1><<<grid, kRowsThreads, 0, s>>>(q); break;
     case 2: k_rows<MODE, P, 2><<<grid, kRowsThreads, 0, s>>>(q); break;
-    case 4: k_rows<MODE, P, 4><<<grid, kRowsThreads, 0, s>>>(q); break;
-    default:
-        if constexpr (MODE != kSpread) {
-            if (nf <= 8) k_rows<MODE, P, 8><<<grid, kRowsThreads, 0, s>>>(q);
-            else k_rows<MODE, P, 16><<<grid, kRowsThreads, 0, s>>>(q);
-        }
-        break;
+    default: k_rows<MODE, P, 4><<<grid, kRowsThreads, 0, s>>>(q); break;
     }
     DG_CUDA(cudaGetLastError());
 }
@@ -3134,9 +3111,8 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
     q.n_frames = n_frames;
     q.n_rows = t.n_rows;
     q.n_items = n_frames > 0 ? t.rw_n_items : 0;
-    // the spread is requested exactly when its output is given
-    const int pf = rows_pass_frames(n_frames, od != nullptr);
-    q.frame_blocks = std::max(1, (n_frames + pf - 1) / pf);
+    q.frame_blocks = std::max(1, (n_frames + rows_pass_frames(n_frames) - 1) /
+                                     rows_pass_frames(n_frames));
     return q;
 }
 

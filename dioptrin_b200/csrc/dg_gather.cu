@@ -1499,7 +1499,10 @@ static_assert(Bt7::smem_bytes<kSpread>() <= 227 * 1024, "mapping 7 fits shared m
 static_assert(Bt8::smem_bytes<kSpread>() <= 227 * 1024, "mapping 8 fits shared memory");
 // Per-frame masks on mapping 8's tiles (same rows and chunks, so the same
 // records): one frame per lane leaves registers for the four sums.
-using BtR = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, 1, 4, DG_BT8_BUFS, DG_BT8_AHEAD>;
+#ifndef DG_BTR_F2
+#define DG_BTR_F2 1
+#endif
+using BtR = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, DG_BTR_F2, 4, DG_BT8_BUFS, DG_BT8_AHEAD>;
 static_assert(BtR::kMetaWords == Bt8::kMetaWords && BtR::kMetaHead == Bt8::kMetaHead,
               "masked tiles read mapping 8's chunk records");
 static_assert(BtR::smem_bytes<kRaw>() <= 227 * 1024, "masked tiles fit shared memory");

@@ -34,7 +34,7 @@ EXPORTS = [
     "dg_integrate_raw_device", "dg_host_alloc", "dg_host_free", "dg_host_is_pinned",
     "dg_server_create", "dg_server_destroy",
     "dg_server_register", "dg_server_submit", "dg_server_poll", "dg_server_stats_get",
-    "dg_multi_create", "dg_multi_destroy", "dg_multi_integrate",
+    "dg_multi_create", "dg_multi_destroy", "dg_multi_integrate", "dg_multi_test_resident",
     "dg_device_info_get", "dg_last_error",
 ]
 
@@ -161,6 +161,7 @@ def lib():
         L.dg_multi_create.argtypes = [C.c_int32, C.c_int32, P(vp)]
         L.dg_multi_destroy.argtypes = [vp]
         L.dg_multi_integrate.argtypes = [vp, P(MultiItem), C.c_int32, C.c_int32, C.c_uint32, vp]
+        L.dg_multi_test_resident.argtypes = [vp, C.c_int32]
         L.dg_device_info_get.argtypes = [C.c_int32, P(DeviceInfo)]
         L.dg_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.dg_last_error.restype = C.c_int32

@@ -3161,11 +3161,12 @@ void queue_launch_mode(int mode, QueueHeader *hdr, const QueuePlan *plans, cudaS
 
 }  // namespace
 
-int queue_grid(int dtype, uint32_t flags, int64_t total_tiles) {
+int queue_grid(int dtype, uint32_t flags, int64_t total_tiles, bool resident) {
     // one CTA per tile (the hardware schedules them as CTAs retire, beside
     // other streams' kernels); a batch of more tiles than kQueueDirectTiles
     // runs the resident grid that claims them
-    if (total_tiles <= kQueueDirectTiles) return int(std::max<int64_t>(1, total_tiles));
+    if (!resident && total_tiles <= kQueueDirectTiles)
+        return int(std::max<int64_t>(1, total_tiles));
     const int mode = (flags & DG_AZIMUTHAL_STD) ? kSpread : (flags & DG_ERRORS) ? kErrors
                                                                                 : kIntensity;
     int cap = 1;

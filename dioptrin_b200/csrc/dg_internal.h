@@ -386,8 +386,9 @@ QueuePlan queue_plan(const GatherTable &t, const void *d_frames, int64_t n_pixel
 void queue_launch(int dtype, uint32_t flags, QueueHeader *hdr, const QueuePlan *plans,
                   cudaStream_t s);
 // The work-queue gather's grid for a call of total_tiles tiles: one CTA per
-// claim of tiles, at most the CTAs the SMs hold at once.
-int queue_grid(int dtype, uint32_t flags, int64_t total_tiles);
+// tile, or (beyond 2^24 tiles, or with `resident`) the CTAs the SMs hold at
+// once, which then claim tiles until the queue is empty.
+int queue_grid(int dtype, uint32_t flags, int64_t total_tiles, bool resident = false);
 // The allocation-free path's fixed device array (dg_gather.cu): its address
 // on the current device, looked up on every call, and its size in doubles.
 double *noalloc_scratch(size_t *n_doubles);

@@ -36,6 +36,7 @@ struct dg_multi {
     cudaStream_t capture = nullptr;      // graphs are captured here, launched anywhere
     cudaEvent_t done = nullptr;          // the last call's device work has finished
     bool pending = false;
+    bool resident = false;               // test hook: the claiming grid for every call
     // Per (dtype, flags): the captured graph, its instance, and the gather's
     // kernel node, whose grid is set for each call.
     struct Graph {
@@ -144,6 +145,16 @@ dg_status dg_multi_destroy(dg_multi *multi) {
     cudaSetDevice(multi->device);
     delete multi;
     if (previous >= 0) cudaSetDevice(previous);
+    return DG_OK;
+}
+
+dg_status dg_multi_test_resident(dg_multi *multi, int32_t on) {
+    if (!multi) {
+        dg::set_last_error("multi must not be NULL");
+        return DG_INVALID_INPUT;
+    }
+    std::lock_guard<std::mutex> lock(multi->mu);
+    multi->resident = on != 0;
     return DG_OK;
 }
 
@@ -264,7 +275,8 @@ dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items, int32_
         // this call's grid: one CTA per claim of tiles, up to the resident
         // capacity (the capture used the capacity)
         dg_multi::Graph &gr = g->second;
-        gr.params.gridDim = dim3(unsigned(dg::queue_grid(dtype, flags, items_total)), 1, 1);
+        gr.params.gridDim =
+            dim3(unsigned(dg::queue_grid(dtype, flags, items_total, multi->resident)), 1, 1);
         DG_CUDA(cudaGraphExecKernelNodeSetParams(gr.exec, gr.kernel, &gr.params));
         DG_CUDA(cudaGraphLaunch(gr.exec, s));
         DG_CUDA(cudaEventRecord(multi->done, s));

@@ -411,6 +411,10 @@ DG_EXPORT dg_status dg_multi_destroy(dg_multi *multi);
 DG_EXPORT dg_status dg_multi_integrate(dg_multi *multi, const dg_multi_item *items,
                                        int32_t n_items, int32_t dtype, uint32_t flags,
                                        void *stream);
+/* Test hook: with on != 0, later calls run the resident grid (the CTAs the
+ * SMs hold at once, claiming tiles from the queue's counter) that otherwise
+ * only batches of more than 2^24 tiles use. Results are the same either way. */
+DG_EXPORT dg_status dg_multi_test_resident(dg_multi *multi, int32_t on);
 
 /* Device description; cuda_info (src/integration/cuda.rs:262-329). */
 typedef struct dg_device_info {

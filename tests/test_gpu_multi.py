@@ -113,6 +113,28 @@ def test_multi_equals_each_plan_alone(dg, flags):
         p.close()
 
 
+def test_resident_claiming_grid_equals_the_per_tile_grid(dg):
+    # The claiming form (resident CTAs taking four tiles per atomic add) runs
+    # only for batches beyond 2^24 tiles; the test hook forces it here.
+    import torch
+    from dioptrin_b200 import _native as N
+    plans = _plans(dg)
+    gen = np.random.default_rng(17)
+    frames = [torch.from_numpy(gen.poisson(70.0, (n,) + shape).astype(np.uint16)).cuda()
+              for (_, shape, _, _), n in zip(plans, (9, 3, 5))]
+    items = [(p, f, nb) for (p, _, nb, _), f in zip(plans, frames)]
+    h = _multi()
+    direct = _run_multi(h, items, N.DG_U16, N.DG_ERRORS)
+    N.check(N.lib().dg_multi_test_resident(h, 1))
+    for _ in range(2):  # the captured graph replayed with the other grid
+        resident = _run_multi(h, items, N.DG_U16, N.DG_ERRORS)
+        for a, b in zip(direct, resident):
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    N.lib().dg_multi_destroy(h)
+    for p, _, _, _ in plans:
+        p.close()
+
+
 def test_multi_with_the_spread_matches_the_oracle(dg, oracle):
     import torch
     from dioptrin_b200 import _native as N

@@ -33,11 +33,18 @@ thread_local std::string g_last_error;
 
 // Detector rows per gather strip (see dg_gather.cu): small enough that a
 // unit's bins cover a few kilobytes of each frame, large enough that a bin's
-// ring is cut into few segments.
+// ring is cut into few segments. A 2D bin is a compact patch of ~100
+// entries, so its plans take taller strips: most of its rows are then one
+// segment, with fewer partial sums to write and fold (the Eiger-9M cake's
+// 64-frame batch: 1.17 against 1.35 ms, 261 k → 153 k segments).
 #ifndef DG_STRIP_ROWS
 #define DG_STRIP_ROWS 16
 #endif
+#ifndef DG_STRIP_ROWS_2D
+#define DG_STRIP_ROWS_2D 64
+#endif
 constexpr int32_t kStripRows = DG_STRIP_ROWS;
+constexpr int32_t kStripRows2d = DG_STRIP_ROWS_2D;
 
 }  // namespace
 
@@ -236,8 +243,8 @@ dg_status dg_plan_create(const dg_geometry *geometry, const dg_method *method,
                 DG_CUDA(cudaMemcpyAsync(d_mask.ptr, mask, size_t(npix), cudaMemcpyHostToDevice, s));
             }
             dg::compact_table(built.full, any ? d_mask.ptr : nullptr, int32_t(npix), s, plan->table);
-            dg::make_gather_table(plan->table, built.norm.ptr, dim1, dim2, kStripRows, s,
-                                  plan->gather);
+            dg::make_gather_table(plan->table, built.norm.ptr, dim1, dim2,
+                                  n_azimuthal ? kStripRows2d : kStripRows, s, plan->gather);
             if (method->flags & DG_PLAN_FLIP_VERTICAL) dg::flip_gather_rows(plan->gather, dim1, dim2, s);
             DG_CUDA(cudaEventRecord(e1, s));
             DG_CUDA(cudaEventSynchronize(e1));

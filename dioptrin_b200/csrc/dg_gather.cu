@@ -1376,7 +1376,8 @@ __global__ void __launch_bounds__(256)
 // chunk size.
 // The same kernel writes raw sums instead (flag `raw`: S and V, with the
 // row's strict N and C), and in mode kRaw applies per-frame masks on mapping
-// 8's tiles with one frame per lane (BtR): a chunk's mask bytes are staged
+// 8's tiles (BtR: two frames per lane, one for 2-byte pixels): a chunk's mask
+// bytes are staged
 // next to its pixels, and a masked entry adds nothing to S, V, N or C. Bytes
 // the kernel loads rather than copies (masks, 2-byte pixels) are loaded with
 // a chunk's copies and stored after the warp has summed the chunk before it.
@@ -1499,13 +1500,20 @@ static_assert(Bt7::smem_bytes<kSpread>() <= 227 * 1024, "mapping 7 fits shared m
 static_assert(Bt8::smem_bytes<kSpread>() <= 227 * 1024, "mapping 8 fits shared memory");
 // Per-frame masks on mapping 8's tiles (same rows and chunks, so the same
 // records): one frame per lane leaves registers for the four sums.
-#ifndef DG_BTR_F2
-#define DG_BTR_F2 1
-#endif
-using BtR = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, DG_BTR_F2, 4, DG_BT8_BUFS, DG_BT8_AHEAD>;
-static_assert(BtR::kMetaWords == Bt8::kMetaWords && BtR::kMetaHead == Bt8::kMetaHead,
+// Two frames per lane for 4-byte pixels (the FP64 folds leave the registers
+// for four sums of two frames: 76 k against 72 k frames/s on the Eiger-4M
+// batch); 2-byte pixels, whose mask and pixel loads are deferred in
+// registers, keep one.
+template <typename P>
+using BtR = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, sizeof(P) == 2 ? 1 : 2, 4, DG_BT8_BUFS,
+                  DG_BT8_AHEAD>;
+static_assert(BtR<float>::kMetaWords == Bt8::kMetaWords &&
+                  BtR<uint16_t>::kMetaWords == Bt8::kMetaWords &&
+                  BtR<float>::kMetaHead == Bt8::kMetaHead,
               "masked tiles read mapping 8's chunk records");
-static_assert(BtR::smem_bytes<kRaw>() <= 227 * 1024, "masked tiles fit shared memory");
+static_assert(BtR<float>::smem_bytes<kRaw>() <= 227 * 1024 &&
+                  BtR<uint16_t>::smem_bytes<kRaw>() <= 227 * 1024,
+              "masked tiles fit shared memory");
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -3371,8 +3379,8 @@ bool launch_raw(GatherTable &t, const void *frames, int64_t n_pixels, int nf, in
             DG_CUDA(cudaGetLastError());
             bt.raw_built = true;
         }
-        if (raw) launch_bins<kRaw, P, BtR>(t, bt, fp, n_pixels, nf, o0, o2, o1, s, o3, 1, masks, mask_stride);
-        else launch_bins<kRaw, P, BtR>(t, bt, fp, n_pixels, nf, o0, o1, nullptr, s, nullptr, 0, masks, mask_stride);
+        if (raw) launch_bins<kRaw, P, BtR<P>>(t, bt, fp, n_pixels, nf, o0, o2, o1, s, o3, 1, masks, mask_stride);
+        else launch_bins<kRaw, P, BtR<P>>(t, bt, fp, n_pixels, nf, o0, o1, nullptr, s, nullptr, 0, masks, mask_stride);
         DG_CUDA(cudaGetLastError());
         return true;
     }

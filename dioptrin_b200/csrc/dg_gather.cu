@@ -1483,6 +1483,11 @@ struct BtCfg {
 #define DG_BT_ACC64 1
 #endif
 using BtAcc = std::conditional<DG_BT_ACC64 != 0, AccP64, Acc2>::type;
+// Mapping 8's neighbouring tiles launched as 2-CTA clusters (1) or one CTA
+// per tile (0).
+#ifndef DG_BT_CLUSTER_PAIRS
+#define DG_BT_CLUSTER_PAIRS 0
+#endif
 // Bin tiles run largest first (1) or in bin order (0).
 #ifndef DG_BT_LARGEST_FIRST
 #define DG_BT_LARGEST_FIRST 1
@@ -1493,6 +1498,7 @@ using BtAcc = std::conditional<DG_BT_ACC64 != 0, AccP64, Acc2>::type;
 #define DG_BT_FOLD_PAIRS 32
 #endif
 constexpr int kBtFoldPairs = DG_BT_FOLD_PAIRS;
+constexpr bool kBtClusterPairs = DG_BT_CLUSTER_PAIRS != 0;
 using Bt7 = BtCfg<24, 384, 640, 1, 4>;  // mapping 7
 using Bt8 = BtCfg<DG_BT8_ROWS, DG_BT8_DCAP, DG_BT8_PCAP, 2, (DG_BT8_ROWS > 16 ? 2 : 4),
                   DG_BT8_BUFS, DG_BT8_AHEAD>;  // mapping 8
@@ -1594,7 +1600,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                   double *__restrict__ out_i, double *__restrict__ out_s,
                   double *__restrict__ out_d, int *__restrict__ wait_err, int withhold,
                   const double *__restrict__ raw_cnt, double *__restrict__ out_c, int raw,
-                  const uint8_t *__restrict__ masks, int64_t mask_stride) {
+                  const uint8_t *__restrict__ masks, int64_t mask_stride, int paired) {
     using S = StagedPx<P>;
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
@@ -1615,8 +1621,19 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     constexpr int MS = CFG::kMStride;
     extern __shared__ __align__(16) unsigned char smem[];
     const int groups = (n_frames + CFG::kFrames - 1) / CFG::kFrames;
-    const int4 it = items[blockIdx.x / groups];
-    const int f0 = (blockIdx.x % groups) * CFG::kFrames;
+    // Paired tiles: the two CTAs of a cluster take neighbouring tiles 2m and
+    // 2m + 1 for the same frames.
+    int item_idx, group;
+    if (paired) {
+        const int per = 2 * groups, m = int(blockIdx.x) / per, rm = int(blockIdx.x) % per;
+        item_idx = 2 * m + (rm & 1);
+        group = rm >> 1;
+    } else {
+        item_idx = int(blockIdx.x) / groups;
+        group = int(blockIdx.x) % groups;
+    }
+    const int4 it = items[item_idx];
+    const int f0 = group * CFG::kFrames;
     const int nv = min(CFG::kFrames, n_frames - f0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int row0 = it.x, nrows = it.y, ch0 = it.z, nch = it.w;
@@ -2451,10 +2468,38 @@ void launch_bins(const GatherTable &t, const BinTiles &bt, const P *fp, int64_t 
     check_bin_tile_waits(t);
     const float4 *pa = MODE == kSpread ? bt.pair_as.ptr : MODE == kRaw ? bt.pair_ra.ptr : bt.pair_a.ptr;
     const float4 *pb = MODE == kRaw ? bt.pair_rb.ptr : bt.pair_b.ptr;
-    kern<<<unsigned(grid), CFG::kThreads, smem, s>>>(
-        bt.item.ptr, bt.meta.ptr, pa, pb, bt.pair_c.ptr, bt.org.ptr, t.entry_std.ptr, t.den.ptr,
-        t.den_std.ptr, t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od, bt.wait_err.dev,
-        t.withhold_test, t.cnt.ptr, oc, raw, masks, mask_stride);
+    const int paired = bt.paired ? 1 : 0;
+    if (!paired) {
+        kern<<<unsigned(grid), CFG::kThreads, smem, s>>>(
+            bt.item.ptr, bt.meta.ptr, pa, pb, bt.pair_c.ptr, bt.org.ptr, t.entry_std.ptr,
+            t.den.ptr, t.den_std.ptr, t.valid_std.ptr, fp, n_pixels, nf, t.n_rows, oi, os, od,
+            bt.wait_err.dev, t.withhold_test, t.cnt.ptr, oc, raw, masks, mask_stride, paired);
+        return;
+    }
+    // one 2-CTA cluster per (tile pair, frame group): both CTAs on one GPC
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(unsigned(grid), 1, 1);
+    lc.blockDim = dim3(CFG::kThreads, 1, 1);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    DG_CUDA(cudaLaunchKernelEx(&lc, kern, static_cast<const int4 *>(bt.item.ptr),
+                               static_cast<const int32_t *>(bt.meta.ptr), pa, pb,
+                               static_cast<const float2 *>(bt.pair_c.ptr),
+                               static_cast<const int4 *>(bt.org.ptr),
+                               static_cast<const float4 *>(t.entry_std.ptr),
+                               static_cast<const double *>(t.den.ptr),
+                               static_cast<const double *>(t.den_std.ptr),
+                               static_cast<const int32_t *>(t.valid_std.ptr), fp, n_pixels, nf,
+                               int(t.n_rows), oi, os, od, bt.wait_err.dev, t.withhold_test,
+                               static_cast<const double *>(t.cnt.ptr), oc, raw, masks,
+                               mask_stride, paired));
 }
 
 // Row warps (mapping 10): F frames per pass over a row's entries, one CTA
@@ -2792,16 +2837,16 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     };
     const int nt = int(std::min<int64_t>(
         n_items, std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
-    auto parallel = [&](auto &&fn) {
+    auto parallel = [&](auto &&fn, int64_t count) {
         std::vector<std::thread> pool;
         std::atomic<int64_t> next{0};
         for (int t = 0; t < nt; ++t)
             pool.emplace_back([&]() {
-                for (int64_t i; (i = next.fetch_add(1)) < n_items;) fn(i);
+                for (int64_t i; (i = next.fetch_add(1)) < count;) fn(i);
             });
         for (auto &th : pool) th.join();
     };
-    parallel(build);
+    parallel(build, n_items);
     // Tile order, then flatten.
     std::vector<int64_t> order(static_cast<size_t>(n_items));
     for (int64_t i = 0; i < n_items; ++i) order[size_t(i)] = i;
@@ -2810,20 +2855,48 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         return tiles[size_t(a)].entries > tiles[size_t(b)].entries;
     });
 #endif
+    // Mapping 8: neighbouring tiles 2m, 2m + 1 side by side (pairs largest
+    // first), launched as 2-CTA clusters so both run on one GPC and read the
+    // pixel runs they share through the same L2; -1 marks the empty partner
+    // of an odd last tile.
+    out.paired = false;
+    if (kBtClusterPairs && std::is_same<CFG, Bt8>::value && n_items > 1) {
+        const int64_t np = (n_items + 1) / 2;
+        std::vector<int64_t> pairs_order(static_cast<size_t>(np));
+        auto pair_size = [&](int64_t m) {
+            int64_t e = tiles[size_t(2 * m)].entries;
+            if (2 * m + 1 < n_items) e = std::max<int64_t>(e, tiles[size_t(2 * m + 1)].entries);
+            return e;
+        };
+        for (int64_t m = 0; m < np; ++m) pairs_order[size_t(m)] = m;
+        std::stable_sort(pairs_order.begin(), pairs_order.end(),
+                         [&](int64_t a, int64_t b) { return pair_size(a) > pair_size(b); });
+        order.clear();
+        for (int64_t m : pairs_order) {
+            order.push_back(2 * m);
+            order.push_back(2 * m + 1 < n_items ? 2 * m + 1 : -1);
+        }
+        out.paired = true;
+    }
+    const int64_t n_slots = int64_t(order.size());
     // Output offsets of every tile, then the tiles copied in parallel.
-    std::vector<int64_t> o_ch(size_t(n_items) + 1, 0), o_px(size_t(n_items) + 1, 0),
-        o_pr(size_t(n_items) + 1, 0);
-    for (int64_t i = 0; i < n_items; ++i) {
-        const Tile &T = tiles[size_t(order[size_t(i)])];
+    std::vector<int64_t> o_ch(size_t(n_slots) + 1, 0), o_px(size_t(n_slots) + 1, 0),
+        o_pr(size_t(n_slots) + 1, 0);
+    const Tile empty_tile;
+    auto tile_at = [&](int64_t i) -> const Tile & {
+        return order[size_t(i)] < 0 ? empty_tile : tiles[size_t(order[size_t(i)])];
+    };
+    for (int64_t i = 0; i < n_slots; ++i) {
+        const Tile &T = tile_at(i);
         o_ch[size_t(i) + 1] = o_ch[size_t(i)] + int64_t(T.chunks.size());
         o_px[size_t(i) + 1] = o_px[size_t(i)] + int64_t(T.px.size());
         o_pr[size_t(i) + 1] = o_pr[size_t(i)] + int64_t(T.pairs.size());
     }
-    if (o_pr[size_t(n_items)] > INT32_MAX || o_px[size_t(n_items)] > INT32_MAX)
+    if (o_pr[size_t(n_slots)] > INT32_MAX || o_px[size_t(n_slots)] > INT32_MAX)
         fail(DG_UNSUPPORTED, "table too large for bin tiles");
     // default-initialised (not zeroed): every element is written below
-    const size_t n_chunks = size_t(o_ch[size_t(n_items)]), n_pairs = size_t(o_pr[size_t(n_items)]);
-    std::vector<int4> items(static_cast<size_t>(n_items)), org(static_cast<size_t>(nb));
+    const size_t n_chunks = size_t(o_ch[size_t(n_slots)]), n_pairs = size_t(o_pr[size_t(n_slots)]);
+    std::vector<int4> items(static_cast<size_t>(n_slots)), org(static_cast<size_t>(nb));
     // per row {origin entry, first valid entry, row end, 0} (row_origin)
     for (int64_t r = 0; r < nb; ++r)
         org[size_t(r)] = make_int4(oe[size_t(r)], fv[size_t(r)], int(rp[size_t(r) + 1]), 0);
@@ -2831,6 +2904,10 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
     std::unique_ptr<int4[]> pairs(new int4[std::max<size_t>(n_pairs, 1)]);
     auto flatten = [&](int64_t i) {
         const int64_t ti = order[size_t(i)];
+        if (ti < 0) {  // the empty partner: no rows, no chunks
+            items[size_t(i)] = make_int4(0, 0, int(o_ch[size_t(i)]), 0);
+            return;
+        }
         Tile &T = tiles[size_t(ti)];
         const int64_t c0 = o_ch[size_t(i)], pr0 = o_pr[size_t(i)];
         for (size_t c = 0; c < T.chunks.size(); ++c) {
@@ -2851,7 +2928,7 @@ void build_bin_tiles(GatherTable &gt, BinTiles &out, const DeviceCsr &table, cud
         items[size_t(i)] = make_int4(int(r0), nr, int(c0), int(T.chunks.size()));
         T = Tile();
     };
-    parallel(flatten);
+    parallel(flatten, n_slots);
     out.n_items = int32_t(items.size());
     out.item.alloc(items.size());
     out.meta.alloc(std::max<size_t>(n_chunks * kBtMetaWords, 1));

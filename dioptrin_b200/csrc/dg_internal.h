@@ -240,6 +240,9 @@ struct BinTiles {
     bool built = false;
     int32_t n_items = 0;
     DeviceArray<int4> item;        // {first row, rows, first chunk, chunks}, largest first
+    // Items 2m and 2m + 1 are neighbouring tiles launched as one 2-CTA
+    // cluster per frame group (an odd count ends with an empty item).
+    bool paired = false;
     DeviceArray<int32_t> meta;     // per chunk: {pixels, pairs, first pair}, row offsets, pixels
     DeviceArray<int4> org;         // per row {origin entry, first valid entry, row end, 0}
     DeviceArray<float4> pair_a, pair_as, pair_b;

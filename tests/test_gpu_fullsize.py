@@ -17,8 +17,12 @@ spread, with the empty-bin rules (I = 0, sigma = 0, spread NaN).
 across the detector, supersampled n_ss=4 and pyfai_full): row pointers and
 column indices of the device tables bit-exact against the oracle's builders
 (shared_grid.rs:13-232, pyfai_split.rs:35-168, supersampled.rs:1437-1477),
-and the entry-lane gather of lane mapping 2 (the one the benchmark's
-autotuner picks for them) against the oracle on uint16 frames."""
+and the entry-lane gather of lane mapping 2 against the oracle on uint16
+frames.
+
+Few-frame launches: the row warps (mapping 10, the plain path's launch) on
+the Eiger-4M table with the spread and on the 2D cake, and the entry-lane
+mapping 3 that the cake's 64-frame batches pick."""
 import os
 
 import numpy as np
@@ -156,4 +160,41 @@ def test_2d_cake_full_size(dg, oracle, name):
     print(name, f"intensity {ri:.3g} sigma {rs:.3g}")
     assert ri <= TOL_I and rs <= TOL_I
     assert np.all(gi[~nz] == 0) and np.all(gs[~nz] == 0)
+    plan.close()
+
+
+@pytest.mark.parametrize("name,n,variant", [("eiger4m_ps2000_b256", 3, 10),
+                                            ("eiger9m_2d_ss4", 5, 10),
+                                            ("eiger9m_2d_ss4", 9, 3)])
+def test_few_frame_launches_full_size(dg, oracle, name, n, variant):
+    """The few-frame launches on the benchmark's tables: the row warps
+    (mapping 10: rows of more than 512 entries one per CTA on Eiger-4M,
+    rows of at most 64 entries eight lanes each on the 2D cake, a pass of
+    four frames and a partial second pass) and the entry-lane mapping the
+    2D cake's batches pick, against the oracle frame by frame."""
+    from dioptrin_b200 import _native as N
+    from dioptrin_b200 import workloads as W
+    w = W.WORKLOADS[name]
+    full, table, mask, norm, den = _oracle_setup(oracle, w)
+    plan = _plan(dg, w)
+    plan.gather_variant = variant
+    assert plan.gather_variant == variant
+    frames = W.frames_torch(w, n, kind=w.kind)
+    flags = (N.DG_ERRORS if w.errors else 0) | (N.DG_AZIMUTHAL_STD if w.azimuthal_std else 0)
+    nb = w.n_points * max(1, w.n_azimuthal)
+    gi, gs, gd = _integrate_device(plan, frames, flags, nb)
+    host = frames.cpu().numpy()
+    yi, ys, yd = oracle.integrate_frames_mt(table, den, full, mask, norm, host, w.errors,
+                                            w.azimuthal_std, os.cpu_count() or 1)
+    if w.azimuthal_std:
+        valid = np.isfinite(yd)
+        assert np.array_equal(valid, np.isfinite(gd)), "NaN pattern of the spread differs"
+        assert _rel(gd, yd, valid & (yd != 0)).max() <= TOL_STD
+        assert np.all(gi[~valid] == 0) and np.all(gs[~valid] == 0)
+        nz = yi != 0
+    else:
+        nz = np.broadcast_to(den != 0, gi.shape)
+        assert np.all(gi[~nz] == 0) and np.all(gs[~nz] == 0)
+    assert _rel(gi, yi, nz & (yi != 0)).max() <= TOL_I
+    assert _rel(gs, ys, nz & (ys != 0)).max() <= TOL_I
     plan.close()

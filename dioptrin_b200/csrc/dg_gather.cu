@@ -535,7 +535,7 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
     constexpr int NA = NAcc<MODE, P>::value;
     constexpr bool SPREAD = MODE == kSpread;
     constexpr int NW = kRowsWarps;
-    const int2 *__restrict__ items = qp.item;
+    const int4 *__restrict__ items = qp.item;
     const int32_t *__restrict__ rows = qp.rows;
     const int32_t *__restrict__ row_ptr = qp.row_ptr;
     const int2 *__restrict__ entry = qp.entry;
@@ -552,17 +552,19 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
     double *__restrict__ out_i = qp.out_i;
     double *__restrict__ out_s = qp.out_s;
     double *__restrict__ out_d = qp.out_d;
-    const int2 it = items[k];
+    const int4 it = items[k];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // {first, 0}: one long row for the whole CTA; {first, n > 0}: a row per
-    // warp; {first, -n}: tiny rows, 8 lanes each (four per warp).
+    // {row, 0, begin, end}: one long row for the whole CTA, its entry range
+    // inline; {first, n > 0}: a row per warp; {first, -n}: tiny rows, 8 lanes
+    // each (four per warp), rows[first ..] and their row pointers.
     const bool whole = it.y == 0, tiny = it.y < 0;
     if (!whole && !tiny && warp >= it.y) return;  // no CTA-wide barrier in this case
     const int sub = int(threadIdx.x) >> 3;
     if (tiny && (sub & ~3) >= -it.y) return;  // a warp whose four rows are all past the end
     const bool live = !tiny || sub < -it.y;    // lanes past the end still shuffle
-    const int row = rows[it.x + (whole ? 0 : tiny ? (live ? sub : 0) : warp)];
-    const int e0 = row_ptr[row], e1 = live ? row_ptr[row + 1] : e0;
+    const int row = whole ? it.x : rows[it.x + (tiny ? (live ? sub : 0) : warp)];
+    const int e0 = whole ? it.z : row_ptr[row];
+    const int e1 = whole ? it.w : live ? row_ptr[row + 1] : e0;
     const int li = whole ? int(threadIdx.x) : tiny ? (lane & 7) : lane;
     const int nl = whole ? kRowsThreads : tiny ? 8 : 32;
     const int org = SPREAD ? origin_entry[row] : -1, fvalid = SPREAD ? first_valid[row] : -1;
@@ -3121,7 +3123,7 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
     // Row warps (mapping 10): long rows one per CTA, longest first; the
     // others eight per CTA in row order.
     std::vector<int32_t> rw_ptr, rw_rows;
-    std::vector<int2> rw_items;
+    std::vector<int4> rw_items;
     if (table.nnz <= INT32_MAX && nb > 0) {
         rw_ptr.assign(rp.begin(), rp.end());
         for (int64_t r = 0; r < nb; ++r)
@@ -3129,20 +3131,23 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
         std::stable_sort(rw_rows.begin(), rw_rows.end(), [&](int32_t a, int32_t b) {
             return rp[size_t(a) + 1] - rp[size_t(a)] > rp[size_t(b) + 1] - rp[size_t(b)];
         });
-        for (size_t i = 0; i < rw_rows.size(); ++i) rw_items.push_back(make_int2(int(i), 0));
+        for (size_t i = 0; i < rw_rows.size(); ++i) {  // long rows carry their range
+            const int32_t r = rw_rows[i];
+            rw_items.push_back(make_int4(r, 0, int(rp[size_t(r)]), int(rp[size_t(r) + 1])));
+        }
         auto len = [&](int64_t r) { return rp[size_t(r) + 1] - rp[size_t(r)]; };
         const size_t first_mid = rw_rows.size();
         for (int64_t r = 0; r < nb; ++r)
             if (len(r) <= kRowsLong && len(r) > kRowsTiny) rw_rows.push_back(int32_t(r));
         for (size_t i = first_mid; i < rw_rows.size(); i += kRowsWarps)
-            rw_items.push_back(make_int2(int(i), int(std::min<size_t>(kRowsWarps,
-                                                                      rw_rows.size() - i))));
+            rw_items.push_back(make_int4(int(i), int(std::min<size_t>(kRowsWarps,
+                                                                      rw_rows.size() - i)), 0, 0));
         const size_t first_tiny = rw_rows.size();
         for (int64_t r = 0; r < nb; ++r)
             if (len(r) <= kRowsTiny) rw_rows.push_back(int32_t(r));
         for (size_t i = first_tiny; i < rw_rows.size(); i += 4 * kRowsWarps)
-            rw_items.push_back(make_int2(int(i), -int(std::min<size_t>(4 * kRowsWarps,
-                                                                       rw_rows.size() - i))));
+            rw_items.push_back(make_int4(int(i), -int(std::min<size_t>(4 * kRowsWarps,
+                                                                       rw_rows.size() - i)), 0, 0));
         out.rw_row_ptr.alloc(rw_ptr.size());
         out.rw_rows.alloc(rw_rows.size());
         out.rw_item.alloc(rw_items.size());
@@ -3150,7 +3155,7 @@ void make_gather_table(const DeviceCsr &table, const double *d_norm, int32_t dim
                                 cudaMemcpyHostToDevice, s));
         DG_CUDA(cudaMemcpyAsync(out.rw_rows.ptr, rw_rows.data(), rw_rows.size() * 4,
                                 cudaMemcpyHostToDevice, s));
-        DG_CUDA(cudaMemcpyAsync(out.rw_item.ptr, rw_items.data(), rw_items.size() * sizeof(int2),
+        DG_CUDA(cudaMemcpyAsync(out.rw_item.ptr, rw_items.data(), rw_items.size() * sizeof(int4),
                                 cudaMemcpyHostToDevice, s));
         out.rw_n_items = int32_t(rw_items.size());
     }

@@ -305,8 +305,9 @@ struct GatherTable {
     BinTiles bt[2];
     // Row warps (k_rows), mapping 10: row pointers, rows with more than
     // kRowsLong entries (longest first) then the others, and one item per
-    // CTA: {first row in rw_rows, 0} for a long row, {first, count <= 8} for
-    // short rows taken one per warp.
+    // CTA: {row, 0, entry begin, entry end} for a long row, {first in
+    // rw_rows, count <= 8} for rows taken one per warp, {first, -count <= 32}
+    // for rows of at most kRowsTiny entries taken eight lanes each.
     int32_t rw_n_items = 0;
     // Per pixel (frame storage order) its norm n as an FP32 pair {n, n - n32},
     // {0, 0} where n is not finite or not positive: the row warps' spread
@@ -314,7 +315,7 @@ struct GatherTable {
     DeviceArray<float2> px_norm;
     DeviceArray<int32_t> rw_row_ptr;
     DeviceArray<int32_t> rw_rows;
-    DeviceArray<int2> rw_item;
+    DeviceArray<int4> rw_item;
     int variant = 0;                  // gather lane mapping (dg_gather.cu kVariantCount)
     int withhold_test = 0;            // bin tiles: stall one warp (dg_plan_test_wait_timeout)
     int32_t flip_rows = 0, flip_cols = 0;  // frames stored bottom row first (0: detector order)
@@ -355,7 +356,7 @@ void reserve_partials(GatherTable &t, int64_t n_frames, uint32_t flags, int dtyp
 // until total_items are done; item_first is the prefix index of a plan's
 // first tile.
 struct QueuePlan {
-    const int2 *item;
+    const int4 *item;
     const int32_t *rows;
     const int32_t *row_ptr;
     const int2 *entry;

@@ -663,7 +663,7 @@ int32_t dg_host_is_pinned(const void *ptr) {
 
 dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
                        uint32_t flags, double *oi, double *os, double *od) {
-    return guarded([&] {
+    const dg_status st = guarded([&] {
         check_frames(plan, frames, dtype, n_frames, flags, oi, os, od);
         if (n_frames == 0) return;
         std::lock_guard<std::mutex> lock(plan->mu);
@@ -672,26 +672,54 @@ dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t
         const int64_t npix = int64_t(plan->dim1) * plan->dim2;
         const size_t es = dtype_size(dtype);
         const int64_t nb = plan->n_bins;
-        const int64_t chunk = std::min<int64_t>(plan->max_batch_frames, n_frames);
+        // Two staging slots: chunk k + 1's frames cross the host link on the
+        // copy stream while the plan's stream gathers chunk k and returns its
+        // results, so the link never waits for a gather. The chunk budget
+        // counts 8 bytes a pixel, so two slots of max_batch_frames frames of
+        // at most 4-byte pixels fit it; 8-byte pixels take half as many.
+        const int64_t per_slot =
+            std::max<int64_t>(1, es <= 4 ? plan->max_batch_frames : plan->max_batch_frames / 2);
+        const int64_t chunk = std::min<int64_t>(per_slot, n_frames);
+        const int64_t n_chunks = (n_frames + chunk - 1) / chunk;
+        const int n_slots = n_chunks > 1 ? 2 : 1;
+        const size_t slot_bytes = (size_t(chunk * npix) * es + 255) / 256 * 256;
         const int nout = 1 + ((flags & DG_ERRORS) ? 1 : 0) + ((flags & DG_AZIMUTHAL_STD) ? 1 : 0);
-        if (plan->stage_in.count < size_t(chunk * npix * es)) {
+        if (plan->stage_in.count < n_slots * slot_bytes) {
             plan->stage_in.release();
-            plan->stage_in.alloc(size_t(chunk * npix * es));
+            plan->stage_in.alloc(n_slots * slot_bytes);
         }
         if (plan->stage_out.count < size_t(chunk * nb * nout)) {
             plan->stage_out.release();
             plan->stage_out.alloc(size_t(chunk * nb * nout));
         }
-        for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
-            const int64_t nf = std::min<int64_t>(chunk, n_frames - f0);
-            DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr,
+        dg::ensure_copy_pipeline(plan);
+        cudaStream_t cs = plan->copy_stream;
+        cudaEvent_t *copied = plan->bs_copied, *consumed = plan->bs_decoded;
+        // the copy stream starts after everything already queued on the plan
+        DG_CUDA(cudaEventRecord(consumed[0], s));
+        DG_CUDA(cudaStreamWaitEvent(cs, consumed[0], 0));
+        auto copy_in = [&](int64_t k) {
+            const int slot = int(k % n_slots);
+            // the slot's previous chunk must have been gathered
+            if (k >= n_slots) DG_CUDA(cudaStreamWaitEvent(cs, consumed[slot], 0));
+            const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
+            DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr + slot * slot_bytes,
                                     static_cast<const unsigned char *>(frames) + f0 * npix * es,
-                                    size_t(nf * npix * es), cudaMemcpyHostToDevice, s));
+                                    size_t(nf * npix) * es, cudaMemcpyHostToDevice, cs));
+            DG_CUDA(cudaEventRecord(copied[slot], cs));
+        };
+        copy_in(0);
+        for (int64_t k = 0; k < n_chunks; ++k) {
+            const int slot = int(k % n_slots);
+            const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
+            DG_CUDA(cudaStreamWaitEvent(s, copied[slot], 0));
+            if (k + 1 < n_chunks) copy_in(k + 1);
             double *di = plan->stage_out.ptr;
             double *ds = (flags & DG_ERRORS) ? di + nf * nb : nullptr;
             double *dd = (flags & DG_AZIMUTHAL_STD) ? di + nf * nb * (ds ? 2 : 1) : nullptr;
-            dg::run_gather(plan->gather, plan->stage_in.ptr, dtype, npix, nf, flags,
-                           plan->method.precision, di, ds, dd, s);
+            dg::run_gather(plan->gather, plan->stage_in.ptr + slot * slot_bytes, dtype, npix, nf,
+                           flags, plan->method.precision, di, ds, dd, s);
+            DG_CUDA(cudaEventRecord(consumed[slot], s));
             DG_CUDA(cudaMemcpyAsync(oi + f0 * nb, di, size_t(nf * nb) * 8, cudaMemcpyDeviceToHost, s));
             if (ds)
                 DG_CUDA(cudaMemcpyAsync(os + f0 * nb, ds, size_t(nf * nb) * 8,
@@ -703,6 +731,13 @@ dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t
         DG_CUDA(cudaStreamSynchronize(s));
         dg::check_bin_tile_waits(plan->gather);
     });
+    if (st != DG_OK && plan) {
+        // leave nothing of this call in flight (queued copies read the
+        // caller's frames until they complete)
+        if (plan->copy_stream) cudaStreamSynchronize(plan->copy_stream);
+        if (plan->stream) cudaStreamSynchronize(plan->stream);
+    }
+    return st;
 }
 
 dg_status dg_plan_profile(dg_plan *plan, int32_t enable) {

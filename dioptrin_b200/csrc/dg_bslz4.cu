@@ -501,6 +501,17 @@ void bslz4_release(dg_plan *plan) {
     plan->copy_stream = nullptr;
 }
 
+void ensure_copy_pipeline(dg_plan *plan) {
+    if (!plan->copy_stream)
+        DG_CUDA(cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+        if (!plan->bs_copied[k])
+            DG_CUDA(cudaEventCreateWithFlags(&plan->bs_copied[k], cudaEventDisableTiming));
+        if (!plan->bs_decoded[k])
+            DG_CUDA(cudaEventCreateWithFlags(&plan->bs_decoded[k], cudaEventDisableTiming));
+    }
+}
+
 }  // namespace dg
 
 extern "C" {
@@ -657,14 +668,7 @@ dg_status dg_integrate_bslz4(dg_plan *plan, const void *const *chunks, const int
             plan->stage_desc.release();
             plan->stage_desc.alloc(n_slots * desc_slot + 256);
         }
-        if (!plan->copy_stream)
-            DG_CUDA(cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking));
-        for (int k = 0; k < 2; ++k) {
-            if (!plan->bs_copied[k])
-                DG_CUDA(cudaEventCreateWithFlags(&plan->bs_copied[k], cudaEventDisableTiming));
-            if (!plan->bs_decoded[k])
-                DG_CUDA(cudaEventCreateWithFlags(&plan->bs_decoded[k], cudaEventDisableTiming));
-        }
+        ensure_copy_pipeline(plan);
         cudaStream_t s = plan->stream, cs = plan->copy_stream;
         int *d_err = reinterpret_cast<int *>(plan->stage_desc.ptr + n_slots * desc_slot);
         DG_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s));

@@ -446,6 +446,9 @@ struct dg_plan;
 namespace dg {
 // Frees the Bitshuffle/LZ4 staging, copy stream and events of a plan (dg_bslz4.cu).
 void bslz4_release(dg_plan *plan);
+// Creates the plan's copy stream and its two pairs of slot events if missing
+// (dg_bslz4.cu).
+void ensure_copy_pipeline(dg_plan *plan);
 }  // namespace dg
 
 struct dg_plan {
@@ -473,7 +476,10 @@ struct dg_plan {
     // compressed frames and their block descriptors (dg_integrate_bslz4)
     dg::DeviceArray<unsigned char> stage_comp;
     dg::DeviceArray<unsigned char> stage_desc;
-    cudaStream_t copy_stream = nullptr;  // compressed-frame copies
+    // Host-to-device copies of the two-slot host pipelines (dg_integrate's
+    // frames, dg_integrate_bslz4's compressed bytes): per slot, copied (the
+    // slot landed) and decoded (the device is done reading it).
+    cudaStream_t copy_stream = nullptr;
     cudaEvent_t bs_copied[2] = {nullptr, nullptr};
     cudaEvent_t bs_decoded[2] = {nullptr, nullptr};
     dg::EventPool decode_events;  // decode-kernel timing (dg_plan_decode_time)

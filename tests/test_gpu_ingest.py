@@ -138,3 +138,40 @@ def test_flip_vertical_per_frame_masks_on_bin_tiles(dg):
             (b.sum_signal, b.sum_norm, b.sum_variance, b.count))
     det.close()
     flip.close()
+
+
+@pytest.mark.parametrize("dtype", [np.uint16, np.uint32, np.int32, np.float32, np.float64])
+def test_host_frames_in_two_slot_chunks_equal_device_frames(dg, dtype):
+    # dg_integrate copies host frames through two staging slots (the next
+    # chunk crosses the host link while the current one is gathered). A
+    # small chunk budget makes 11 frames take several chunks in both slots,
+    # with a short last chunk; the results must equal the same frames
+    # integrated from device memory in one call, bit for bit.
+    import ctypes as C
+
+    import torch
+    from dioptrin_b200 import _native as N
+    it = _integrator(dg)
+    nb = 70
+    per_frame = SHAPE[0] * SHAPE[1] * 8 + nb * 24
+    plan = it.prepare_cuda1d(SHAPE, nb, max_batch_bytes=3 * per_frame)
+    assert plan.max_batch_frames == 3
+    gen = np.random.default_rng(5)
+    frames = gen.poisson(60.0, (11,) + SHAPE).astype(dtype)
+    flags = N.DG_ERRORS | N.DG_AZIMUTHAL_STD
+    host = plan.integrate_stack(frames, errors=True, azimuthal_std=True)
+    codes = {np.uint16: N.DG_U16, np.uint32: N.DG_U32, np.int32: N.DG_I32,
+             np.float32: N.DG_F32, np.float64: N.DG_F64}
+    tdt = {np.uint16: torch.uint16, np.uint32: torch.uint32, np.int32: torch.int32,
+           np.float32: torch.float32, np.float64: torch.float64}[dtype]
+    dev = torch.from_numpy(frames.view(np.int16) if dtype == np.uint16 else frames)
+    dev = dev.view(tdt).cuda()
+    out = [torch.full((11, nb), -7.0, dtype=torch.float64, device="cuda") for _ in range(3)]
+    torch.cuda.synchronize()
+    N.check(N.lib().dg_integrate_device(plan.handle, C.c_void_p(dev.data_ptr()), codes[dtype], 11,
+                                        flags, *[C.c_void_p(o.data_ptr()) for o in out], None))
+    torch.cuda.synchronize()
+    _eq(host, [o.cpu().numpy() for o in out])
+    # a second call reuses the slots and the copy stream
+    _eq(plan.integrate_stack(frames, errors=True, azimuthal_std=True), host)
+    plan.close()

@@ -818,6 +818,29 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async4_s(unsigned d, const void *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
+// L2 eviction priority of the bin tiles' 4-byte pixel copies: 0 the default
+// policy, 1 evict-first (frame sectors stream through L2 and leave it to the
+// entry-pair records that a tile's frame groups share), 2 evict-last.
+#ifndef DG_BT_L2HINT
+#define DG_BT_L2HINT 0
+#endif
+__device__ __forceinline__ uint64_t bt_l2_policy() {
+    uint64_t p = 0;
+    if constexpr (DG_BT_L2HINT == 1)
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+    else if constexpr (DG_BT_L2HINT == 2)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void cp_async4_sp(unsigned d, const void *src, uint64_t policy) {
+    if constexpr (DG_BT_L2HINT == 0) {
+        cp_async4_s(d, src);
+    } else {
+        asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;\n" ::"r"(d),
+                     "l"(src), "l"(policy)
+                     : "memory");
+    }
+}
 __device__ __forceinline__ uint32_t lds32(unsigned a) {
     uint32_t v;
     asm volatile("ld.shared.b32 %0, [%1];\n" : "=r"(v) : "r"(a));
@@ -1711,6 +1734,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
     // The first of two halves of staging chunk c: mask loads and copies.
     // The frames this warp stages (4-byte pixels), found once per tile.
     const P *stage_frame[FS];
+    const uint64_t l2pol = bt_l2_policy();
 #pragma unroll
     for (int j = 0; j < FS; ++j)
         stage_frame[j] = frames + int64_t(f0 + min(warp / KS + j * FSTEP, max(nv - 1, 0))) * n_pixels;
@@ -1766,7 +1790,7 @@ __global__ void __launch_bounds__(CFG::kThreads, 1)
                 constexpr unsigned kStep = 4u * (PAIRED ? 64u : 32u);  // 32 slots on
 #pragma unroll
                 for (int i = 0; i < KSTEP; ++i)
-                    if (kin[i]) cp_async4_s(drow + kStep * unsigned(i), fsrc + boff[i]);
+                    if (kin[i]) cp_async4_sp(drow + kStep * unsigned(i), fsrc + boff[i], l2pol);
 #else
                 const P *fsrc = base + int64_t(j * FSTEP) * n_pixels;
                 int idx[KSTEP];

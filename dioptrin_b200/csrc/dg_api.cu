@@ -517,47 +517,92 @@ void run_masked_host(dg_plan *plan, const void *frames, int32_t dtype, int64_t n
     const int64_t npix = int64_t(plan->dim1) * plan->dim2;
     const size_t es = dtype_size(dtype);
     const int64_t nb = plan->n_bins;
-    const int64_t chunk = std::min<int64_t>(plan->max_batch_frames, n_frames);
+    // Two staging slots of frames (and of per-frame masks), as in
+    // dg_integrate: chunk k + 1 is copied on the copy stream while chunk k is
+    // gathered. Two slots of max_batch_frames frames fit the chunk budget
+    // (8 bytes a pixel) while a frame and its mask take at most 4 bytes a
+    // pixel; otherwise each slot holds half as many.
+    const size_t per_px = es + ((masks && mask_stride) ? 1 : 0);
+    const int64_t per_slot =
+        std::max<int64_t>(1, per_px <= 4 ? plan->max_batch_frames : plan->max_batch_frames / 2);
+    const int64_t chunk = std::min<int64_t>(per_slot, n_frames);
+    const int64_t n_chunks = (n_frames + chunk - 1) / chunk;
+    const int n_slots = n_chunks > 1 ? 2 : 1;
+    const size_t slot_bytes = (size_t(chunk * npix) * es + 255) / 256 * 256;
     const int nout = raw ? 4 : 2;
-    if (plan->stage_in.count < size_t(chunk * npix * es)) {
+    if (plan->stage_in.count < n_slots * slot_bytes) {
         plan->stage_in.release();
-        plan->stage_in.alloc(size_t(chunk * npix * es));
+        plan->stage_in.alloc(n_slots * slot_bytes);
     }
     if (plan->stage_out.count < size_t(chunk * nb * nout)) {
         plan->stage_out.release();
         plan->stage_out.alloc(size_t(chunk * nb * nout));
     }
-    const int64_t mask_rows = masks ? (mask_stride ? chunk : 1) : 0;
-    if (plan->stage_mask.count < size_t(mask_rows * npix)) {
+    // per-frame masks: a slot of chunk rows each; one plan-wide mask: one row
+    const size_t mask_slot = (masks && mask_stride) ? (size_t(chunk * npix) + 255) / 256 * 256 : 0;
+    const size_t mask_bytes = masks ? (mask_stride ? n_slots * mask_slot : size_t(npix)) : 0;
+    if (plan->stage_mask.count < mask_bytes) {
         plan->stage_mask.release();
-        plan->stage_mask.alloc(size_t(mask_rows * npix));
+        plan->stage_mask.alloc(mask_bytes);
     }
     dg::prepare_raw(plan->gather, plan->table, plan->norm.ptr, s);
     if (masks && !mask_stride)
         DG_CUDA(cudaMemcpyAsync(plan->stage_mask.ptr, masks, size_t(npix), cudaMemcpyHostToDevice, s));
-    for (int64_t f0 = 0; f0 < n_frames; f0 += chunk) {
-        const int64_t nf = std::min<int64_t>(chunk, n_frames - f0);
-        DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr,
+    dg::ensure_copy_pipeline(plan);
+    cudaStream_t cs = plan->copy_stream;
+    cudaEvent_t *copied = plan->bs_copied, *consumed = plan->bs_decoded;
+    // On an error, nothing of this call stays in flight (queued copies read
+    // the caller's frames and masks until they complete).
+    struct Drain {
+        cudaStream_t a, b;
+        bool done = false;
+        ~Drain() {
+            if (!done) {
+                cudaStreamSynchronize(a);
+                cudaStreamSynchronize(b);
+            }
+        }
+    } drain{cs, s};
+    // the copy stream starts after everything already queued on the plan
+    DG_CUDA(cudaEventRecord(consumed[0], s));
+    DG_CUDA(cudaStreamWaitEvent(cs, consumed[0], 0));
+    auto copy_in = [&](int64_t k) {
+        const int slot = int(k % n_slots);
+        // the slot's previous chunk must have been gathered
+        if (k >= n_slots) DG_CUDA(cudaStreamWaitEvent(cs, consumed[slot], 0));
+        const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
+        DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr + slot * slot_bytes,
                                 static_cast<const unsigned char *>(frames) + f0 * npix * es,
-                                size_t(nf * npix * es), cudaMemcpyHostToDevice, s));
+                                size_t(nf * npix) * es, cudaMemcpyHostToDevice, cs));
         if (masks && mask_stride)
-            DG_CUDA(cudaMemcpy2DAsync(plan->stage_mask.ptr, size_t(npix), masks + f0 * mask_stride,
-                                      size_t(mask_stride), size_t(npix), size_t(nf),
-                                      cudaMemcpyHostToDevice, s));
+            DG_CUDA(cudaMemcpy2DAsync(plan->stage_mask.ptr + slot * mask_slot, size_t(npix),
+                                      masks + f0 * mask_stride, size_t(mask_stride), size_t(npix),
+                                      size_t(nf), cudaMemcpyHostToDevice, cs));
+        DG_CUDA(cudaEventRecord(copied[slot], cs));
+    };
+    copy_in(0);
+    for (int64_t k = 0; k < n_chunks; ++k) {
+        const int slot = int(k % n_slots);
+        const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
+        DG_CUDA(cudaStreamWaitEvent(s, copied[slot], 0));
+        if (k + 1 < n_chunks) copy_in(k + 1);
         double *d[4];
-        for (int k = 0; k < 4; ++k) d[k] = plan->stage_out.ptr + k * nf * nb;
+        for (int q = 0; q < 4; ++q) d[q] = plan->stage_out.ptr + q * nf * nb;
         double *h[4] = {o0, o1, o2, o3};
         const bool used[4] = {true, raw || (flags & DG_ERRORS), raw && (flags & DG_ERRORS), raw};
-        dg::run_gather_raw(plan->gather, plan->stage_in.ptr, dtype, npix, nf,
-                           masks ? plan->stage_mask.ptr : nullptr, mask_stride ? npix : 0, flags,
-                           raw, d[0], used[1] ? d[1] : nullptr, used[2] ? d[2] : nullptr,
-                           used[3] ? d[3] : nullptr, s);
-        for (int k = 0; k < 4; ++k)
-            if (used[k])
-                DG_CUDA(cudaMemcpyAsync(h[k] + f0 * nb, d[k], size_t(nf * nb) * 8,
+        const uint8_t *dm = masks ? plan->stage_mask.ptr + (mask_stride ? slot * mask_slot : 0)
+                                  : nullptr;
+        dg::run_gather_raw(plan->gather, plan->stage_in.ptr + slot * slot_bytes, dtype, npix, nf,
+                           dm, mask_stride ? npix : 0, flags, raw, d[0], used[1] ? d[1] : nullptr,
+                           used[2] ? d[2] : nullptr, used[3] ? d[3] : nullptr, s);
+        DG_CUDA(cudaEventRecord(consumed[slot], s));
+        for (int q = 0; q < 4; ++q)
+            if (used[q])
+                DG_CUDA(cudaMemcpyAsync(h[q] + f0 * nb, d[q], size_t(nf * nb) * 8,
                                         cudaMemcpyDeviceToHost, s));
     }
     DG_CUDA(cudaStreamSynchronize(s));
+    drain.done = true;
 }
 
 }  // namespace

@@ -175,3 +175,58 @@ def test_host_frames_in_two_slot_chunks_equal_device_frames(dg, dtype):
     # a second call reuses the slots and the copy stream
     _eq(plan.integrate_stack(frames, errors=True, azimuthal_std=True), host)
     plan.close()
+
+
+@pytest.mark.parametrize("dtype", [np.uint32, np.float64])
+def test_masked_and_raw_host_calls_in_two_slot_chunks(dg, dtype):
+    # dg_integrate_dynamic and dg_integrate_raw stage host frames and their
+    # per-frame masks through the same two slots; with a small chunk budget
+    # 11 frames take several chunks. Results equal the device-memory calls
+    # on the same frames and masks bit for bit, for per-frame masks, for one
+    # shared mask and (raw sums) for none.
+    import ctypes as C
+
+    import torch
+    from dioptrin_b200 import _native as N
+    it = _integrator(dg, mask=False)
+    nb = 70
+    per_frame = SHAPE[0] * SHAPE[1] * 8 + nb * 24
+    plan = it.prepare_cuda1d(SHAPE, nb, max_batch_bytes=4 * per_frame)
+    gen = np.random.default_rng(9)
+    n = 11
+    frames = gen.poisson(50.0, (n,) + SHAPE).astype(dtype)
+    masks = (gen.random((n,) + SHAPE) < 0.1).astype(np.uint8)
+    code = N.DG_U32 if dtype == np.uint32 else N.DG_F64
+    tdt = torch.uint32 if dtype == np.uint32 else torch.float64
+    dframes = torch.from_numpy(frames).view(tdt).cuda()
+    dmasks = torch.from_numpy(masks).cuda()
+    npix = SHAPE[0] * SHAPE[1]
+    L = N.lib()
+    vp = C.c_void_p
+    for mask_kind in ("per_frame", "shared", "none"):
+        hm = masks if mask_kind == "per_frame" else masks[:1] if mask_kind == "shared" else None
+        stride = npix if mask_kind == "per_frame" else 0
+        dm = None if hm is None else vp(dmasks.data_ptr())
+        hmp = None if hm is None else vp(np.ascontiguousarray(hm).ctypes.data)
+        for raw in (False, True):
+            if hm is None and not raw:
+                continue  # per-frame-mask calls need a mask
+            k = 4 if raw else 2
+            host = [np.full((n, nb), -7.0) for _ in range(k)]
+            dev = [torch.full((n, nb), -7.0, dtype=torch.float64, device="cuda") for _ in range(k)]
+            hp = [h.ctypes.data_as(C.POINTER(C.c_double)) for h in host]
+            dp = [vp(d.data_ptr()) for d in dev]
+            torch.cuda.synchronize()
+            if raw:
+                N.check(L.dg_integrate_raw(plan.handle, vp(frames.ctypes.data), code, n, hmp, stride,
+                                           N.DG_ERRORS, *hp))
+                N.check(L.dg_integrate_raw_device(plan.handle, vp(dframes.data_ptr()), code, n, dm,
+                                                  stride, N.DG_ERRORS, *dp, None))
+            else:
+                N.check(L.dg_integrate_dynamic(plan.handle, vp(frames.ctypes.data), code, n, hmp,
+                                               stride, N.DG_ERRORS, *hp))
+                N.check(L.dg_integrate_dynamic_device(plan.handle, vp(dframes.data_ptr()), code, n,
+                                                      dm, stride, N.DG_ERRORS, *dp, None))
+            torch.cuda.synchronize()
+            _eq(host, [d.cpu().numpy() for d in dev])
+    plan.close()

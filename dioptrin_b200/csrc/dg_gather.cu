@@ -700,8 +700,18 @@ __device__ __forceinline__ void rows_item(const QueuePlan &qp, int k, int fb, Ro
 }
 
 // Lane mapping 10 for one plan's batch: one CTA per (item, frame block).
+// Resident CTAs per SM the compiler must allow for (0: as many as the
+// registers it chooses leave; the spread's one-frame form takes 64, four CTAs).
+#ifndef DG_ROWS_MINB
+#define DG_ROWS_MINB 0
+#endif
+#if DG_ROWS_MINB > 0
+#define DG_ROWS_BOUNDS __launch_bounds__(kRowsThreads, DG_ROWS_MINB)
+#else
+#define DG_ROWS_BOUNDS __launch_bounds__(kRowsThreads)
+#endif
 template <int MODE, typename P, int F>
-__global__ void __launch_bounds__(kRowsThreads) k_rows(const QueuePlan q) {
+__global__ void DG_ROWS_BOUNDS k_rows(const QueuePlan q) {
     __shared__ RowsRed s_red;
     rows_item<MODE, P, F>(q, blockIdx.x, blockIdx.y, s_red);
 }

@@ -59,6 +59,7 @@ struct PlanSpec {
 struct PinnedPool {
     std::mutex mu;
     std::unordered_map<size_t, std::vector<void *>> free;
+    std::unordered_map<size_t, size_t> made;  // buffers allocated, by size
     void *get(size_t bytes) {
         {
             std::lock_guard<std::mutex> lock(mu);
@@ -68,13 +69,37 @@ struct PinnedPool {
                 v.pop_back();
                 return p;
             }
+            made[bytes]++;
         }
         void *p = nullptr;
         if (cudaMallocHost(&p, bytes) != cudaSuccess) {
             (void)cudaGetLastError();
+            std::lock_guard<std::mutex> lock(mu);
+            made[bytes]--;
             return nullptr;
         }
         return p;
+    }
+    // Allocates buffers of `bytes` until `count` of that size exist, the new
+    // ones free. A page-locked allocation is slow and keeps copies on other
+    // streams from overlapping it, so it belongs before a stream's requests
+    // rather than on a worker's path.
+    void reserve(size_t bytes, size_t count) {
+        for (;;) {
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                if (made[bytes] >= count) return;
+                made[bytes]++;
+            }
+            void *p = nullptr;
+            if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+                (void)cudaGetLastError();
+                std::lock_guard<std::mutex> lock(mu);
+                made[bytes]--;
+                return;
+            }
+            put(bytes, p);
+        }
     }
     void put(size_t bytes, void *p) {
         if (!p) return;
@@ -286,6 +311,16 @@ struct dg_server {
                     dg::reserve_partials(plan->gather, 1, hint.second, hint.first);
                 } catch (const dg::Error &) {
                 }
+            }
+            // Result buffers for the plan's requests, page-locked now: as many
+            // as the workers' batches hold at once, at most 1 GiB of them (a
+            // rebuilt key with the same bins finds its buffers made already).
+            {
+                const int nout = 1 + ((hint.second & DG_ERRORS) ? 1 : 0) +
+                                 ((hint.second & DG_AZIMUTHAL_STD) ? 1 : 0);
+                const size_t bytes = size_t(nout) * size_t(spec.n_bins()) * 8;
+                const size_t want = size_t(kWorkers) * size_t(std::max(cfg.max_coalesce, 1)) + 16;
+                pinned.reserve(bytes, std::min(want, std::max<size_t>(1, (size_t(1) << 30) / bytes)));
             }
             dg_plan_info info{};
             dg_plan_query(plan, &info);

@@ -506,8 +506,58 @@ void check_masked(const dg_plan *plan, const void *frames, int32_t dtype, int64_
     }
 }
 
+// Runs the n_chunks chunks of a host-memory call through two staging slots
+// (one when there is a single chunk): copy_in(k, slot, cs) queues chunk k's
+// host-to-device copies on the plan's copy stream, gather(k, slot, s) its
+// kernels on the plan's stream and results(k, s) the copies of its results
+// back. Chunk k + 1's copies are queued before chunk k's gather, and a slot
+// is copied into again only once the gather that read it has run, so the
+// host link never waits for a gather. On an error nothing of the call stays
+// in flight (queued copies read the caller's buffers until they complete).
+extern "C++" {  // a template inside the C-ABI block
+template <class CopyIn, class Gather, class Results>
+void run_two_slots(dg_plan *plan, int64_t n_chunks, CopyIn copy_in, Gather gather,
+                   Results results) {
+    cudaStream_t s = plan->stream;
+    dg::ensure_copy_pipeline(plan);
+    cudaStream_t cs = plan->copy_stream;
+    cudaEvent_t *copied = plan->bs_copied, *consumed = plan->bs_decoded;
+    const int n_slots = n_chunks > 1 ? 2 : 1;
+    struct Drain {
+        cudaStream_t a, b;
+        bool done = false;
+        ~Drain() {
+            if (!done) {
+                cudaStreamSynchronize(a);
+                cudaStreamSynchronize(b);
+            }
+        }
+    } drain{cs, s};
+    // the copy stream starts after everything already queued on the plan
+    DG_CUDA(cudaEventRecord(consumed[0], s));
+    DG_CUDA(cudaStreamWaitEvent(cs, consumed[0], 0));
+    auto issue = [&](int64_t k) {
+        const int slot = int(k % n_slots);
+        if (k >= n_slots) DG_CUDA(cudaStreamWaitEvent(cs, consumed[slot], 0));
+        copy_in(k, slot, cs);
+        DG_CUDA(cudaEventRecord(copied[slot], cs));
+    };
+    issue(0);
+    for (int64_t k = 0; k < n_chunks; ++k) {
+        const int slot = int(k % n_slots);
+        DG_CUDA(cudaStreamWaitEvent(s, copied[slot], 0));
+        if (k + 1 < n_chunks) issue(k + 1);
+        gather(k, slot, s);
+        DG_CUDA(cudaEventRecord(consumed[slot], s));
+        results(k, s);
+    }
+    DG_CUDA(cudaStreamSynchronize(s));
+    drain.done = true;
+}
+}  // extern "C++"
+
 // Host-memory form of the masked / raw calls: frames, masks and results
-// staged through the plan's buffers in chunks of max_batch_frames.
+// staged through the plan's buffers in chunks, two slots (run_two_slots).
 void run_masked_host(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
                      const uint8_t *masks, int64_t mask_stride, uint32_t flags, bool raw,
                      double *o0, double *o1, double *o2, double *o3) {
@@ -548,61 +598,39 @@ void run_masked_host(dg_plan *plan, const void *frames, int32_t dtype, int64_t n
     dg::prepare_raw(plan->gather, plan->table, plan->norm.ptr, s);
     if (masks && !mask_stride)
         DG_CUDA(cudaMemcpyAsync(plan->stage_mask.ptr, masks, size_t(npix), cudaMemcpyHostToDevice, s));
-    dg::ensure_copy_pipeline(plan);
-    cudaStream_t cs = plan->copy_stream;
-    cudaEvent_t *copied = plan->bs_copied, *consumed = plan->bs_decoded;
-    // On an error, nothing of this call stays in flight (queued copies read
-    // the caller's frames and masks until they complete).
-    struct Drain {
-        cudaStream_t a, b;
-        bool done = false;
-        ~Drain() {
-            if (!done) {
-                cudaStreamSynchronize(a);
-                cudaStreamSynchronize(b);
-            }
-        }
-    } drain{cs, s};
-    // the copy stream starts after everything already queued on the plan
-    DG_CUDA(cudaEventRecord(consumed[0], s));
-    DG_CUDA(cudaStreamWaitEvent(cs, consumed[0], 0));
-    auto copy_in = [&](int64_t k) {
-        const int slot = int(k % n_slots);
-        // the slot's previous chunk must have been gathered
-        if (k >= n_slots) DG_CUDA(cudaStreamWaitEvent(cs, consumed[slot], 0));
-        const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
-        DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr + slot * slot_bytes,
-                                static_cast<const unsigned char *>(frames) + f0 * npix * es,
-                                size_t(nf * npix) * es, cudaMemcpyHostToDevice, cs));
-        if (masks && mask_stride)
-            DG_CUDA(cudaMemcpy2DAsync(plan->stage_mask.ptr + slot * mask_slot, size_t(npix),
-                                      masks + f0 * mask_stride, size_t(mask_stride), size_t(npix),
-                                      size_t(nf), cudaMemcpyHostToDevice, cs));
-        DG_CUDA(cudaEventRecord(copied[slot], cs));
-    };
-    copy_in(0);
-    for (int64_t k = 0; k < n_chunks; ++k) {
-        const int slot = int(k % n_slots);
-        const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
-        DG_CUDA(cudaStreamWaitEvent(s, copied[slot], 0));
-        if (k + 1 < n_chunks) copy_in(k + 1);
-        double *d[4];
-        for (int q = 0; q < 4; ++q) d[q] = plan->stage_out.ptr + q * nf * nb;
-        double *h[4] = {o0, o1, o2, o3};
-        const bool used[4] = {true, raw || (flags & DG_ERRORS), raw && (flags & DG_ERRORS), raw};
-        const uint8_t *dm = masks ? plan->stage_mask.ptr + (mask_stride ? slot * mask_slot : 0)
-                                  : nullptr;
-        dg::run_gather_raw(plan->gather, plan->stage_in.ptr + slot * slot_bytes, dtype, npix, nf,
-                           dm, mask_stride ? npix : 0, flags, raw, d[0], used[1] ? d[1] : nullptr,
-                           used[2] ? d[2] : nullptr, used[3] ? d[3] : nullptr, s);
-        DG_CUDA(cudaEventRecord(consumed[slot], s));
-        for (int q = 0; q < 4; ++q)
-            if (used[q])
-                DG_CUDA(cudaMemcpyAsync(h[q] + f0 * nb, d[q], size_t(nf * nb) * 8,
-                                        cudaMemcpyDeviceToHost, s));
-    }
-    DG_CUDA(cudaStreamSynchronize(s));
-    drain.done = true;
+    const bool used[4] = {true, raw || (flags & DG_ERRORS), raw && (flags & DG_ERRORS), raw};
+    double *const h[4] = {o0, o1, o2, o3};
+    auto frames_of = [&](int64_t k) { return std::min<int64_t>(chunk, n_frames - k * chunk); };
+    run_two_slots(
+        plan, n_chunks,
+        [&](int64_t k, int slot, cudaStream_t cs) {
+            const int64_t f0 = k * chunk, nf = frames_of(k);
+            DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr + slot * slot_bytes,
+                                    static_cast<const unsigned char *>(frames) + f0 * npix * es,
+                                    size_t(nf * npix) * es, cudaMemcpyHostToDevice, cs));
+            if (masks && mask_stride)
+                DG_CUDA(cudaMemcpy2DAsync(plan->stage_mask.ptr + slot * mask_slot, size_t(npix),
+                                          masks + f0 * mask_stride, size_t(mask_stride),
+                                          size_t(npix), size_t(nf), cudaMemcpyHostToDevice, cs));
+        },
+        [&](int64_t k, int slot, cudaStream_t gs) {
+            const int64_t nf = frames_of(k);
+            double *d[4];
+            for (int q = 0; q < 4; ++q) d[q] = plan->stage_out.ptr + q * nf * nb;
+            const uint8_t *dm =
+                masks ? plan->stage_mask.ptr + (mask_stride ? slot * mask_slot : 0) : nullptr;
+            dg::run_gather_raw(plan->gather, plan->stage_in.ptr + slot * slot_bytes, dtype, npix,
+                               nf, dm, mask_stride ? npix : 0, flags, raw, d[0],
+                               used[1] ? d[1] : nullptr, used[2] ? d[2] : nullptr,
+                               used[3] ? d[3] : nullptr, gs);
+        },
+        [&](int64_t k, cudaStream_t gs) {
+            const int64_t f0 = k * chunk, nf = frames_of(k);
+            for (int q = 0; q < 4; ++q)
+                if (used[q])
+                    DG_CUDA(cudaMemcpyAsync(h[q] + f0 * nb, plan->stage_out.ptr + q * nf * nb,
+                                            size_t(nf * nb) * 8, cudaMemcpyDeviceToHost, gs));
+        });
 }
 
 }  // namespace
@@ -708,12 +736,11 @@ int32_t dg_host_is_pinned(const void *ptr) {
 
 dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t n_frames,
                        uint32_t flags, double *oi, double *os, double *od) {
-    const dg_status st = guarded([&] {
+    return guarded([&] {
         check_frames(plan, frames, dtype, n_frames, flags, oi, os, od);
         if (n_frames == 0) return;
         std::lock_guard<std::mutex> lock(plan->mu);
         DeviceScope scope(plan->device);
-        cudaStream_t s = plan->stream;
         const int64_t npix = int64_t(plan->dim1) * plan->dim2;
         const size_t es = dtype_size(dtype);
         const int64_t nb = plan->n_bins;
@@ -737,52 +764,40 @@ dg_status dg_integrate(dg_plan *plan, const void *frames, int32_t dtype, int64_t
             plan->stage_out.release();
             plan->stage_out.alloc(size_t(chunk * nb * nout));
         }
-        dg::ensure_copy_pipeline(plan);
-        cudaStream_t cs = plan->copy_stream;
-        cudaEvent_t *copied = plan->bs_copied, *consumed = plan->bs_decoded;
-        // the copy stream starts after everything already queued on the plan
-        DG_CUDA(cudaEventRecord(consumed[0], s));
-        DG_CUDA(cudaStreamWaitEvent(cs, consumed[0], 0));
-        auto copy_in = [&](int64_t k) {
-            const int slot = int(k % n_slots);
-            // the slot's previous chunk must have been gathered
-            if (k >= n_slots) DG_CUDA(cudaStreamWaitEvent(cs, consumed[slot], 0));
-            const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
-            DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr + slot * slot_bytes,
-                                    static_cast<const unsigned char *>(frames) + f0 * npix * es,
-                                    size_t(nf * npix) * es, cudaMemcpyHostToDevice, cs));
-            DG_CUDA(cudaEventRecord(copied[slot], cs));
+        auto frames_of = [&](int64_t k) { return std::min<int64_t>(chunk, n_frames - k * chunk); };
+        auto outs = [&](int64_t k, double **d) {
+            const int64_t nf = frames_of(k);
+            d[0] = plan->stage_out.ptr;
+            d[1] = (flags & DG_ERRORS) ? d[0] + nf * nb : nullptr;
+            d[2] = (flags & DG_AZIMUTHAL_STD) ? d[0] + nf * nb * (d[1] ? 2 : 1) : nullptr;
         };
-        copy_in(0);
-        for (int64_t k = 0; k < n_chunks; ++k) {
-            const int slot = int(k % n_slots);
-            const int64_t f0 = k * chunk, nf = std::min<int64_t>(chunk, n_frames - f0);
-            DG_CUDA(cudaStreamWaitEvent(s, copied[slot], 0));
-            if (k + 1 < n_chunks) copy_in(k + 1);
-            double *di = plan->stage_out.ptr;
-            double *ds = (flags & DG_ERRORS) ? di + nf * nb : nullptr;
-            double *dd = (flags & DG_AZIMUTHAL_STD) ? di + nf * nb * (ds ? 2 : 1) : nullptr;
-            dg::run_gather(plan->gather, plan->stage_in.ptr + slot * slot_bytes, dtype, npix, nf,
-                           flags, plan->method.precision, di, ds, dd, s);
-            DG_CUDA(cudaEventRecord(consumed[slot], s));
-            DG_CUDA(cudaMemcpyAsync(oi + f0 * nb, di, size_t(nf * nb) * 8, cudaMemcpyDeviceToHost, s));
-            if (ds)
-                DG_CUDA(cudaMemcpyAsync(os + f0 * nb, ds, size_t(nf * nb) * 8,
-                                        cudaMemcpyDeviceToHost, s));
-            if (dd)
-                DG_CUDA(cudaMemcpyAsync(od + f0 * nb, dd, size_t(nf * nb) * 8,
-                                        cudaMemcpyDeviceToHost, s));
-        }
-        DG_CUDA(cudaStreamSynchronize(s));
+        run_two_slots(
+            plan, n_chunks,
+            [&](int64_t k, int slot, cudaStream_t cs) {
+                DG_CUDA(cudaMemcpyAsync(plan->stage_in.ptr + slot * slot_bytes,
+                                        static_cast<const unsigned char *>(frames) +
+                                            k * chunk * npix * es,
+                                        size_t(frames_of(k) * npix) * es, cudaMemcpyHostToDevice,
+                                        cs));
+            },
+            [&](int64_t k, int slot, cudaStream_t gs) {
+                double *d[3];
+                outs(k, d);
+                dg::run_gather(plan->gather, plan->stage_in.ptr + slot * slot_bytes, dtype, npix,
+                               frames_of(k), flags, plan->method.precision, d[0], d[1], d[2], gs);
+            },
+            [&](int64_t k, cudaStream_t gs) {
+                double *d[3];
+                outs(k, d);
+                double *const h[3] = {oi, os, od};
+                const int64_t f0 = k * chunk, nf = frames_of(k);
+                for (int q = 0; q < 3; ++q)
+                    if (d[q])
+                        DG_CUDA(cudaMemcpyAsync(h[q] + f0 * nb, d[q], size_t(nf * nb) * 8,
+                                                cudaMemcpyDeviceToHost, gs));
+            });
         dg::check_bin_tile_waits(plan->gather);
     });
-    if (st != DG_OK && plan) {
-        // leave nothing of this call in flight (queued copies read the
-        // caller's frames until they complete)
-        if (plan->copy_stream) cudaStreamSynchronize(plan->copy_stream);
-        if (plan->stream) cudaStreamSynchronize(plan->stream);
-    }
-    return st;
 }
 
 dg_status dg_plan_profile(dg_plan *plan, int32_t enable) {

@@ -800,9 +800,28 @@ def main():
         for _ in range(reps):
             e2e_step()
         dt = time.perf_counter() - t0
+        h2d = int(host.numel() * host.element_size())
         line["e2e"] = {"value": round(n_frames * reps / dt, 2), "unit": "frames/s",
-                       "h2d_bytes_per_step": int(host.numel() * host.element_size()),
+                       "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": int(n_frames * nb * k_out * 8)}
+        # The host link's own rate for comparison: the same page-locked
+        # frames copied to the device (onto identical contents) with nothing
+        # else queued, CUDA events on the copying stream.
+        with torch.cuda.stream(stream):
+            frames.copy_(host, non_blocking=True)
+        torch.cuda.synchronize()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(reps):
+                frames.copy_(host, non_blocking=True)
+        l1.record(stream)
+        torch.cuda.synchronize()
+        link = h2d * reps / (l0.elapsed_time(l1) / 1000.0) / 1e9
+        line["e2e"]["link"] = {"h2d_gbs": round(link, 1),
+                               "e2e_h2d_gbs": round(h2d * reps / dt / 1e9, 1),
+                               "frac": round(h2d * reps / dt / 1e9 / link, 3),
+                               "what": "bare page-locked host-to-device copy of the same frames"}
         del host
         if w.dtype in ("uint16", "uint32", "int32"):
             line["e2e_bslz4"] = bslz4_leg(w, plan, frames, n_frames, flags, hi, hs, hd, peak)
